@@ -1,0 +1,106 @@
+"""ctypes binding of libanechoic.so (the C ABI in include/anechoic.h).
+
+The library is built in-tree (``python -m anechoic_b200.build_ext``). There is no fallback: if the library is missing
+or CUDA is unavailable, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libanechoic.so")
+
+ANC_OK, ANC_EINVAL, ANC_ECUDA, ANC_ETIMEOUT, ANC_EMISMATCH = 0, -1, -2, -3, -4
+ENGINES = {"auto": 0, "plain": 1, "tensor": 2}
+
+EXPORTS = ("anc_instance_create", "anc_instance_create_csr", "anc_instance_get_info", "anc_instance_destroy",
+           "anc_tables_create", "anc_tables_from_schedule", "anc_tables_steps", "anc_tables_read", "anc_tables_destroy",
+           "anc_range_plan", "anc_schedule_tables", "anc_plan_ranges", "anc_spin_words", "anc_np", "anc_run",
+           "anc_run_fields", "anc_run_device",
+           "anc_run_batch", "anc_last_device_ms", "anc_last_error", "anc_version")
+
+
+class AncError(RuntimeError):
+    """Error status from the C ABI (code is one of ANC_E*)."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+class InstanceInfo(C.Structure):
+    _fields_ = [("n", C.c_int), ("np", C.c_int), ("kbits", C.c_int), ("sparse", C.c_int), ("nnz", C.c_int64),
+                ("sumw", C.c_int64), ("maxabs", C.c_int32), ("hmax", C.c_int64), ("bmax", C.c_int32),
+                ("mean_row_sq", C.c_double)]
+
+
+class RunOpts(C.Structure):
+    _fields_ = [("engine", C.c_int), ("wide", C.c_int), ("threads", C.c_int), ("reserved", C.c_int * 5)]
+
+
+class Job(C.Structure):
+    _fields_ = [("inst", C.c_void_p), ("tb", C.c_void_p), ("seed", C.c_uint64), ("trial_offset", C.c_uint32),
+                ("nchains", C.c_int), ("spins", C.c_void_p), ("sum_sh", C.c_void_p), ("sum_bs", C.c_void_p),
+                ("flips", C.c_void_p), ("trace", C.c_void_p)]
+
+
+_lib = None
+_lock = threading.Lock()
+
+_vp, _i, _u32, _u64, _d = C.c_void_p, C.c_int, C.c_uint32, C.c_uint64, C.c_double
+
+
+def load(path: str = LIB_PATH) -> C.CDLL:
+    """Load the library once; raise if it is missing (no CPU fallback exists)."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} is missing: build it with `python -m anechoic_b200.build_ext`")
+        L = C.CDLL(path)
+        L.anc_instance_create.argtypes = [_vp, _i, _i, _vp, C.POINTER(_vp)]
+        L.anc_instance_create_csr.argtypes = [_i, _vp, _vp, _vp, _vp, C.POINTER(_vp)]
+        L.anc_instance_get_info.argtypes = [_vp, C.POINTER(InstanceInfo)]
+        L.anc_instance_destroy.argtypes = [_vp]
+        L.anc_instance_destroy.restype = None
+        L.anc_tables_create.argtypes = [_vp, _vp, _vp, _vp, _i, C.POINTER(_vp)]
+        L.anc_tables_from_schedule.argtypes = [_i, _d, _d, _d, _d, _d, _d, _i, _d, C.POINTER(_vp)]
+        L.anc_tables_steps.argtypes = [_vp]
+        L.anc_tables_read.argtypes = [_vp, _vp, _vp, _vp, _vp]
+        L.anc_tables_destroy.argtypes = [_vp]
+        L.anc_tables_destroy.restype = None
+        L.anc_range_plan.argtypes = [_vp, _vp, C.POINTER(_i), C.POINTER(C.c_int32)]
+        L.anc_schedule_tables.argtypes = [_i, _d, _d, _d, _d, _d, _d, _i, _d, _vp, _vp, _vp, _vp]
+        L.anc_plan_ranges.argtypes = [_i, C.c_int64, C.c_int64, _vp, _vp, _vp, _vp, _i, C.POINTER(_i),
+                                      C.POINTER(C.c_int32)]
+        L.anc_spin_words.argtypes = [_i]
+        L.anc_np.argtypes = [_i]
+        L.anc_run.argtypes = [_vp, _vp, _u64, _u32, _i, C.POINTER(RunOpts), _vp, _vp, _vp, _vp, _vp]
+        L.anc_run_fields.argtypes = [_vp, _vp, _u64, _u32, _i, C.POINTER(RunOpts), _vp, _vp, _vp, _vp, _vp, _vp]
+        L.anc_run_device.argtypes = [_vp, _vp, _u64, _u32, _i, C.POINTER(RunOpts), _vp, _vp, _vp, _vp, _vp, _vp]
+        L.anc_run_batch.argtypes = [_i, C.POINTER(Job), C.POINTER(RunOpts)]
+        L.anc_last_device_ms.argtypes = []
+        L.anc_last_device_ms.restype = C.c_double
+        L.anc_last_error.argtypes = []
+        L.anc_last_error.restype = C.c_char_p
+        L.anc_version.argtypes = []
+        L.anc_version.restype = C.c_char_p
+        _lib = L
+        return L
+
+
+def check(rc: int):
+    if rc != ANC_OK:
+        msg = load().anc_last_error().decode(errors="replace")
+        raise AncError(rc, msg)
+
+
+def opts(engine: str = "auto", wide="auto") -> RunOpts:
+    o = RunOpts()
+    o.engine = ENGINES[engine]
+    o.wide = {"auto": -1, 0: 0, 1: 1, False: 0, True: 1, "0": 0, "1": 1}[wide]
+    o.threads = 0
+    return o

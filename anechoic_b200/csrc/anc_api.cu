@@ -1,0 +1,720 @@
+// C ABI of the B200 SCA engines (include/anechoic.h): instances, tables, the int32 range plan, launches and readback.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/anechoic.h"
+#include "anc_plain.cuh"
+#include "anc_tensor.cuh"
+
+namespace {
+
+thread_local std::string g_err;
+thread_local double g_dev_ms = 0.0;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+    return fail(ANC_ECUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define CK(call)                                                   \
+    do {                                                           \
+        cudaError_t e_ = (call);                                   \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call);        \
+    } while (0)
+
+template <typename T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    ~DevBuf() { if (p) cudaFree(p); }
+    cudaError_t ensure(size_t count) {
+        if (count <= n && p) return cudaSuccess;
+        if (p) { cudaFree(p); p = nullptr; n = 0; }
+        cudaError_t e = cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T));
+        if (e == cudaSuccess) n = count;
+        return e;
+    }
+};
+
+int pad_np(int n) { return std::max(2048, ((n + 255) / 256) * 256); }
+
+}  // namespace
+
+struct anc_instance {
+    int n = 0, np = 0, nw = 0, nwj = 0, K = 0;   // K = 0: sparse
+    anc_instance_info info{};
+    std::vector<int32_t> bias;                    // host copy (empty = none)
+    DevBuf<uint32_t> planes;
+    DevBuf<int32_t> row_ptr;
+    DevBuf<uint32_t> adj;
+    DevBuf<int32_t> d_bias;
+    std::vector<int8_t> dense;                    // host copy of dense couplings (tensor engine packs lazily)
+    anc::TensorInstance tensor;                   // tensor-engine operands (built on first use)
+    bool tensor_ready = false;
+    // per-handle workspace for single-job launches
+    DevBuf<int> counter;
+    DevBuf<uint32_t> w_spins;
+    DevBuf<long long> w_sh, w_bs, w_fl;
+    DevBuf<int32_t> w_trace, w_h;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int device = 0, sms = 0;
+    ~anc_instance() {
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+struct anc_tables {
+    int S = 0;
+    std::vector<int32_t> fourT, q, kconst;
+    std::vector<int64_t> kcorr;
+    DevBuf<int32_t> d_fourT, d_q, d_kconst;
+    DevBuf<int64_t> d_kcorr;
+};
+
+namespace {
+
+void compute_info(anc_instance* I, const int32_t* row_ptr, const int32_t* col, const int8_t* val) {
+    anc_instance_info& f = I->info;
+    f.n = I->n;
+    f.np = I->np;
+    f.kbits = I->K;
+    f.sparse = I->K == 0;
+    int64_t sumw = 0, hmax = 0, nnz = 0;
+    int32_t maxabs = 0;
+    double sq = 0;
+    for (int x = 0; x < I->n; ++x) {
+        int64_t row = 0;
+        for (int k = row_ptr[x]; k < row_ptr[x + 1]; ++k) {
+            const int v = val[k];
+            if (col[k] > x) sumw -= v;
+            row += std::abs(v);
+            maxabs = std::max(maxabs, int32_t(std::abs(v)));
+            sq += double(v) * v;
+            ++nnz;
+        }
+        hmax = std::max(hmax, row);
+    }
+    f.nnz = nnz;
+    f.sumw = sumw;
+    f.maxabs = maxabs;
+    f.hmax = hmax;
+    f.mean_row_sq = I->n ? sq / I->n : 0.0;
+    int32_t bm = 0;
+    for (int32_t b : I->bias) bm = std::max(bm, int32_t(std::abs(b)));
+    f.bmax = bm;
+}
+
+int finish_common(anc_instance* I, const int32_t* bias) {
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    I->device = dev;
+    CK(cudaDeviceGetAttribute(&I->sms, cudaDevAttrMultiProcessorCount, dev));
+    if (bias) {
+        I->bias.assign(bias, bias + I->n);
+        for (int32_t b : I->bias)
+            if (b < -32767 || b > 32767) return fail(ANC_EINVAL, "bias outside |b| <= 32767 (B_BITS = 16)");
+        CK(I->d_bias.ensure(I->n));
+        CK(cudaMemcpy(I->d_bias.p, bias, sizeof(int32_t) * I->n, cudaMemcpyHostToDevice));
+    }
+    CK(cudaStreamCreateWithFlags(&I->stream, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&I->ev0));
+    CK(cudaEventCreate(&I->ev1));
+    CK(I->counter.ensure(1));
+    return ANC_OK;
+}
+
+anc::DevTables dev_tables(anc_tables* tb) {
+    anc::DevTables d;
+    d.fourT = tb->d_fourT.p;
+    d.q = tb->d_q.p;
+    d.kcorr = tb->d_kcorr.p;
+    d.kconst = tb->d_kconst.p;
+    d.S = tb->S;
+    return d;
+}
+
+struct Plan {
+    bool plain_ok = false;
+    int32_t hclamp = 0;
+};
+
+// Range plan: host::plan_ranges (gpu/multibit_bias_20261008/src/sca_gpu_bias.cu:543-557) semantics. The decision
+// evaluates hs * 65536 + x with |x| <= |q| + |corr| + 4T; n_lin <= n bounds |corr|.
+int range_plan_raw(int n, int64_t hmax, int64_t bmax, const int32_t* fourT, const int32_t* q, const int64_t* kcorr,
+                   const int32_t* kconst, int S, Plan* out) {
+    const int64_t lim = (int64_t(1) << 31) - 1;
+    int64_t xm = 0;
+    for (int t = 0; t < S; ++t) {
+        if (fourT[t] <= 0) return fail(ANC_EINVAL, "fourT must be positive (step %d)", t);
+        const int64_t kc = kcorr[t] < 0 ? -kcorr[t] : kcorr[t];
+        if (kc > (int64_t(1) << 40)) return fail(ANC_EINVAL, "kcorr out of range at step %d", t);
+        const int64_t corr_max = ((int64_t(n) * kc) >> 8) + std::llabs(int64_t(kconst[t])) + 1;
+        xm = std::max<int64_t>(xm, std::llabs(int64_t(q[t])) + corr_max + int64_t(fourT[t]));
+    }
+    const int64_t H = hmax + bmax;
+    out->plain_ok = H * 65536 + xm < lim;
+    const int64_t hc = xm / 65536 + 1;
+    if (65536 * hc + xm >= lim)
+        return fail(ANC_EINVAL, "table range exceeds int32 kernel arithmetic even with clamping");
+    out->hclamp = int32_t(hc);
+    return ANC_OK;
+}
+
+int range_plan(const anc_instance* I, const anc_tables* tb, Plan* out) {
+    return range_plan_raw(I->n, I->info.hmax, I->info.bmax, tb->fourT.data(), tb->q.data(), tb->kcorr.data(),
+                          tb->kconst.data(), tb->S, out);
+}
+
+int resolve_clamp(const anc_instance* I, const anc_tables* tb, const anc_run_opts* o, int32_t* hclamp) {
+    Plan pl;
+    int rc = range_plan(I, tb, &pl);
+    if (rc) return rc;
+    const int wide = o ? o->wide : -1;
+    if (wide == 0 && !pl.plain_ok)
+        return fail(ANC_EINVAL, "instance needs the clamped decision (|J| row sum + |b| too large for int32 decisions)");
+    *hclamp = (wide == 1 || !pl.plain_ok) ? pl.hclamp : 0;
+    return ANC_OK;
+}
+
+int plain_P(int np_max) { return np_max <= 2048 ? 12 : 16; }
+
+struct OutPtrs {
+    uint32_t* spins;
+    long long *sh, *bs, *fl;
+    int32_t *trace, *h;
+};
+
+anc::PlainJob make_job(anc_instance* I, anc_tables* tb, uint64_t seed, uint32_t off, int nchains, int32_t hclamp,
+                       const OutPtrs& o) {
+    anc::PlainJob j{};
+    j.n = I->n;
+    j.np = I->np;
+    j.nw = I->nw;
+    j.nwj = I->nwj;
+    j.K = I->K;
+    j.planes = I->planes.p;
+    j.row_ptr = I->row_ptr.p;
+    j.adj = I->adj.p;
+    j.bias = I->bias.empty() ? nullptr : I->d_bias.p;
+    j.tab = dev_tables(tb);
+    j.seed = seed;
+    j.trial_offset = off;
+    j.ntrials = nchains;
+    j.trace = o.trace != nullptr;
+    j.hclamp = hclamp;
+    j.out_spins = o.spins;
+    j.out_sum_sh = reinterpret_cast<int64_t*>(o.sh);
+    j.out_sum_bs = reinterpret_cast<int64_t*>(o.bs);
+    j.out_flips = reinterpret_cast<int64_t*>(o.fl);
+    j.out_trace = o.trace;
+    j.out_h = o.h;
+    return j;
+}
+
+int launch_plain_single(anc_instance* I, const anc::PlainJob& job, cudaStream_t st) {
+    anc::PlainLaunch L{};
+    L.job0 = job;
+    L.jobs = nullptr;
+    L.items = nullptr;
+    L.nitems = job.ntrials;
+    L.next_item = I->counter.p;
+    L.np_max = I->np;
+    L.nwj_max = I->K == 0 ? I->nw : I->nwj;
+    const int P = plain_P(I->np);
+    const size_t smem = anc::plain_smem_bytes(L.np_max, L.nwj_max, I->K, P);
+    if (smem > 227 * 1024) return fail(ANC_EINVAL, "instance too large for the plain engine (%zu B shared memory)", smem);
+    int per_sm = 0;
+    int rc = anc::plain_max_blocks_per_sm(I->K, P, smem, &per_sm);
+    if (rc) return cuda_fail(cudaError_t(rc), "occupancy");
+    if (per_sm < 1) return fail(ANC_EINVAL, "plain engine cannot be resident (smem %zu)", smem);
+    const int grid = std::max(1, std::min(job.ntrials, per_sm * I->sms));
+    CK(cudaMemsetAsync(I->counter.p, 0, sizeof(int), st));
+    rc = anc::plain_launch(L, I->K, P, grid, smem, st);
+    if (rc) return cuda_fail(cudaError_t(rc), "plain engine launch");
+    return ANC_OK;
+}
+
+int pick_engine(anc_instance* I, anc_tables* tb, int nchains, const anc_run_opts* o) {
+    const int e = o ? o->engine : ANC_ENGINE_AUTO;
+    if (e == ANC_ENGINE_PLAIN || e == ANC_ENGINE_TENSOR) return e;
+    return anc::tensor_supported(I->n, I->K, nchains) && anc::tensor_prefer(I->n, I->K, nchains, tb->S)
+               ? ANC_ENGINE_TENSOR
+               : ANC_ENGINE_PLAIN;
+}
+
+int ensure_tensor(anc_instance* I) {
+    if (I->tensor_ready) return ANC_OK;
+    if (I->dense.empty()) return fail(ANC_EINVAL, "the tensor engine needs dense couplings");
+    std::string why;
+    const int rc = anc::tensor_build_instance(I->dense.data(), I->n, &I->tensor, &why);
+    if (rc) return fail(rc == -2 ? ANC_ECUDA : ANC_EINVAL, "tensor engine setup: %s", why.c_str());
+    I->tensor_ready = true;
+    return ANC_OK;
+}
+
+// Launch on device outputs; no synchronisation.
+int run_device_impl(anc_instance* I, anc_tables* tb, uint64_t seed, uint32_t off, int nchains, const anc_run_opts* o,
+                    const OutPtrs& out, cudaStream_t st) {
+    if (!I || !tb) return fail(ANC_EINVAL, "null handle");
+    if (nchains < 1) return fail(ANC_EINVAL, "nchains must be >= 1");
+    if (!out.spins || !out.sh || !out.fl) return fail(ANC_EINVAL, "spins, sum_sh and flips outputs are required");
+    int32_t hclamp = 0;
+    int rc = resolve_clamp(I, tb, o, &hclamp);
+    if (rc) return rc;
+    const int engine = pick_engine(I, tb, nchains, o);
+    if (engine == ANC_ENGINE_TENSOR) {
+        if (!anc::tensor_supported(I->n, I->K, nchains))
+            return fail(ANC_EINVAL, "tensor engine does not support n=%d K=%d", I->n, I->K);
+        rc = ensure_tensor(I);
+        if (rc) return rc;
+        anc::TensorRun r{};
+        r.tab = dev_tables(tb);
+        r.seed = seed;
+        r.trial_offset = off;
+        r.nchains = nchains;
+        r.hclamp = hclamp;
+        r.bias = I->bias.empty() ? nullptr : I->d_bias.p;
+        r.out_spins = out.spins;
+        r.out_sum_sh = reinterpret_cast<int64_t*>(out.sh);
+        r.out_sum_bs = reinterpret_cast<int64_t*>(out.bs);
+        r.out_flips = reinterpret_cast<int64_t*>(out.fl);
+        r.out_trace = out.trace;
+        r.out_h = out.h;
+        std::string why;
+        rc = anc::tensor_run(&I->tensor, r, st, &why);
+        if (rc == -3) return fail(ANC_ETIMEOUT, "tensor engine: %s", why.c_str());
+        if (rc) return fail(rc == -2 ? ANC_ECUDA : ANC_EINVAL, "tensor engine: %s", why.c_str());
+        return ANC_OK;
+    }
+    const anc::PlainJob job = make_job(I, tb, seed, off, nchains, hclamp, out);
+    return launch_plain_single(I, job, st);
+}
+
+int run_host_impl(anc_instance* I, anc_tables* tb, uint64_t seed, uint32_t off, int nchains, const anc_run_opts* o,
+                  uint64_t* spins, int64_t* sum_sh, int64_t* sum_bs, int64_t* flips, int32_t* trace,
+                  int32_t* fields) {
+    if (!I || !tb) return fail(ANC_EINVAL, "null handle");
+    if (nchains < 1) return fail(ANC_EINVAL, "nchains must be >= 1");
+    if (!spins || !sum_sh) return fail(ANC_EINVAL, "spins and sum_sh outputs are required");
+    const size_t nw = size_t(I->nw);
+    CK(I->w_spins.ensure(nw * nchains));
+    CK(I->w_sh.ensure(nchains));
+    CK(I->w_bs.ensure(nchains));
+    CK(I->w_fl.ensure(nchains));
+    if (trace) CK(I->w_trace.ensure(size_t(nchains) * tb->S));
+    if (fields) CK(I->w_h.ensure(size_t(nchains) * I->n));
+    OutPtrs out{I->w_spins.p, I->w_sh.p, I->w_bs.p, I->w_fl.p, trace ? I->w_trace.p : nullptr,
+                fields ? I->w_h.p : nullptr};
+    cudaStream_t st = I->stream;
+    CK(cudaEventRecord(I->ev0, st));
+    int rc = run_device_impl(I, tb, seed, off, nchains, o, out, st);
+    if (rc) return rc;
+    CK(cudaEventRecord(I->ev1, st));
+    CK(cudaMemcpyAsync(spins, I->w_spins.p, nw * nchains * 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(sum_sh, I->w_sh.p, size_t(nchains) * 8, cudaMemcpyDeviceToHost, st));
+    if (sum_bs) CK(cudaMemcpyAsync(sum_bs, I->w_bs.p, size_t(nchains) * 8, cudaMemcpyDeviceToHost, st));
+    if (flips) CK(cudaMemcpyAsync(flips, I->w_fl.p, size_t(nchains) * 8, cudaMemcpyDeviceToHost, st));
+    if (trace) CK(cudaMemcpyAsync(trace, I->w_trace.p, size_t(nchains) * tb->S * 4, cudaMemcpyDeviceToHost, st));
+    if (fields) CK(cudaMemcpyAsync(fields, I->w_h.p, size_t(nchains) * I->n * 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, I->ev0, I->ev1));
+    g_dev_ms = ms;
+    return ANC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* anc_last_error(void) { return g_err.c_str(); }
+const char* anc_version(void) { return "anechoic-b200 0.1 (sm_100a)"; }
+double anc_last_device_ms(void) { return g_dev_ms; }
+int anc_np(int n) { return pad_np(n); }
+int anc_spin_words(int n) { return pad_np(n) / 64; }
+
+int anc_instance_create(const int8_t* J, int n, int kbits, const int32_t* bias, anc_instance** out) {
+    if (!out) return fail(ANC_EINVAL, "out is null");
+    *out = nullptr;
+    if (!J || n < 1 || n > 65536) return fail(ANC_EINVAL, "need J and 1 <= n <= 65536");
+    std::unique_ptr<anc_instance> I(new anc_instance());
+    I->n = n;
+    I->np = pad_np(n);
+    I->nw = I->np / 32;
+    I->nwj = ((I->nw + 31) / 32) * 32;
+    // validate and derive statistics (via CSR of the nonzeros)
+    std::vector<int32_t> rp(size_t(n) + 1, 0), col;
+    std::vector<int8_t> val;
+    bool pm1 = true;
+    int maxabs = 0;
+    for (int x = 0; x < n; ++x) {
+        const int8_t* row = J + size_t(x) * n;
+        if (row[x] != 0) return fail(ANC_EINVAL, "nonzero diagonal coupling at %d", x);
+        for (int y = 0; y < n; ++y) {
+            const int v = row[y];
+            if (v != J[size_t(y) * n + x]) return fail(ANC_EINVAL, "J not symmetric at (%d, %d)", x, y);
+            if (y != x && v != 1 && v != -1) pm1 = false;
+            if (v) { col.push_back(y); val.push_back(int8_t(v)); maxabs = std::max(maxabs, std::abs(v)); }
+        }
+        rp[x + 1] = int32_t(col.size());
+    }
+    int K = kbits;
+    if (K == 0) K = pm1 ? 1 : (maxabs <= 1 ? 2 : (maxabs <= 7 ? 4 : 8));
+    if (K == 1 && !pm1) return fail(ANC_EINVAL, "kbits = 1 needs a +-1 complete graph");
+    if (K != 1 && K != 2 && K != 4) return fail(ANC_EINVAL, "kbits must be 1, 2 or 4 (|J| <= 7)");
+    if (maxabs > (1 << (K - 1)) - 1 && K != 1) return fail(ANC_EINVAL, "|J| = %d exceeds 2^(K-1)-1 for K=%d", maxabs, K);
+    I->K = K;
+    if (bias) I->bias.assign(bias, bias + n);
+    compute_info(I.get(), rp.data(), col.data(), val.data());
+    // bit planes: [Kp][np][nwj]; K = 1: bit = [J = +1]; K >= 2: plane 0 = [J < 0], plane b = bit b-1 of |J|
+    const int Kp = K;
+    const size_t plane_words = size_t(I->np) * I->nwj;
+    std::vector<uint32_t> P(plane_words * Kp, 0u);
+    for (int x = 0; x < n; ++x) {
+        const int8_t* row = J + size_t(x) * n;
+        for (int y = 0; y < n; ++y) {
+            const int v = row[y];
+            if (!v) continue;
+            const size_t wd = size_t(x) * I->nwj + (y >> 5);
+            const uint32_t bit = 1u << (y & 31);
+            if (K == 1) {
+                if (v > 0) P[wd] |= bit;
+            } else {
+                if (v < 0) P[wd] |= bit;
+                const int a = std::abs(v);
+                for (int b = 1; b < K; ++b)
+                    if ((a >> (b - 1)) & 1) P[size_t(b) * plane_words + wd] |= bit;
+            }
+        }
+    }
+    I->dense.assign(J, J + size_t(n) * n);
+    int rc = finish_common(I.get(), bias);
+    if (rc) return rc;
+    cudaError_t e = I->planes.ensure(P.size());
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(planes)");
+    e = cudaMemcpy(I->planes.p, P.data(), P.size() * 4, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy(planes)");
+    *out = I.release();
+    return ANC_OK;
+}
+
+int anc_instance_create_csr(int n, const int32_t* row_ptr, const int32_t* col, const int8_t* val, const int32_t* bias,
+                            anc_instance** out) {
+    if (!out) return fail(ANC_EINVAL, "out is null");
+    *out = nullptr;
+    if (!row_ptr || n < 1 || n > (1 << 24)) return fail(ANC_EINVAL, "need row_ptr and 1 <= n < 2^24");
+    if (row_ptr[0] != 0) return fail(ANC_EINVAL, "row_ptr[0] must be 0");
+    for (int x = 0; x < n; ++x)
+        if (row_ptr[x + 1] < row_ptr[x]) return fail(ANC_EINVAL, "row_ptr not monotone at %d", x);
+    const int64_t nnz = row_ptr[n];
+    if (nnz > 0 && (!col || !val)) return fail(ANC_EINVAL, "col and val required");
+    std::vector<std::pair<int64_t, int8_t>> keys, keysT;
+    keys.reserve(nnz);
+    keysT.reserve(nnz);
+    std::vector<uint32_t> adj(nnz);
+    for (int x = 0; x < n; ++x)
+        for (int k = row_ptr[x]; k < row_ptr[x + 1]; ++k) {
+            const int y = col[k];
+            if (y < 0 || y >= n) return fail(ANC_EINVAL, "column index out of range in row %d", x);
+            if (y == x) return fail(ANC_EINVAL, "nonzero diagonal coupling at %d", x);
+            if (val[k] == 0) return fail(ANC_EINVAL, "explicit zero coupling in row %d", x);
+            if (val[k] == -128) return fail(ANC_EINVAL, "coupling -128 not supported");
+            keys.push_back({int64_t(x) * n + y, val[k]});
+            keysT.push_back({int64_t(y) * n + x, val[k]});
+            adj[k] = (uint32_t(y) << 8) | uint8_t(val[k]);
+        }
+    std::sort(keys.begin(), keys.end());
+    std::sort(keysT.begin(), keysT.end());
+    if (keys != keysT) return fail(ANC_EINVAL, "J not symmetric (or duplicate entries)");
+    for (size_t i = 1; i < keys.size(); ++i)
+        if (keys[i].first == keys[i - 1].first) return fail(ANC_EINVAL, "duplicate coupling");
+    std::unique_ptr<anc_instance> I(new anc_instance());
+    I->n = n;
+    I->np = pad_np(n);
+    I->nw = I->np / 32;
+    I->nwj = ((I->nw + 31) / 32) * 32;
+    I->K = 0;
+    if (bias) I->bias.assign(bias, bias + n);
+    compute_info(I.get(), row_ptr, col, val);
+    int rc = finish_common(I.get(), bias);
+    if (rc) return rc;
+    cudaError_t e = I->row_ptr.ensure(size_t(n) + 1);
+    if (e == cudaSuccess) e = cudaMemcpy(I->row_ptr.p, row_ptr, (size_t(n) + 1) * 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = I->adj.ensure(std::max<int64_t>(nnz, 1));
+    if (e == cudaSuccess && nnz) e = cudaMemcpy(I->adj.p, adj.data(), size_t(nnz) * 4, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(e, "upload CSR");
+    *out = I.release();
+    return ANC_OK;
+}
+
+int anc_instance_get_info(const anc_instance* I, anc_instance_info* info) {
+    if (!I || !info) return fail(ANC_EINVAL, "null argument");
+    *info = I->info;
+    return ANC_OK;
+}
+
+void anc_instance_destroy(anc_instance* I) {
+    if (I) anc::tensor_free_instance(&I->tensor);
+    delete I;
+}
+
+int anc_tables_create(const int32_t* fourT, const int32_t* q, const int64_t* kcorr, const int32_t* kconst, int S,
+                      anc_tables** out) {
+    if (!out) return fail(ANC_EINVAL, "out is null");
+    *out = nullptr;
+    if (S < 1 || S > (1 << 20) || !fourT || !q || !kcorr || !kconst) return fail(ANC_EINVAL, "need 1 <= S and all arrays");
+    for (int t = 0; t < S; ++t)
+        if (fourT[t] <= 0) return fail(ANC_EINVAL, "fourT must be positive (step %d)", t);
+    std::unique_ptr<anc_tables> tb(new anc_tables());
+    tb->S = S;
+    tb->fourT.assign(fourT, fourT + S);
+    tb->q.assign(q, q + S);
+    tb->kcorr.assign(kcorr, kcorr + S);
+    tb->kconst.assign(kconst, kconst + S);
+    cudaError_t e = tb->d_fourT.ensure(S);
+    if (e == cudaSuccess) e = tb->d_q.ensure(S);
+    if (e == cudaSuccess) e = tb->d_kconst.ensure(S);
+    if (e == cudaSuccess) e = tb->d_kcorr.ensure(S);
+    if (e == cudaSuccess) e = cudaMemcpy(tb->d_fourT.p, fourT, size_t(S) * 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(tb->d_q.p, q, size_t(S) * 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(tb->d_kconst.p, kconst, size_t(S) * 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(tb->d_kcorr.p, kcorr, size_t(S) * 8, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(e, "upload tables");
+    *out = tb.release();
+    return ANC_OK;
+}
+
+// v80host::geom / build_tables (tables.hpp:14-40) and mb::tables (mb_common.hpp:132-154): the same double-precision
+// formula and rounding (std::pow, std::llround), so the tables are bit-identical to the reference's.
+int anc_tables_from_schedule(int S, double t0, double t1, double q, double lam, double jv, double kappa, int ramp,
+                             double scale, anc_tables** out) {
+    if (S < 1) return fail(ANC_EINVAL, "steps must be >= 1");
+    std::vector<int32_t> f(S), qq(S), kc(S);
+    std::vector<int64_t> kr(S);
+    const int rc = anc_schedule_tables(S, t0, t1, q, lam, jv, kappa, ramp, scale, f.data(), qq.data(), kr.data(),
+                                       kc.data());
+    if (rc) return rc;
+    return anc_tables_create(f.data(), qq.data(), kr.data(), kc.data(), S, out);
+}
+
+int anc_plan_ranges(int n, int64_t hmax, int64_t bmax, const int32_t* fourT, const int32_t* q, const int64_t* kcorr,
+                    const int32_t* kconst, int S, int* plain_ok, int32_t* hclamp) {
+    if (n < 1 || S < 1 || !fourT || !q || !kcorr || !kconst) return fail(ANC_EINVAL, "bad arguments");
+    Plan pl;
+    const int rc = range_plan_raw(n, hmax, bmax, fourT, q, kcorr, kconst, S, &pl);
+    if (rc) return rc;
+    if (plain_ok) *plain_ok = pl.plain_ok;
+    if (hclamp) *hclamp = pl.hclamp;
+    return ANC_OK;
+}
+
+int anc_schedule_tables(int S, double t0, double t1, double q, double lam, double jv, double kappa, int ramp,
+                        double scale, int32_t* fourT, int32_t* q_out, int64_t* kcorr, int32_t* kconst) {
+    if (S < 1 || !fourT || !q_out || !kcorr || !kconst) return fail(ANC_EINVAL, "bad arguments");
+    if (!(t0 > 0) || !(t1 > 0)) return fail(ANC_EINVAL, "temperatures must be positive");
+    std::vector<double> T(S), L(S, lam);
+    for (int t = 0; t < S; ++t) T[t] = t0 * std::pow(t1 / t0, double(t) / std::max(1, S - 1));
+    if (ramp)
+        for (int t = 0; t < S; ++t)
+            if (t >= 0.7 * S) L[t] = lam * (S - 1 - t) / std::max(1.0, S - 1 - 0.7 * S);
+    if (scale != 1.0)
+        for (double& l : L) l *= scale;
+    for (int t = 0; t < S; ++t) {
+        const double f = 4.0 * T[t] * 65536.0;
+        if (!(f >= 1.0 && f < 2147483647.0)) return fail(ANC_EINVAL, "4T out of the Q16.16 range at step %d", t);
+        fourT[t] = int32_t(std::llround(f));
+        q_out[t] = int32_t(std::llround(q * 65536.0));
+        kcorr[t] = t == 0 ? 0 : int64_t(std::llround(L[t] / (2.0 * T[t - 1]) * 16777216.0));
+        kconst[t] = t == 0 ? 0 : int32_t(std::llround(-jv * 65536.0));
+    }
+    if (kappa > 0)
+        for (int t = 1; t < S; ++t) {
+            const double rf = (ramp && t >= 0.7 * S) ? (S - 1 - t) / std::max(1.0, S - 1 - 0.7 * S) : 1.0;
+            const double k = scale != 1.0 ? kappa * scale : kappa;
+            kconst[t] = int32_t(std::llround(k * T[t - 1] * rf * 65536.0));
+            kcorr[t] = 0;
+        }
+    return ANC_OK;
+}
+
+int anc_tables_steps(const anc_tables* tb) { return tb ? tb->S : 0; }
+
+int anc_tables_read(const anc_tables* tb, int32_t* fourT, int32_t* q, int64_t* kcorr, int32_t* kconst) {
+    if (!tb) return fail(ANC_EINVAL, "null handle");
+    if (fourT) std::memcpy(fourT, tb->fourT.data(), size_t(tb->S) * 4);
+    if (q) std::memcpy(q, tb->q.data(), size_t(tb->S) * 4);
+    if (kcorr) std::memcpy(kcorr, tb->kcorr.data(), size_t(tb->S) * 8);
+    if (kconst) std::memcpy(kconst, tb->kconst.data(), size_t(tb->S) * 4);
+    return ANC_OK;
+}
+
+void anc_tables_destroy(anc_tables* tb) { delete tb; }
+
+int anc_range_plan(const anc_instance* I, const anc_tables* tb, int* plain_ok, int32_t* hclamp) {
+    if (!I || !tb) return fail(ANC_EINVAL, "null handle");
+    Plan pl;
+    const int rc = range_plan(I, tb, &pl);
+    if (rc) return rc;
+    if (plain_ok) *plain_ok = pl.plain_ok;
+    if (hclamp) *hclamp = pl.hclamp;
+    return ANC_OK;
+}
+
+int anc_run(anc_instance* I, anc_tables* tb, uint64_t seed, uint32_t off, int nchains, const anc_run_opts* o,
+            uint64_t* spins, int64_t* sum_sh, int64_t* sum_bs, int64_t* flips, int32_t* trace) {
+    return run_host_impl(I, tb, seed, off, nchains, o, spins, sum_sh, sum_bs, flips, trace, nullptr);
+}
+
+int anc_run_fields(anc_instance* I, anc_tables* tb, uint64_t seed, uint32_t off, int nchains, const anc_run_opts* o,
+                   uint64_t* spins, int64_t* sum_sh, int64_t* sum_bs, int64_t* flips, int32_t* trace,
+                   int32_t* fields) {
+    if (!fields) return fail(ANC_EINVAL, "fields output required");
+    return run_host_impl(I, tb, seed, off, nchains, o, spins, sum_sh, sum_bs, flips, trace, fields);
+}
+
+int anc_run_device(anc_instance* I, anc_tables* tb, uint64_t seed, uint32_t off, int nchains, const anc_run_opts* o,
+                   uint64_t* d_spins, int64_t* d_sum_sh, int64_t* d_sum_bs, int64_t* d_flips, int32_t* d_trace,
+                   void* stream) {
+    OutPtrs out{reinterpret_cast<uint32_t*>(d_spins), reinterpret_cast<long long*>(d_sum_sh),
+                reinterpret_cast<long long*>(d_sum_bs), reinterpret_cast<long long*>(d_flips), d_trace, nullptr};
+    if (!d_sum_bs) return fail(ANC_EINVAL, "sum_bs output required on the device path");
+    return run_device_impl(I, tb, seed, off, nchains, o, out, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int anc_run_batch(int njobs, const anc_job* jobs, const anc_run_opts* o) {
+    if (njobs < 1 || !jobs) return fail(ANC_EINVAL, "need jobs");
+    // group by kernel kind (sparse / dense K); each group is one persistent launch with a cost-ordered work queue
+    struct Prepared {
+        int idx;
+        int32_t hclamp;
+    };
+    std::vector<Prepared> prep;
+    for (int k = 0; k < njobs; ++k) {
+        const anc_job& j = jobs[k];
+        if (!j.inst || !j.tb || j.nchains < 1 || !j.spins || !j.sum_sh)
+            return fail(ANC_EINVAL, "job %d: need inst, tb, nchains >= 1, spins, sum_sh", k);
+        int32_t hc = 0;
+        const int rc = resolve_clamp(j.inst, j.tb, o, &hc);
+        if (rc) return rc;
+        prep.push_back({k, hc});
+    }
+    int dev = 0, sms = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    cudaStream_t st = nullptr;
+    CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    std::unique_ptr<CUstream_st, void (*)(cudaStream_t)> st_guard(st, [](cudaStream_t s) { cudaStreamDestroy(s); });
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    std::unique_ptr<CUevent_st, void (*)(cudaEvent_t)> g0(e0, [](cudaEvent_t e) { cudaEventDestroy(e); });
+    std::unique_ptr<CUevent_st, void (*)(cudaEvent_t)> g1(e1, [](cudaEvent_t e) { cudaEventDestroy(e); });
+    // per-job device outputs
+    struct JobBufs {
+        DevBuf<uint32_t> spins;
+        DevBuf<long long> sh, bs, fl;
+        DevBuf<int32_t> trace;
+    };
+    std::vector<std::unique_ptr<JobBufs>> bufs(njobs);
+    std::vector<anc::PlainJob> pj(njobs);
+    for (const Prepared& p : prep) {
+        const anc_job& j = jobs[p.idx];
+        bufs[p.idx].reset(new JobBufs());
+        JobBufs& b = *bufs[p.idx];
+        CK(b.spins.ensure(size_t(j.inst->nw) * j.nchains));
+        CK(b.sh.ensure(j.nchains));
+        CK(b.bs.ensure(j.nchains));
+        CK(b.fl.ensure(j.nchains));
+        if (j.trace) CK(b.trace.ensure(size_t(j.nchains) * j.tb->S));
+        OutPtrs out{b.spins.p, b.sh.p, b.bs.p, b.fl.p, j.trace ? b.trace.p : nullptr, nullptr};
+        pj[p.idx] = make_job(j.inst, j.tb, j.seed, j.trial_offset, j.nchains, p.hclamp, out);
+    }
+    DevBuf<anc::PlainJob> d_jobs;
+    CK(d_jobs.ensure(njobs));
+    CK(cudaMemcpy(d_jobs.p, pj.data(), sizeof(anc::PlainJob) * njobs, cudaMemcpyHostToDevice));
+    DevBuf<int> counters;
+    const int kinds[4] = {0, 1, 2, 4};
+    CK(counters.ensure(4));
+    CK(cudaMemsetAsync(counters.p, 0, 4 * sizeof(int), st));
+    std::vector<DevBuf<int2>> d_items(4);
+    CK(cudaEventRecord(e0, st));
+    for (int ki = 0; ki < 4; ++ki) {
+        const int K = kinds[ki];
+        std::vector<int> sel;
+        int np_max = 0, nwj_max = 0;
+        for (int k = 0; k < njobs; ++k)
+            if (jobs[k].inst->K == K) {
+                sel.push_back(k);
+                np_max = std::max(np_max, jobs[k].inst->np);
+                nwj_max = std::max(nwj_max, K == 0 ? jobs[k].inst->nw : jobs[k].inst->nwj);
+            }
+        if (sel.empty()) continue;
+        // longest-processing-time-first queue: cost ~ np * S per anneal (dense np^2 * S)
+        std::vector<std::pair<double, int2>> items;
+        for (int k : sel) {
+            const double cost = double(jobs[k].inst->np) * jobs[k].tb->S * (K == 0 ? 1.0 : double(jobs[k].inst->np));
+            for (int c = 0; c < jobs[k].nchains; ++c) items.push_back({cost, make_int2(k, c)});
+        }
+        std::stable_sort(items.begin(), items.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+        std::vector<int2> it(items.size());
+        for (size_t i = 0; i < items.size(); ++i) it[i] = items[i].second;
+        CK(d_items[ki].ensure(it.size()));
+        CK(cudaMemcpyAsync(d_items[ki].p, it.data(), it.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
+        anc::PlainLaunch L{};
+        L.jobs = d_jobs.p;
+        L.items = d_items[ki].p;
+        L.nitems = int(it.size());
+        L.next_item = counters.p + ki;
+        L.np_max = np_max;
+        L.nwj_max = nwj_max;
+        const int P = plain_P(np_max);
+        const size_t smem = anc::plain_smem_bytes(np_max, nwj_max, K, P);
+        if (smem > 227 * 1024) return fail(ANC_EINVAL, "batch instance too large for the plain engine");
+        int per_sm = 0;
+        int rc = anc::plain_max_blocks_per_sm(K, P, smem, &per_sm);
+        if (rc) return cuda_fail(cudaError_t(rc), "occupancy");
+        if (per_sm < 1) return fail(ANC_EINVAL, "plain engine cannot be resident");
+        const int grid = std::max(1, std::min(L.nitems, per_sm * sms));
+        rc = anc::plain_launch(L, K, P, grid, smem, st);
+        if (rc) return cuda_fail(cudaError_t(rc), "plain engine launch");
+    }
+    CK(cudaEventRecord(e1, st));
+    for (const Prepared& p : prep) {
+        const anc_job& j = jobs[p.idx];
+        JobBufs& b = *bufs[p.idx];
+        CK(cudaMemcpyAsync(j.spins, b.spins.p, size_t(j.inst->nw) * j.nchains * 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(j.sum_sh, b.sh.p, size_t(j.nchains) * 8, cudaMemcpyDeviceToHost, st));
+        if (j.sum_bs) CK(cudaMemcpyAsync(j.sum_bs, b.bs.p, size_t(j.nchains) * 8, cudaMemcpyDeviceToHost, st));
+        if (j.flips) CK(cudaMemcpyAsync(j.flips, b.fl.p, size_t(j.nchains) * 8, cudaMemcpyDeviceToHost, st));
+        if (j.trace)
+            CK(cudaMemcpyAsync(j.trace, b.trace.p, size_t(j.nchains) * j.tb->S * 4, cudaMemcpyDeviceToHost, st));
+    }
+    CK(cudaStreamSynchronize(st));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    g_dev_ms = ms;
+    return ANC_OK;
+}
+
+}  // extern "C"

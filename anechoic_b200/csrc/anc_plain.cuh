@@ -1,0 +1,73 @@
+// Plain SCA engine ("bit-column" path): one CTA of 512 threads runs one anneal at a time; a persistent grid pulls
+// (job, trial) items from a queue, so one launch carries many anneals and many instances of uneven size.
+//
+// Per step (exactly sca::run_trial_bias, reference gpu/multibit_bias_20261008/src/sca_ref_bias.hpp:44-68):
+//   1. Warps 0..7 own RNG lanes 0..255. For each round k, lane l decides slot i = k*256 + l. The 32 slots of a warp
+//      in one round are spin word k*8 + warp, so one __ballot_sync gives the flip word, one gives the n_lin band word
+//      (n_lin = sum of __popc over them), and flipped slots are appended to a compact flip list in shared memory.
+//   2. Field update h_y += 2 * s'_x * J_xy over the flipped x only.
+//      Dense couplings are bit planes, row x = NWJ 32-bit words (32 couplings each): K = 1 one plane (bit = [J = +1]);
+//      K = 2, 4 a sign plane and K-1 magnitude planes. Thread (group g, word w) reads word w of each flipped row of
+//      its group (coalesced: a warp reads 128 contiguous bytes of one row) and adds it into bit-sliced counters with
+//      carry-save adders (a Harley-Seal tree over batches of 8 rows, LOP3 arithmetic, 32 couplings per op). The
+//      groups' counters are summed by a bit-sliced adder tree in shared memory; the deciding thread of slot y
+//      extracts y's count at the start of the next step, when it reads h_y.
+//      Sparse couplings (CSR rows) are scattered with shared-memory atomics, one warp per flipped row.
+//   The initial field h = b + J s0 reuses step 2 with F = all active slots and factor 1.
+// All arithmetic is integer and order-independent, so the result is bit-exact with the golden model.
+#pragma once
+#include <cstdint>
+
+#include "anc_common.cuh"
+
+namespace anc {
+
+constexpr int kPlainThreads = 512;
+
+struct PlainJob {
+    // instance
+    int n, np, nw, nwj, K;             // K = 0: sparse CSR
+    const uint32_t* planes;            // dense: [max(K,1)][np][nwj]
+    const int32_t* row_ptr;            // sparse: [n + 1]
+    const uint32_t* adj;               // sparse: (y << 8) | uint8(J_xy)
+    const int32_t* bias;               // [n] or null
+    DevTables tab;
+    uint64_t seed;
+    uint32_t trial_offset;
+    int ntrials;
+    int trace;
+    int32_t hclamp;                    // > 0: clamp s*h to +-hclamp in the decision (exact; host range plan)
+    // outputs (device pointers)
+    uint32_t* out_spins;               // [ntrials][nw]: bit i of word i/32 = [s_i = +1], active spins only
+    int64_t* out_sum_sh;               // [ntrials]
+    int64_t* out_sum_bs;               // [ntrials]
+    int64_t* out_flips;                // [ntrials]
+    int32_t* out_trace;                // [ntrials][S] or null
+    int32_t* out_h;                    // [ntrials][n] or null (final fields)
+};
+
+struct PlainLaunch {
+    PlainJob job0;                     // the job when items == nullptr (item index = trial index)
+    const PlainJob* jobs;              // device array when items != nullptr
+    const int2* items;                 // (job, trial index), or nullptr
+    int nitems;
+    int* next_item;                    // queue head (zeroed before launch)
+    int np_max, nwj_max;               // shared-memory layout
+};
+
+// Shared-memory bytes for a launch (P = counter planes).
+inline size_t plain_smem_bytes(int np_max, int nwj_max, int K, int P) {
+    const size_t C = K <= 1 ? 1 : size_t(2 * (K - 1));
+    size_t b = size_t(np_max) * 4 * 2 + size_t(nwj_max) * 4 * 2;
+    if (K != 0) {
+        const size_t comb = size_t(nwj_max > kPlainThreads ? nwj_max : kPlainThreads);
+        b += comb * P * 4 + C * size_t(nwj_max) * P * 4;
+    }
+    return b;
+}
+
+// Host launcher (plain_engine.cu). Returns a cudaError_t value.
+int plain_launch(const PlainLaunch& L, int K, int P, int grid, size_t smem, cudaStream_t stream);
+int plain_max_blocks_per_sm(int K, int P, size_t smem, int* out);
+
+}  // namespace anc

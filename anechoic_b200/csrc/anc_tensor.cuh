@@ -1,0 +1,37 @@
+// Batched SCA engine for replicas sharing J (tcgen05 int8 J * dS update); host-facing interface.
+#pragma once
+#include <cstdint>
+#include <string>
+
+#include "anc_common.cuh"
+
+namespace anc {
+
+struct TensorInstance {
+    int n = 0, np = 0;
+    int8_t* d_J = nullptr;       // operand layout built by tensor_build_instance
+    size_t bytes = 0;
+};
+
+struct TensorRun {
+    DevTables tab;
+    uint64_t seed;
+    uint32_t trial_offset;
+    int nchains;
+    int32_t hclamp;
+    const int32_t* bias;
+    uint32_t* out_spins;
+    int64_t* out_sum_sh;
+    int64_t* out_sum_bs;
+    int64_t* out_flips;
+    int32_t* out_trace;
+    int32_t* out_h;
+};
+
+bool tensor_supported(int n, int K, int nchains);
+bool tensor_prefer(int n, int K, int nchains, int S);
+int tensor_build_instance(const int8_t* J, int n, TensorInstance* out, std::string* why);
+int tensor_run(TensorInstance* ti, const TensorRun& r, cudaStream_t st, std::string* why);
+void tensor_free_instance(TensorInstance* ti);
+
+}  // namespace anc

@@ -1,0 +1,434 @@
+// Plain SCA engine kernels (see anc_plain.cuh for the algorithm and the reference lines it follows).
+#include "anc_plain.cuh"
+
+namespace anc {
+namespace {
+
+constexpr int T = kPlainThreads;
+constexpr uint32_t FULL = 0xffffffffu;
+
+// Bit-sliced counter: plane p holds bit p of 32 independent counts (one per bit position of the word).
+template <int P>
+struct BitCounter {
+    uint32_t c[P];
+
+    __device__ __forceinline__ void clear() {
+#pragma unroll
+        for (int p = 0; p < P; ++p) c[p] = 0;
+    }
+    // add 8 words (Harley-Seal: 7 carry-save adders, then the weight-8 carry ripples upward while any lane has one)
+    __device__ __forceinline__ void add8(const uint32_t (&a)[8]) {
+        uint32_t t1a, t1b, t2a, t2b, t3;
+        csa(c[0], t1a, c[0], a[0], a[1]);
+        csa(c[0], t1b, c[0], a[2], a[3]);
+        csa(c[1], t2a, c[1], t1a, t1b);
+        csa(c[0], t1a, c[0], a[4], a[5]);
+        csa(c[0], t1b, c[0], a[6], a[7]);
+        csa(c[1], t2b, c[1], t1a, t1b);
+        csa(c[2], t3, c[2], t2a, t2b);
+#pragma unroll
+        for (int p = 3; p < P; ++p) {
+            if (!__any_sync(FULL, t3)) break;
+            const uint32_t k = c[p] & t3;
+            c[p] ^= t3;
+            t3 = k;
+        }
+    }
+    // c += other (ripple-carry over the planes; the total stays below 2^P by construction)
+    __device__ __forceinline__ void add_planes(const uint32_t* o) {
+        uint32_t carry = 0;
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+            const uint32_t a = c[p], b = o[p], u = a ^ b;
+            c[p] = u ^ carry;
+            carry = (a & b) | (u & carry);
+        }
+    }
+    __device__ __forceinline__ void store(uint32_t* dst) const {
+#pragma unroll
+        for (int p = 0; p < P; ++p) dst[p] = c[p];
+    }
+};
+
+// count of slot (word wi, bit lane) from combined planes res[wi * P + p]
+template <int P>
+__device__ __forceinline__ int32_t extract_count(const uint32_t* res_w, int lane) {
+    int32_t v = 0;
+#pragma unroll
+    for (int p = 0; p < P; ++p) v |= int32_t((res_w[p] >> lane) & 1u) << p;
+    return v;
+}
+
+__device__ __forceinline__ uint32_t valid_mask(int w, int n) {
+    const int lo = 32 * w;
+    if (lo + 32 <= n) return FULL;
+    if (lo >= n) return 0u;
+    return (1u << (n - lo)) - 1u;
+}
+
+// Append the flagged slot i (with its new-spin sign bit `neg`) to the flip list; warp-cooperative.
+__device__ __forceinline__ void append_flip(bool flag, int i, uint32_t neg, uint32_t* flist, int* counter, int lane) {
+    const uint32_t b = __ballot_sync(FULL, flag);
+    if (!b) return;
+    int base = 0;
+    if (lane == 0) base = atomicAdd(counter, __popc(b));
+    base = __shfl_sync(FULL, base, 0);
+    if (flag) flist[base + __popc(b & lanemask_lt())] = uint32_t(i) | (neg << 31);
+}
+
+__device__ __forceinline__ int64_t warp_sum64(int64_t v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+    return v;
+}
+
+// Dense field pass: bit-sliced counts of the flipped rows, combined across groups into res[cc][w][P].
+template <int K, int P>
+__device__ __forceinline__ void dense_pass(const uint32_t* __restrict__ planes, size_t plane_stride, int nwj, int nf,
+                                           const uint32_t* flist, uint32_t* comb, uint32_t* res) {
+    constexpr int NC = K <= 1 ? 1 : 2 * (K - 1);
+    const int tid = threadIdx.x;
+    if (nwj <= T) {
+        const int G = T / nwj, g = tid / nwj, w = tid - g * nwj;
+        const bool active = g < G;
+        BitCounter<P> cnt[NC];
+#pragma unroll
+        for (int cc = 0; cc < NC; ++cc) cnt[cc].clear();
+        if (active) {
+            for (int f0 = g; f0 < nf; f0 += 8 * G) {
+                uint32_t a[NC][8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const int f = f0 + j * G;
+                    if (f < nf) {
+                        const uint32_t e = flist[f];
+                        const uint32_t neg = (e >> 31) ? FULL : 0u;
+                        const uint32_t* row = planes + size_t(e & 0x7fffffffu) * nwj + w;
+                        if (K <= 1) {
+                            a[0][j] = __ldg(row) ^ neg;
+                        } else {
+                            const uint32_t t = __ldg(row) ^ neg;   // 1 where s'_x * sign(J_xy) = -1
+#pragma unroll
+                            for (int b = 1; b < (K <= 1 ? 2 : K); ++b) {
+                                const uint32_t m = __ldg(row + size_t(b) * plane_stride);
+                                a[2 * (b - 1)][j] = m & ~t;
+                                a[2 * (b - 1) + 1][j] = m & t;
+                            }
+                        }
+                    } else {
+#pragma unroll
+                        for (int cc = 0; cc < NC; ++cc) a[cc][j] = 0u;
+                    }
+                }
+#pragma unroll
+                for (int cc = 0; cc < NC; ++cc) cnt[cc].add8(a[cc]);
+            }
+        }
+        if (G == 1) {
+            if (active) {
+#pragma unroll
+                for (int cc = 0; cc < NC; ++cc) cnt[cc].store(res + (size_t(cc) * nwj + w) * P);
+            }
+            return;
+        }
+        int top = 1;
+        while (top < G) top <<= 1;
+#pragma unroll
+        for (int cc = 0; cc < NC; ++cc) {
+            if (active) cnt[cc].store(comb + (size_t(g) * nwj + w) * P);
+            __syncthreads();
+            for (int stride = top >> 1; stride >= 1; stride >>= 1) {
+                if (active && g < stride && g + stride < G) {
+                    cnt[cc].add_planes(comb + (size_t(g + stride) * nwj + w) * P);
+                    if (stride > 1) cnt[cc].store(comb + (size_t(g) * nwj + w) * P);
+                }
+                __syncthreads();
+            }
+            if (active && g == 0) cnt[cc].store(res + (size_t(cc) * nwj + w) * P);
+        }
+    } else {
+        for (int w0 = 0; w0 < nwj; w0 += T) {
+            const int w = w0 + tid;
+            if (w >= nwj) continue;   // nwj is a multiple of 32: whole warps skip together
+            BitCounter<P> cnt[NC];
+#pragma unroll
+            for (int cc = 0; cc < NC; ++cc) cnt[cc].clear();
+            for (int f0 = 0; f0 < nf; f0 += 8) {
+                uint32_t a[NC][8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const int f = f0 + j;
+                    if (f < nf) {
+                        const uint32_t e = flist[f];
+                        const uint32_t neg = (e >> 31) ? FULL : 0u;
+                        const uint32_t* row = planes + size_t(e & 0x7fffffffu) * nwj + w;
+                        if (K <= 1) {
+                            a[0][j] = __ldg(row) ^ neg;
+                        } else {
+                            const uint32_t t = __ldg(row) ^ neg;
+#pragma unroll
+                            for (int b = 1; b < (K <= 1 ? 2 : K); ++b) {
+                                const uint32_t m = __ldg(row + size_t(b) * plane_stride);
+                                a[2 * (b - 1)][j] = m & ~t;
+                                a[2 * (b - 1) + 1][j] = m & t;
+                            }
+                        }
+                    } else {
+#pragma unroll
+                        for (int cc = 0; cc < NC; ++cc) a[cc][j] = 0u;
+                    }
+                }
+#pragma unroll
+                for (int cc = 0; cc < NC; ++cc) cnt[cc].add8(a[cc]);
+            }
+#pragma unroll
+            for (int cc = 0; cc < NC; ++cc) cnt[cc].store(res + (size_t(cc) * nwj + w) * P);
+        }
+    }
+}
+
+// Field change of slot (wi, lane) from the last dense pass: sum_{x in F} s'_x J_xy, with the K = 1 diagonal and
+// membership corrections (in_f: y was in the pass's F; s_up: y's current spin is +1).
+template <int K, int P>
+__device__ __forceinline__ int32_t dense_delta(const uint32_t* res, int nwj, int wi, int lane, int nfp, bool in_f,
+                                               bool s_up) {
+    if (K <= 1) {
+        // raw count of x in F with s'_x J_xy = +1, plus x = y when y flipped to -1 (diagonal bit reads as +1 there)
+        const int32_t raw = extract_count<P>(res + size_t(wi) * P, lane);
+        const int32_t pos = raw - ((in_f && !s_up) ? 1 : 0);
+        return 2 * pos - nfp + (in_f ? 1 : 0);
+    } else {
+        int32_t v = 0;
+#pragma unroll
+        for (int b = 1; b < (K <= 1 ? 2 : K); ++b) {
+            const int32_t pc = extract_count<P>(res + (size_t(2 * (b - 1)) * nwj + wi) * P, lane);
+            const int32_t nc = extract_count<P>(res + (size_t(2 * (b - 1) + 1) * nwj + wi) * P, lane);
+            v += (pc - nc) << (b - 1);
+        }
+        return v;
+    }
+}
+
+template <int K, int P, bool SPARSE>
+__global__ void __launch_bounds__(T, 1) plain_kernel(const __grid_constant__ PlainLaunch L) {
+    extern __shared__ __align__(16) uint8_t smem_raw[];
+    __shared__ int s_item, s_nf[2], s_lin[8];
+    __shared__ long long s_red[2][16];
+    int32_t* h = reinterpret_cast<int32_t*>(smem_raw);
+    uint32_t* flist = reinterpret_cast<uint32_t*>(h + L.np_max);
+    uint32_t* Sw = flist + L.np_max;
+    uint32_t* Dw = Sw + L.nwj_max;
+    uint32_t* comb = Dw + L.nwj_max;
+    uint32_t* res = comb + size_t(L.nwj_max > T ? L.nwj_max : T) * P;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const bool decider = tid < kLanes;
+
+    for (;;) {
+        __syncthreads();
+        if (tid == 0) s_item = atomicAdd(L.next_item, 1);
+        __syncthreads();
+        const int item = s_item;
+        if (item >= L.nitems) break;
+        const int2 it = L.items ? L.items[item] : make_int2(0, item);
+        const PlainJob& job = L.items ? L.jobs[it.x] : L.job0;
+        const int n = job.n, np = job.np, R = np / kLanes, nw = job.nw, nwj = job.nwj, S = job.tab.S;
+        const int c = it.y;
+        const uint32_t* __restrict__ planes = job.planes;
+        const size_t plane_stride = size_t(np) * nwj;
+        const int32_t* __restrict__ fourT_t = job.tab.fourT;
+        const int32_t* __restrict__ q_t = job.tab.q;
+        const int64_t* __restrict__ kcorr_t = job.tab.kcorr;
+        const int32_t* __restrict__ kconst_t = job.tab.kconst;
+        const int32_t hclamp = job.hclamp;
+        const int32_t* __restrict__ bias = job.bias;
+        int32_t* trace_out = (job.trace && job.out_trace) ? job.out_trace + size_t(c) * S : nullptr;
+
+        for (int i = tid; i < np; i += T) h[i] = (i < n && bias) ? bias[i] : 0;
+        if (tid == 0) { s_nf[0] = 0; s_nf[1] = 0; }
+        __syncthreads();
+
+        // seed, initial spins (draw >> 31; padding +1), s_prev = +1 everywhere, initial flip list = all active slots
+        Xoshiro rng;
+        if (decider) {
+            rng_seed(rng, job.seed, job.trial_offset + uint32_t(c), uint32_t(tid));
+            for (int k = 0; k < R; ++k) {
+                const uint32_t r = rng_next(rng);
+                const int i = k * kLanes + tid;
+                const bool valid = i < n;
+                const uint32_t sbit = valid ? (r >> 31) : 1u;
+                const uint32_t sw = __ballot_sync(FULL, sbit != 0);
+                const uint32_t dw = __ballot_sync(FULL, valid && !sbit);
+                if (lane == 0) { Sw[k * 8 + warp] = sw; Dw[k * 8 + warp] = dw; }
+                append_flip(valid, i, sbit ^ 1u, flist, &s_nf[0], lane);
+            }
+        }
+        __syncthreads();
+        int pass_nf = s_nf[0];
+        int pass_mult = 1;
+        bool pass_init = true, pass_pending = false;
+        if (SPARSE) {
+            for (int f = warp; f < pass_nf; f += T / 32) {
+                const uint32_t e = flist[f];
+                const int x = int(e & 0x7fffffffu);
+                const int32_t m = (e >> 31) ? -1 : 1;
+                for (int k = job.row_ptr[x] + lane; k < job.row_ptr[x + 1]; k += 32) {
+                    const uint32_t a = __ldg(job.adj + k);
+                    atomicAdd(&h[a >> 8], m * int32_t(int8_t(a & 0xffu)));
+                }
+            }
+        } else {
+            dense_pass<K, P>(planes, plane_stride, nwj, pass_nf, flist, comb, res);
+            pass_pending = true;
+        }
+        __syncthreads();
+
+        int32_t nlin_prev = 0;
+        long long flips = 0;
+        for (int t = 0; t < S; ++t) {
+            const int buf = (t + 1) & 1;
+            if (tid == 0) s_nf[t & 1] = 0;   // buffer of step t-1 (or of the initial pass); step t appends to buf
+            if (decider) {
+                const int32_t fourT = __ldg(fourT_t + t), twoT = fourT >> 1, qv = __ldg(q_t + t);
+                const int32_t corr = step_corr(nlin_prev, __ldg(kcorr_t + t), __ldg(kconst_t + t));
+                const uint32_t lw = uint32_t(2 * twoT - 1);
+                int nl = 0;
+                for (int k = 0; k < R; ++k) {
+                    const uint32_t u = rng_next(rng);
+                    const int i = k * kLanes + tid, wi = k * 8 + warp;
+                    const bool valid = i < n;
+                    const uint32_t Sword = Sw[wi], Dword = Dw[wi];
+                    const bool s_up = (Sword >> lane) & 1u, dif = (Dword >> lane) & 1u;
+                    int32_t hv = h[i];
+                    if (!SPARSE && pass_pending) {
+                        hv += pass_mult * dense_delta<K, P>(res, nwj, wi, lane, pass_nf, pass_init || dif, s_up);
+                        if (valid) h[i] = hv;
+                    }
+                    int32_t hs = s_up ? hv : -hv;
+                    if (hclamp > 0) hs = max(-hclamp, min(hs, hclamp));
+                    const int32_t x = qv + (dif ? corr : -corr);      // q - (s == s_prev ? corr : -corr)
+                    const int32_t zt = hs * 65536 + x;
+                    const int32_t r = threshold16(u, fourT);
+                    const bool fl = valid && (zt - r < 0);
+                    const bool ln = valid && (uint32_t(zt + twoT - 1) < lw);
+                    const uint32_t fb = __ballot_sync(FULL, fl);
+                    nl += __popc(__ballot_sync(FULL, ln));
+                    if (lane == 0) { Sw[wi] = Sword ^ fb; Dw[wi] = fb; }
+                    append_flip(fl, i, s_up ? 1u : 0u, flist, &s_nf[buf], lane);
+                }
+                if (lane == 0) s_lin[warp] = nl;
+            }
+            __syncthreads();
+            const int nf = s_nf[buf];
+            int32_t nlin = 0;
+#pragma unroll
+            for (int w = 0; w < 8; ++w) nlin += s_lin[w];
+            if (tid == 0) {
+                flips += nf;
+                if (trace_out) trace_out[t] = nlin;
+            }
+            nlin_prev = nlin;
+            pass_nf = nf;
+            pass_mult = 2;
+            pass_init = false;
+            pass_pending = false;
+            if (nf > 0) {
+                if (SPARSE) {
+                    for (int f = warp; f < nf; f += T / 32) {
+                        const uint32_t e = flist[f];
+                        const int x = int(e & 0x7fffffffu);
+                        const int32_t m = (e >> 31) ? -2 : 2;
+                        for (int k = job.row_ptr[x] + lane; k < job.row_ptr[x + 1]; k += 32) {
+                            const uint32_t a = __ldg(job.adj + k);
+                            atomicAdd(&h[a >> 8], m * int32_t(int8_t(a & 0xffu)));
+                        }
+                    }
+                } else {
+                    dense_pass<K, P>(planes, plane_stride, nwj, nf, flist, comb, res);
+                    pass_pending = true;
+                }
+            }
+            __syncthreads();
+        }
+        // apply the last pending dense pass
+        if (!SPARSE && pass_pending && decider) {
+            for (int k = 0; k < R; ++k) {
+                const int i = k * kLanes + tid, wi = k * 8 + warp;
+                const bool s_up = (Sw[wi] >> lane) & 1u, dif = (Dw[wi] >> lane) & 1u;
+                if (i < n) h[i] += pass_mult * dense_delta<K, P>(res, nwj, wi, lane, pass_nf, pass_init || dif, s_up);
+            }
+        }
+        __syncthreads();
+        // outputs
+        long long sh = 0, bs = 0;
+        for (int i = tid; i < n; i += T) {
+            const bool up = (Sw[i >> 5] >> (i & 31)) & 1u;
+            const int32_t hv = h[i];
+            sh += up ? hv : -hv;
+            if (bias) bs += up ? bias[i] : -bias[i];
+            if (job.out_h) job.out_h[size_t(c) * n + i] = hv;
+        }
+        for (int w = tid; w < nw; w += T) job.out_spins[size_t(c) * nw + w] = Sw[w] & valid_mask(w, n);
+        sh = warp_sum64(sh);
+        bs = warp_sum64(bs);
+        if (lane == 0) { s_red[0][warp] = sh; s_red[1][warp] = bs; }
+        __syncthreads();
+        if (tid == 0) {
+            long long a = 0, b = 0;
+            for (int w = 0; w < T / 32; ++w) { a += s_red[0][w]; b += s_red[1][w]; }
+            job.out_sum_sh[c] = a;
+            job.out_sum_bs[c] = b;
+            job.out_flips[c] = flips;
+        }
+    }
+}
+
+template <int K, int P, bool SPARSE>
+int launch_t(const PlainLaunch& L, int grid, size_t smem, cudaStream_t st) {
+    auto fn = plain_kernel<K, P, SPARSE>;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return int(e);
+    fn<<<grid, T, smem, st>>>(L);
+    return int(cudaGetLastError());
+}
+
+template <int K, int P, bool SPARSE>
+int occ_t(size_t smem, int* out) {
+    auto fn = plain_kernel<K, P, SPARSE>;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return int(e);
+    return int(cudaOccupancyMaxActiveBlocksPerMultiprocessor(out, fn, T, smem));
+}
+
+}  // namespace
+
+// K: 0 = sparse, 1/2/4 dense planes. P: 12 or 16 counter planes (dense only).
+int plain_launch(const PlainLaunch& L, int K, int P, int grid, size_t smem, cudaStream_t st) {
+    if (K == 0) return launch_t<1, 12, true>(L, grid, smem, st);
+    if (P == 12) {
+        if (K == 1) return launch_t<1, 12, false>(L, grid, smem, st);
+        if (K == 2) return launch_t<2, 12, false>(L, grid, smem, st);
+        if (K == 4) return launch_t<4, 12, false>(L, grid, smem, st);
+    } else if (P == 16) {
+        if (K == 1) return launch_t<1, 16, false>(L, grid, smem, st);
+        if (K == 2) return launch_t<2, 16, false>(L, grid, smem, st);
+        if (K == 4) return launch_t<4, 16, false>(L, grid, smem, st);
+    }
+    return int(cudaErrorInvalidValue);
+}
+
+int plain_max_blocks_per_sm(int K, int P, size_t smem, int* out) {
+    if (K == 0) return occ_t<1, 12, true>(smem, out);
+    if (P == 12) {
+        if (K == 1) return occ_t<1, 12, false>(smem, out);
+        if (K == 2) return occ_t<2, 12, false>(smem, out);
+        if (K == 4) return occ_t<4, 12, false>(smem, out);
+    } else if (P == 16) {
+        if (K == 1) return occ_t<1, 16, false>(smem, out);
+        if (K == 2) return occ_t<2, 16, false>(smem, out);
+        if (K == 4) return occ_t<4, 16, false>(smem, out);
+    }
+    return int(cudaErrorInvalidValue);
+}
+
+}  // namespace anc

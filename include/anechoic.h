@@ -1,0 +1,162 @@
+/* anechoic-b200: C ABI of the B200 SCA (stochastic cellular automata) annealing engines.
+ *
+ * The reference has no library API: its drop-in surface is the CLI pair sca_gpu / sca_gpu_bias, their output files,
+ * and the golden model's header functions. Each entry point below names the reference interface it replaces
+ * (paths relative to the reference project root).
+ *
+ * Conventions
+ *   - Plain C types only; the caller owns every host buffer. Handles own their device memory and free it in destroy.
+ *   - Every function returns an int status (ANC_OK = 0 or a negative ANC_E* code); anc_last_error() returns the
+ *     message of the calling thread's last failure. No C++ exception crosses the ABI.
+ *   - Spin vectors are uint64 words, bit i of word i/64 set iff s_i = +1 (active spins only), anc_spin_words(n)
+ *     words per anneal: the layout of the reference's PREFIX.spins.bin records (32 words for n <= 2048).
+ *   - Calls on one handle must be serialised by the caller. Synchronous calls return after the results are on the
+ *     host. One process drives one GPU (the current CUDA device when the handle is created).
+ */
+#ifndef ANECHOIC_H
+#define ANECHOIC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define ANC_API __attribute__((visibility("default")))
+#else
+#define ANC_API
+#endif
+
+#define ANC_OK 0
+#define ANC_EINVAL (-1)    /* invalid argument, or the int32 range plan refused the tables (reference: FAIL + exit 1) */
+#define ANC_ECUDA (-2)     /* CUDA runtime error */
+#define ANC_ETIMEOUT (-3)  /* a bounded device-side wait gave up (the kernel returned an error status) */
+#define ANC_EMISMATCH (-4) /* internal consistency check failed (reference: cut mismatch, exit 2) */
+
+#define ANC_ENGINE_AUTO 0   /* pick per launch (autotuned crossover) */
+#define ANC_ENGINE_PLAIN 1  /* bit-column engine: one CTA per anneal, bit-packed couplings, flipped columns only */
+#define ANC_ENGINE_TENSOR 2 /* batched engine: replicas sharing J, tcgen05 int8 J * dS update */
+
+typedef struct anc_instance anc_instance;
+typedef struct anc_tables anc_tables;
+
+/* Instance statistics (jmat::finish, gpu/multibit_bias_20261008/src/jmat.hpp:21-40). */
+typedef struct {
+    int n;            /* active spins */
+    int np;           /* padded spins: max(2048, ceil(n/256)*256); 256 RNG lanes x np/256 rounds */
+    int kbits;        /* bits per coupling of the packed planes (1 = +-1 complete graph; 2, 4; 0 = CSR) */
+    int sparse;       /* 1 if couplings are held as CSR rows */
+    int64_t nnz;      /* nonzero couplings (both triangles) */
+    int64_t sumw;     /* sum_{i<j} w_ij, w = -J: cut = (sumw + sum_sh / 2) / 2 */
+    int32_t maxabs;   /* max |J| */
+    int64_t hmax;     /* max_y sum_x |J_xy| */
+    int32_t bmax;     /* max |b| */
+    double mean_row_sq; /* mean_i sum_j J_ij^2 */
+} anc_instance_info;
+
+/* Replaces sca::load_graph / jmat::load + jmat::load_bias (sca_ref.hpp:31-49, jmat.hpp:115-120,164-178) as the way
+ * couplings reach the engine. J_dense: n*n int8 row-major, symmetric, zero diagonal. kbits: 0 = smallest fitting
+ * (1 for a +-1 complete graph, else 2/4), or 1/2/4 explicitly. bias: n int32 (|b| <= 32767) or NULL. */
+ANC_API int anc_instance_create(const int8_t* J_dense, int n, int kbits, const int32_t* bias, anc_instance** out);
+
+/* Sparse couplings as CSR rows: row_ptr[n+1], col[nnz], val[nnz] (every nonzero of row x; each pair in both rows). */
+ANC_API int anc_instance_create_csr(int n, const int32_t* row_ptr, const int32_t* col, const int8_t* val, const int32_t* bias,
+                            anc_instance** out);
+
+ANC_API int anc_instance_get_info(const anc_instance* inst, anc_instance_info* info);
+ANC_API void anc_instance_destroy(anc_instance* inst);
+
+/* Replaces sca::make_tables / v80host::build_tables (sca_ref.hpp:51-68, tables.hpp:24-40): explicit per-step tables.
+ * fourT: Q16.16 of 4T_t (> 0); q: Q16.16; kcorr: Q8.24 of lambda_t / (2 T_{t-1}); kconst: Q16.16. */
+ANC_API int anc_tables_create(const int32_t* fourT, const int32_t* q, const int64_t* kcorr, const int32_t* kconst, int S,
+                      anc_tables** out);
+
+/* Schedule -> tables, bit-identical to v80host::build_tables (scale == 1) and mb::tables (mb_common.hpp:141-154):
+ * T_t = t0 (t1/t0)^(t/(S-1)); lam > 0 counted Onsager (with optional ramp); kappa > 0 temperature-scaled (TEC-T);
+ * jv != 0 TEC; all zero = no correction. */
+ANC_API int anc_tables_from_schedule(int S, double t0, double t1, double q, double lam, double jv, double kappa, int ramp,
+                             double scale, anc_tables** out);
+ANC_API int anc_tables_steps(const anc_tables* tb);
+ANC_API int anc_tables_read(const anc_tables* tb, int32_t* fourT, int32_t* q, int64_t* kcorr, int32_t* kconst);
+ANC_API void anc_tables_destroy(anc_tables* tb);
+
+/* Range plan (host::check_ranges / host::plan_ranges, gpu/onsager_v2_20261007/src/sca_gpu.cu:519-528,
+ * gpu/multibit_bias_20261008/src/sca_gpu_bias.cu:536-557): plain_ok = 1 if s*h*65536 + q -/+ corr fits int32
+ * unclamped; hclamp = clamp bound used otherwise (exact). ANC_EINVAL if even the clamped form overflows. */
+ANC_API int anc_range_plan(const anc_instance* inst, const anc_tables* tb, int* plain_ok, int32_t* hclamp);
+
+/* Host-only forms of the two functions above (no CUDA call; usable without a GPU).
+ * anc_schedule_tables fills caller arrays of S entries exactly as anc_tables_from_schedule would upload them.
+ * anc_plan_ranges takes n, hmax = max_y sum_x |J_xy| and bmax = max |b| (see anc_instance_info). */
+ANC_API int anc_schedule_tables(int S, double t0, double t1, double q, double lam, double jv, double kappa, int ramp,
+                                double scale, int32_t* fourT, int32_t* q_out, int64_t* kcorr, int32_t* kconst);
+ANC_API int anc_plan_ranges(int n, int64_t hmax, int64_t bmax, const int32_t* fourT, const int32_t* q,
+                            const int64_t* kcorr, const int32_t* kconst, int S, int* plain_ok, int32_t* hclamp);
+
+/* Words per spin vector: anc_np(n) / 64. */
+ANC_API int anc_spin_words(int n);
+ANC_API int anc_np(int n);
+
+typedef struct {
+    int engine;      /* ANC_ENGINE_* */
+    int wide;        /* -1 auto (clamp only if the plan needs it), 0 never (EINVAL if needed), 1 always */
+    int threads;     /* host threads for rescoring; 0 = default */
+    int reserved[5];
+} anc_run_opts;
+
+/* Replaces one launch + readback of sca_gpu / sca_gpu_bias (sca_gpu.cu:699-713, sca_gpu_bias.cu:716-733) and
+ * sca::run_trial / run_trial_bias per chain: nchains anneals with trial ids trial_offset + c.
+ * Outputs (host, caller-owned, may be NULL unless noted):
+ *   spins   [nchains][anc_spin_words(n)] (required)
+ *   sum_sh  [nchains]  sum_i s_i h_i over active spins with the biased fields (required)
+ *   sum_bs  [nchains]  sum_i b_i s_i
+ *   flips   [nchains]  total flips
+ *   trace   [nchains][S] n_lin per step (the reference's PREFIX.trace.bin layout)
+ * opts may be NULL (auto engine, auto wide). */
+ANC_API int anc_run(anc_instance* inst, anc_tables* tb, uint64_t seed, uint32_t trial_offset, int nchains,
+            const anc_run_opts* opts, uint64_t* spins, int64_t* sum_sh, int64_t* sum_bs, int64_t* flips,
+            int32_t* trace);
+
+/* As anc_run, also returning the final fields h [nchains][n] (for --check-fields, jmat.hpp:153-161). */
+ANC_API int anc_run_fields(anc_instance* inst, anc_tables* tb, uint64_t seed, uint32_t trial_offset, int nchains,
+                   const anc_run_opts* opts, uint64_t* spins, int64_t* sum_sh, int64_t* sum_bs, int64_t* flips,
+                   int32_t* trace, int32_t* fields);
+
+/* Device-resident variant (no host copies, no synchronisation; graph-capturable once the handle has run once):
+ * outputs are DEVICE pointers laid out as in anc_run; trace may be NULL; stream is a cudaStream_t (NULL = default). */
+ANC_API int anc_run_device(anc_instance* inst, anc_tables* tb, uint64_t seed, uint32_t trial_offset, int nchains,
+                   const anc_run_opts* opts, uint64_t* d_spins, int64_t* d_sum_sh, int64_t* d_sum_bs,
+                   int64_t* d_flips, int32_t* d_trace, void* stream);
+
+/* Many instances / schedules in ONE persistent launch (work queue, uneven sizes). */
+typedef struct {
+    anc_instance* inst;
+    anc_tables* tb;
+    uint64_t seed;
+    uint32_t trial_offset;
+    int nchains;
+    uint64_t* spins;   /* host outputs as in anc_run */
+    int64_t* sum_sh;
+    int64_t* sum_bs;
+    int64_t* flips;
+    int32_t* trace;
+} anc_job;
+
+/* Replaces running sca_gpu_bias once per instance (run_gsel.sh / run_bias.sh loops). */
+ANC_API int anc_run_batch(int njobs, const anc_job* jobs, const anc_run_opts* opts);
+
+/* Last device time of a synchronous run on this thread (ms, CUDA events around the launch). */
+ANC_API double anc_last_device_ms(void);
+
+/* Message of the calling thread's last failure ("" if none). */
+ANC_API const char* anc_last_error(void);
+
+/* Library version string. */
+ANC_API const char* anc_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ANECHOIC_H */
