@@ -258,7 +258,8 @@ int launch_plain_single(anc_instance* I, const anc::PlainJob& job, cudaStream_t 
 int pick_engine(anc_instance* I, anc_tables* tb, int nchains, const anc_run_opts* o) {
     const int e = o ? o->engine : ANC_ENGINE_AUTO;
     if (e == ANC_ENGINE_PLAIN || e == ANC_ENGINE_TENSOR) return e;
-    return anc::tensor_supported(I->n, I->K, nchains) && anc::tensor_prefer(I->n, I->K, nchains, tb->S)
+    return !I->dense.empty() && anc::tensor_supported(I->n, I->K, nchains) &&
+                   anc::tensor_prefer(I->n, I->K, nchains, tb->S)
                ? ANC_ENGINE_TENSOR
                : ANC_ENGINE_PLAIN;
 }
@@ -338,6 +339,13 @@ int run_host_impl(anc_instance* I, anc_tables* tb, uint64_t seed, uint32_t off, 
     if (trace) CK(cudaMemcpyAsync(trace, I->w_trace.p, size_t(nchains) * tb->S * 4, cudaMemcpyDeviceToHost, st));
     if (fields) CK(cudaMemcpyAsync(fields, I->w_h.p, size_t(nchains) * I->n * 4, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    if (I->tensor_ready && I->tensor.last_err) {
+        std::string why;
+        rc = anc::tensor_check_error(&I->tensor, st, &why);
+        I->tensor.last_err = nullptr;
+        if (rc == -3) return fail(ANC_ETIMEOUT, "tensor engine: %s", why.c_str());
+        if (rc) return fail(ANC_ECUDA, "tensor engine: %s", why.c_str());
+    }
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, I->ev0, I->ev1));
     g_dev_ms = ms;

@@ -2,6 +2,7 @@
 #pragma once
 #include <cstdint>
 #include <string>
+#include <vector>
 
 #include "anc_common.cuh"
 
@@ -9,8 +10,13 @@ namespace anc {
 
 struct TensorInstance {
     int n = 0, np = 0;
-    int8_t* d_J = nullptr;       // operand layout built by tensor_build_instance
+    std::vector<int> perm;       // slot i -> permuted index (CTA-contiguous slot slices)
+    int8_t* d_J = nullptr;       // J_perm [np][np] int8 (row = y, contiguous x)
     size_t bytes = 0;
+    void* d_ws = nullptr;        // exchange buffers + error word
+    size_t ws_bytes = 0;
+    int32_t* d_bias_perm = nullptr;
+    int* last_err = nullptr;     // error word of the last launch
 };
 
 struct TensorRun {
@@ -32,6 +38,8 @@ bool tensor_supported(int n, int K, int nchains);
 bool tensor_prefer(int n, int K, int nchains, int S);
 int tensor_build_instance(const int8_t* J, int n, TensorInstance* out, std::string* why);
 int tensor_run(TensorInstance* ti, const TensorRun& r, cudaStream_t st, std::string* why);
+// After the stream has reached the launch: -3 if a bounded device wait expired, 0 otherwise.
+int tensor_check_error(TensorInstance* ti, cudaStream_t st, std::string* why);
 void tensor_free_instance(TensorInstance* ti);
 
 }  // namespace anc

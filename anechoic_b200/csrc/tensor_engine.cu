@@ -1,25 +1,672 @@
-// Batched SCA engine for replicas sharing J. (Interface only in this revision: tensor_supported() is false, so the
-// auto engine always selects the plain engine.)
+// Batched SCA engine for replicas that share J: the field update is a dense int8 contraction on the tcgen05 tensor
+// cores, exact with int32 accumulation in TMEM.
+//
+// Per step of the reference algorithm (sca::run_trial_bias, gpu/multibit_bias_20261008/src/sca_ref_bias.hpp:44-68):
+//   h_y += sum_x D_x J_xy  with  D_x = 2 s'_x for flipped x and 0 otherwise  (D = s0 with factor 1 for h(0) = b + J s0).
+// Layout: a thread-block cluster of C = 16 CTAs runs a group of 128 replicas (one TMEM lane each). Spin slot
+// i = k*256 + l (RNG lane l, round k) is owned by CTA c = l / 16 and held at permuted index
+// p(i) = c*NC + (l % 16)*R + k (NC = NP/16 slots per CTA, R = NP/256 rounds); J is stored permuted the same way
+// (J_perm[p(x)][p(y)] = J_xy), so CTA c's slots are the contiguous column slice [c*NC, (c+1)*NC).
+//   * 16 decision warps: thread (replica r, quarter q) owns RNG lanes 16c + 4q .. 16c + 4q + 3 of replica r, i.e.
+//     4R slots = TMEM columns [4Rq, 4R(q+1)). It reads h with tcgen05.ld, decides exactly as the golden model
+//     (Q16.16 integer threshold from the replica's own xoshiro128** stream, counted / temperature-scaled correction),
+//     and writes its D bytes to a global exchange buffer D[group][parity][r][p]; n_lin partials go to a small buffer.
+//   * barrier.cluster (release / acquire) publishes every CTA's slice of D and n_lin.
+//   * 1 TMA warp streams K-chunks of 128: A = D[group][parity][0..127][chunk] (128 x 128 B) and
+//     B = J_perm[c*NC .. +NC][chunk] (NC x 128 B), 128-byte swizzled, into a 4-stage shared-memory ring
+//     (no multicast anywhere).
+//   * 1 MMA thread issues tcgen05.mma.cta_group::1.kind::i8 (M = 128, N = NC, K = 32) accumulating into h in TMEM,
+//     frees each stage with tcgen05.commit, and signals "h ready" after the last chunk.
+// Every mbarrier wait is bounded by %globaltimer: on expiry the kernel records an error code, skips the remaining
+// work but keeps every cluster barrier, so all CTAs finish; the host reports ANC_ETIMEOUT.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
 #include "anc_tensor.cuh"
 
 namespace anc {
+namespace {
 
-bool tensor_supported(int, int, int) { return false; }
-bool tensor_prefer(int, int, int, int) { return false; }
+constexpr int kC = 16;                  // CTAs per cluster (replica group)
+constexpr int kM = 128;                 // replicas per group (MMA M, TMEM lanes)
+constexpr int kDW = 16;                 // decision warps
+constexpr int kThreads = (kDW + 2) * 32;
+constexpr int kTmaWarp = kDW, kMmaWarp = kDW + 1;
+constexpr int kStages = 4;
+constexpr int kKChunk = 128;            // bytes (= int8 elements) of K per stage
+constexpr uint64_t kWaitNs = 2000000000ull;   // 2 s bound on any single wait
 
-int tensor_build_instance(const int8_t*, int, TensorInstance*, std::string* why) {
-    if (why) *why = "tensor engine not built";
-    return -1;
+// error codes written to the run's error word
+constexpr int kErrFull = 1, kErrEmpty = 2, kErrHready = 3;
+
+struct TensorParams {
+    int n, np, R, nc;                   // active spins, padded, rounds, slots per CTA
+    int S;
+    const int32_t* fourT;
+    const int32_t* q;
+    const int64_t* kcorr;
+    const int32_t* kconst;
+    int32_t hclamp;
+    const int32_t* bias_perm;           // [np] bias at permuted index, or null
+    uint64_t seed;
+    uint32_t trial_offset;
+    int nchains;
+    int8_t* dbuf;                       // [groups][2][128][np]
+    int32_t* nlbuf;                     // [groups][2][16][128]
+    uint32_t* out_spins;                // [nchains][np/32] (zeroed by the host)
+    unsigned long long* out_sum_sh;     // [nchains] (zeroed)
+    unsigned long long* out_sum_bs;     // [nchains] (zeroed)
+    unsigned long long* out_flips;      // [nchains] (zeroed)
+    int32_t* out_trace;                 // [nchains][S] or null
+    int32_t* out_h;                     // [nchains][n] or null
+    int* err;                           // error word (zeroed)
+};
+
+// ------------------------------------------------------------------------------------------------ PTX helpers
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return uint32_t(__cvta_generic_to_shared(p)); }
+
+__device__ __forceinline__ uint64_t globaltimer() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
 }
 
-int tensor_run(TensorInstance*, const TensorRun&, cudaStream_t, std::string* why) {
-    if (why) *why = "tensor engine not built";
-    return -1;
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait on phase `parity`; false (and the error word set) after kWaitNs.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int* err, int code) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = globaltimer();
+    while (true) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (globaltimer() - t0 > kWaitNs) {
+            atomicCAS(err, 0, code);
+            return false;
+        }
+    }
+}
+
+__device__ __forceinline__ bool err_set(const int* err) { return *reinterpret_cast<const volatile int*>(err) != 0; }
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+        ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+
+__device__ __forceinline__ void cluster_sync() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+
+__device__ __forceinline__ uint32_t cluster_id_x() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%clusterid.x;" : "=r"(r));
+    return r;
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// 32 lanes x 16 consecutive 32-bit TMEM columns -> 16 registers per thread
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+        : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&v)[16]) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};"
+        ::"r"(taddr), "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]),
+          "r"(v[8]), "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15])
+        : "memory");
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
+// Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups 1024 B apart (SBO), version 1.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= uint64_t((saddr >> 4) & 0x3FFFu);          // start address
+    d |= uint64_t(1) << 16;                         // leading byte offset (unused for swizzled K-major)
+    d |= uint64_t(1024 >> 4) << 32;                 // stride byte offset
+    d |= uint64_t(1) << 46;                         // descriptor version
+    d |= uint64_t(2) << 61;                         // SWIZZLE_128B
+    return d;
+}
+
+__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\ttcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}"
+        ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc));
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+// ------------------------------------------------------------------------------------------------ the kernel
+template <int R>
+__global__ void __launch_bounds__(kThreads, 1)
+    tensor_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
+                  const __grid_constant__ TensorParams P) {
+    constexpr int NC = 16 * R;            // slots (TMEM columns) per CTA
+    constexpr int COLS = 4 * R;           // columns per decision thread (4 RNG lanes x R rounds)
+    constexpr int NCHUNK = 2 * R;         // K chunks of 128 over NP = 256 R
+    constexpr uint32_t A_BYTES = kM * kKChunk;
+    constexpr uint32_t B_BYTES = NC * kKChunk;
+    constexpr uint32_t STAGE = A_BYTES + B_BYTES;
+    constexpr int TMEM_COLS = NC <= 32 ? 32 : NC <= 64 ? 64 : NC <= 128 ? 128 : 256;
+    constexpr uint32_t IDESC = (2u << 4) | (1u << 7) | (1u << 10) | (uint32_t(NC >> 3) << 17) | (uint32_t(kM >> 4) << 24);
+
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* stages = smem;                                        // kStages x STAGE, 1024-aligned
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kStages * STAGE);
+    // bars: full[kStages], empty[kStages], hready
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kStages + 1);
+    int* nl_s = reinterpret_cast<int*>(tmem_slot + 4);           // [128] n_lin partial of this CTA per replica
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int c = int(cluster_rank());
+    const int g = int(cluster_id_x());                            // replica group
+    const int n = P.n, S = P.S;
+    int* err = P.err;
+
+    const uint32_t bar_full = smem_u32(bars), bar_empty = smem_u32(bars + kStages);
+    const uint32_t bar_h = smem_u32(bars + 2 * kStages);
+
+    if (tid == 0) {
+        for (int s = 0; s < kStages; ++s) {
+            mbar_init(bar_full + 8 * s, 1);
+            mbar_init(bar_empty + 8 * s, 1);
+        }
+        mbar_init(bar_h, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if (tid < kM) nl_s[tid] = 0;
+    if (warp == kMmaWarp) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    // ---------------- decision warps ----------------
+    // replica r = lane quarter (warp % 4) * 32 + lane; column quarter qq = warp / 4
+    const int r = (warp & 3) * 32 + lane;
+    const int qq = warp >> 2;
+    const int chain = g * kM + r;
+    const bool writer = chain < P.nchains;
+    Xoshiro rng[4];
+    uint32_t sw[2] = {0u, 0u}, dw[2] = {0u, 0u};   // spin (1 = +1) and flipped-last-step bits of the COLS slots
+    long long flips = 0;
+    int32_t nlin_prev = 0;
+    const uint32_t taddr = tmem + (uint32_t((warp & 3) * 32) << 16) + uint32_t(qq * COLS);
+    int8_t* drow0 = P.dbuf + (size_t(g) * 2 * kM + r) * P.np + size_t(c) * NC + size_t(qq) * COLS;
+    const size_t dpar_stride = size_t(kM) * P.np;
+
+    // slot of column col (= j*R + k) of this thread: RNG lane l = 16c + 4qq + j, round k, i = k*256 + l
+    auto slot_of = [&](int col) { return (col % R) * 256 + 16 * c + 4 * qq + col / R; };
+
+    if (warp < kDW) {
+        // seeds, initial spins (draw >> 31, padding +1), s_prev = +1 (so "flipped" = [s0 = -1]); h := bias
+        for (int j = 0; j < 4; ++j) rng_seed(rng[j], P.seed, P.trial_offset + uint32_t(chain), uint32_t(16 * c + 4 * qq + j));
+        uint32_t dbytes[COLS / 4];
+#pragma unroll
+        for (int w = 0; w < COLS / 4; ++w) dbytes[w] = 0u;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int k = 0; k < R; ++k) {
+                const int col = j * R + k;
+                const uint32_t rv = rng_next(rng[j]);
+                const int i = k * 256 + 16 * c + 4 * qq + j;
+                const bool valid = i < n;
+                const uint32_t up = valid ? (rv >> 31) : 1u;
+                sw[col >> 5] |= up << (col & 31);
+                if (valid && !up) dw[col >> 5] |= 1u << (col & 31);
+                const uint32_t b = valid ? (up ? 0x01u : 0xFFu) : 0u;
+                dbytes[col >> 2] |= b << (8 * (col & 3));
+            }
+        // D(-1) = s0 into parity 1 (the step index -1 is odd)
+        int8_t* drow = drow0 + dpar_stride;
+#pragma unroll
+        for (int w = 0; w < COLS / 16; ++w)
+            reinterpret_cast<uint4*>(drow)[w] = make_uint4(dbytes[4 * w], dbytes[4 * w + 1], dbytes[4 * w + 2], dbytes[4 * w + 3]);
+        // TMEM h := bias (per column)
+#pragma unroll
+        for (int cb = 0; cb < COLS; cb += 16) {
+            uint32_t v[16];
+#pragma unroll
+            for (int e = 0; e < 16; ++e) {
+                const int col = qq * COLS + cb + e;
+                v[e] = P.bias_perm ? uint32_t(P.bias_perm[c * NC + col]) : 0u;
+            }
+            tmem_st16(taddr + cb, v);
+        }
+        tmem_wait_st();
+        if (qq == 0) P.nlbuf[((size_t(g) * 2 + 1) * kC + c) * kM + r] = 0;
+        asm volatile("fence.proxy.async.global;" ::: "memory");
+        tc_fence_before();
+    }
+
+    // step index m = -1 (initial field), 0 .. S-1; after each: cluster barrier, then the MMA applies D(m)
+    uint32_t stage_it = 0;                     // running stage counter (TMA and MMA threads)
+    for (int m = -1; m < S; ++m) {
+        const int par = m & 1;
+        if (m >= 0 && warp < kDW) {
+            // wait for h (after D(m-1)), read it, decide step m
+            if (!err_set(err)) mbar_wait(bar_h, uint32_t(m & 1), err, kErrHready);
+            tc_fence_after();
+            const int t = m;
+            const int32_t fourT = __ldg(P.fourT + t), twoT = fourT >> 1, qv = __ldg(P.q + t);
+            const int32_t corr = step_corr(nlin_prev, __ldg(P.kcorr + t), __ldg(P.kconst + t));
+            const uint32_t lw = uint32_t(2 * twoT - 1);
+            const int32_t hcl = P.hclamp;
+            uint32_t dbytes[COLS / 4];
+#pragma unroll
+            for (int w = 0; w < COLS / 4; ++w) dbytes[w] = 0u;
+            int nl = 0;
+            uint32_t nsw[2] = {sw[0], sw[1]}, ndw[2] = {0u, 0u};
+#pragma unroll
+            for (int cb = 0; cb < COLS; cb += 16) {
+                uint32_t hv[16];
+                tmem_ld16(taddr + cb, hv);
+                tmem_wait_ld();
+                // draws follow each lane's round order: columns are j*R + k, so 16-column blocks taken in order
+                // visit every lane's rounds in increasing k
+#pragma unroll
+                for (int e = 0; e < 16; ++e) {
+                    const int col = cb + e;
+                    const int j = col / R, k = col % R;
+                    const uint32_t u = rng_next(rng[j]);
+                    const int i = k * 256 + 16 * c + 4 * qq + j;
+                    const bool valid = i < n;
+                    const bool up = (sw[col >> 5] >> (col & 31)) & 1u;
+                    const bool dif = (dw[col >> 5] >> (col & 31)) & 1u;
+                    const int32_t h = int32_t(hv[e]);
+                    int32_t hs = up ? h : -h;
+                    if (hcl > 0) hs = max(-hcl, min(hs, hcl));
+                    const int32_t x = qv + (dif ? corr : -corr);
+                    const int32_t zt = hs * 65536 + x;
+                    const int32_t thr = threshold16(u, fourT);
+                    const bool fl = valid && (zt - thr < 0);
+                    nl += (valid && (uint32_t(zt + twoT - 1) < lw)) ? 1 : 0;
+                    if (fl) {
+                        nsw[col >> 5] ^= 1u << (col & 31);
+                        ndw[col >> 5] |= 1u << (col & 31);
+                        dbytes[col >> 2] |= (up ? 0xFEu : 0x02u) << (8 * (col & 3));   // 2 * s' with s' = -s
+                        ++flips;
+                    }
+                }
+            }
+            sw[0] = nsw[0]; sw[1] = nsw[1];
+            dw[0] = ndw[0]; dw[1] = ndw[1];
+            int8_t* drow = drow0 + size_t(par) * dpar_stride;
+#pragma unroll
+            for (int w = 0; w < COLS / 16; ++w)
+                reinterpret_cast<uint4*>(drow)[w] =
+                    make_uint4(dbytes[4 * w], dbytes[4 * w + 1], dbytes[4 * w + 2], dbytes[4 * w + 3]);
+            atomicAdd(&nl_s[r], nl);
+            tc_fence_before();
+            asm volatile("bar.sync 1, %0;" ::"r"(kDW * 32) : "memory");
+            if (qq == 0) {
+                P.nlbuf[((size_t(g) * 2 + par) * kC + c) * kM + r] = nl_s[r];
+                nl_s[r] = 0;
+            }
+            asm volatile("fence.proxy.async.global;" ::: "memory");
+        }
+        cluster_sync();
+        asm volatile("fence.proxy.async.global;" ::: "memory");
+        if (warp < kDW && m >= 0) {
+            // n_lin of step m for replica r: sum of the 16 CTAs' partials
+            const int32_t* nlp = P.nlbuf + (size_t(g) * 2 + par) * kC * kM + r;
+            int32_t tot = 0;
+#pragma unroll
+            for (int cc = 0; cc < kC; ++cc) tot += __ldcg(nlp + cc * kM);
+            nlin_prev = tot;
+            if (c == 0 && qq == 0 && writer && P.out_trace) P.out_trace[size_t(chain) * S + m] = tot;
+        }
+        if (warp == kTmaWarp) {
+            if (lane == 0) {
+                const int ay = (g * 2 + (par & 1)) * kM;
+                for (int kc = 0; kc < NCHUNK; ++kc, ++stage_it) {
+                    const int s = int(stage_it % kStages);
+                    const uint32_t ph = (stage_it / kStages) & 1u;
+                    if (err_set(err)) continue;   // after a failed wait: issue nothing more
+                    if (stage_it >= kStages && !mbar_wait(bar_empty + 8 * s, ph ^ 1u, err, kErrEmpty)) continue;
+                    const uint32_t dst = smem_u32(stages + size_t(s) * STAGE);
+                    mbar_arrive_expect_tx(bar_full + 8 * s, STAGE);
+                    tma_load_2d(dst, &mapA, kc * kKChunk, ay, bar_full + 8 * s);
+                    tma_load_2d(dst + A_BYTES, &mapB, kc * kKChunk, c * NC, bar_full + 8 * s);
+                }
+            } else {
+                stage_it += NCHUNK;
+            }
+            __syncwarp();
+        } else if (warp == kMmaWarp) {
+            if (lane == 0) {
+                tc_fence_after();
+                for (int kc = 0; kc < NCHUNK; ++kc, ++stage_it) {
+                    const int s = int(stage_it % kStages);
+                    const uint32_t ph = (stage_it / kStages) & 1u;
+                    const bool ok = !err_set(err) && mbar_wait(bar_full + 8 * s, ph, err, kErrFull);
+                    tc_fence_after();
+                    if (ok) {
+                        const uint32_t a0 = smem_u32(stages + size_t(s) * STAGE), b0 = a0 + A_BYTES;
+#pragma unroll
+                        for (int kk = 0; kk < kKChunk / 32; ++kk)
+                            mma_i8(tmem, sw128_desc(a0 + 32 * kk), sw128_desc(b0 + 32 * kk), IDESC, 1u);
+                    }
+                    mma_commit(bar_empty + 8 * s);     // frees the stage once the MMAs above have read it
+                }
+                mma_commit(bar_h);                     // h ready for the next decision
+            } else {
+                stage_it += NCHUNK;
+            }
+            __syncwarp();
+        }
+    }
+
+    // ---------------- final fields and outputs ----------------
+    if (warp < kDW) {
+        if (!err_set(err)) mbar_wait(bar_h, uint32_t(S & 1), err, kErrHready);
+        tc_fence_after();
+        long long sh = 0, bs = 0;
+        const int words = P.np / 32;
+#pragma unroll
+        for (int cb = 0; cb < COLS; cb += 16) {
+            uint32_t hv[16];
+            tmem_ld16(taddr + cb, hv);
+            tmem_wait_ld();
+#pragma unroll
+            for (int e = 0; e < 16; ++e) {
+                const int col = cb + e;
+                const int i = slot_of(col);
+                if (i >= n) continue;
+                const bool up = (sw[col >> 5] >> (col & 31)) & 1u;
+                const int32_t h = int32_t(hv[e]);
+                sh += up ? h : -h;
+                if (P.bias_perm) {
+                    const int32_t b = P.bias_perm[c * NC + qq * COLS + col];
+                    bs += up ? b : -b;
+                }
+                if (writer) {
+                    if (up) atomicOr(P.out_spins + size_t(chain) * words + (i >> 5), 1u << (i & 31));
+                    if (P.out_h) P.out_h[size_t(chain) * n + i] = h;
+                }
+            }
+        }
+        if (writer) {
+            atomicAdd(P.out_sum_sh + chain, static_cast<unsigned long long>(sh));
+            atomicAdd(P.out_sum_bs + chain, static_cast<unsigned long long>(bs));
+            atomicAdd(P.out_flips + chain, static_cast<unsigned long long>(flips));
+        }
+        tc_fence_before();
+    }
+    __syncthreads();
+    cluster_sync();   // no CTA leaves while a peer may still read its D slice through L2 (and keeps TMEM until done)
+    if (warp == kMmaWarp) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+    }
+}
+
+// ------------------------------------------------------------------------------------------------ host side
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    return fn;
+}
+
+// 2-D uint8 tensor [rows][cols] (cols contiguous), box = box_rows x 128 bytes, 128-byte swizzle.
+bool make_map(CUtensorMap* map, void* base, uint64_t cols, uint64_t rows, uint32_t box_rows) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return false;
+    const cuuint64_t dims[2] = {cols, rows};
+    const cuuint64_t strides[1] = {cols};
+    const cuuint32_t box[2] = {uint32_t(kKChunk), box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    return fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+              CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+int rounds_of(int np) { return np / 256; }
+
+template <int R>
+size_t smem_bytes_t() {
+    constexpr size_t NC = 16 * R;
+    return 1024 + kStages * (size_t(kM) * kKChunk + NC * kKChunk) + (2 * kStages + 1) * 8 + 16 + kM * 4;
+}
+
+template <int R>
+int launch_t(const TensorParams& P, int groups, const CUtensorMap& A, const CUtensorMap& B, cudaStream_t st,
+             std::string* why) {
+    auto fn = tensor_kernel<R>;
+    const size_t smem = smem_bytes_t<R>();
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (e != cudaSuccess) {
+        if (why) *why = std::string("kernel attributes: ") + cudaGetErrorString(e);
+        return -2;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = kC;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cfg.gridDim = dim3(kC * groups);
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    e = cudaLaunchKernelEx(&cfg, fn, A, B, P);
+    if (e != cudaSuccess) {
+        if (why) *why = std::string("launch: ") + cudaGetErrorString(e);
+        return -2;
+    }
+    return 0;
+}
+
+}  // namespace
+
+bool tensor_supported(int n, int K, int nchains) {
+    (void)K;
+    const int np = std::max(2048, ((n + 255) / 256) * 256);
+    const int R = np / 256;
+    return nchains >= 1 && (R == 8 || R == 12 || R == 16);
+}
+
+bool tensor_prefer(int n, int K, int nchains, int S) {
+    (void)S;
+    return tensor_supported(n, K, nchains) && nchains >= 256;
+}
+
+int tensor_build_instance(const int8_t* J, int n, TensorInstance* out, std::string* why) {
+    const int np = std::max(2048, ((n + 255) / 256) * 256);
+    const int R = np / 256, nc = 16 * R;
+    if (!(R == 8 || R == 12 || R == 16)) {
+        if (why) *why = "tensor engine supports NP in {2048, 3072, 4096}";
+        return -1;
+    }
+    std::vector<int> p(np);
+    for (int i = 0; i < np; ++i) {
+        const int l = i % 256, k = i / 256, cc = l / 16, jl = l % 16;
+        p[i] = cc * nc + jl * R + k;
+    }
+    std::vector<int8_t> Jp(size_t(np) * np, 0);
+    for (int x = 0; x < n; ++x)
+        for (int y = 0; y < n; ++y) Jp[size_t(p[y]) * np + p[x]] = J[size_t(x) * n + y];   // row = y (N), col = x (K)
+    out->n = n;
+    out->np = np;
+    out->perm.assign(p.begin(), p.end());
+    cudaError_t e = cudaMalloc(&out->d_J, Jp.size());
+    if (e == cudaSuccess) e = cudaMemcpy(out->d_J, Jp.data(), Jp.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        if (why) *why = std::string("upload J: ") + cudaGetErrorString(e);
+        return -2;
+    }
+    out->bytes = Jp.size();
+    return 0;
+}
+
+int tensor_run(TensorInstance* ti, const TensorRun& r, cudaStream_t st, std::string* why) {
+    const int np = ti->np, R = np / 256;
+    const int groups = (r.nchains + kM - 1) / kM;
+    // workspace: exchange buffers, permuted bias, error word
+    const size_t dbytes = size_t(groups) * 2 * kM * np;
+    const size_t nlbytes = size_t(groups) * 2 * kC * kM * 4;
+    cudaError_t e = cudaSuccess;
+    if (ti->ws_bytes < dbytes + nlbytes + 256) {
+        if (ti->d_ws) cudaFree(ti->d_ws);
+        ti->d_ws = nullptr;
+        ti->ws_bytes = 0;
+        e = cudaMalloc(&ti->d_ws, dbytes + nlbytes + 256);
+        if (e != cudaSuccess) {
+            if (why) *why = std::string("workspace: ") + cudaGetErrorString(e);
+            return -2;
+        }
+        ti->ws_bytes = dbytes + nlbytes + 256;
+    }
+    int8_t* dbuf = static_cast<int8_t*>(ti->d_ws);
+    int32_t* nlbuf = reinterpret_cast<int32_t*>(static_cast<uint8_t*>(ti->d_ws) + dbytes);
+    int* err = reinterpret_cast<int*>(static_cast<uint8_t*>(ti->d_ws) + dbytes + nlbytes);
+    if (r.bias && !ti->d_bias_perm) {
+        // permuted bias (host copy of the caller's device bias)
+        std::vector<int32_t> b(ti->n), bp(np, 0);
+        e = cudaMemcpy(b.data(), r.bias, size_t(ti->n) * 4, cudaMemcpyDeviceToHost);
+        for (int i = 0; i < ti->n && e == cudaSuccess; ++i) bp[ti->perm[i]] = b[i];
+        if (e == cudaSuccess) e = cudaMalloc(&ti->d_bias_perm, size_t(np) * 4);
+        if (e == cudaSuccess) e = cudaMemcpy(ti->d_bias_perm, bp.data(), size_t(np) * 4, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            if (why) *why = std::string("bias: ") + cudaGetErrorString(e);
+            return -2;
+        }
+    }
+    CUtensorMap mapA, mapB;
+    if (!make_map(&mapA, dbuf, uint64_t(np), uint64_t(groups) * 2 * kM, kM) ||
+        !make_map(&mapB, ti->d_J, uint64_t(np), uint64_t(np), uint32_t(16 * R))) {
+        if (why) *why = "cuTensorMapEncodeTiled failed";
+        return -2;
+    }
+    const int words = np / 32;
+    e = cudaMemsetAsync(r.out_spins, 0, size_t(r.nchains) * words * 4, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(r.out_sum_sh, 0, size_t(r.nchains) * 8, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(r.out_sum_bs, 0, size_t(r.nchains) * 8, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(r.out_flips, 0, size_t(r.nchains) * 8, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(err, 0, 4, st);
+    if (e != cudaSuccess) {
+        if (why) *why = std::string("memset: ") + cudaGetErrorString(e);
+        return -2;
+    }
+    TensorParams P{};
+    P.n = ti->n;
+    P.np = np;
+    P.R = R;
+    P.nc = 16 * R;
+    P.S = r.tab.S;
+    P.fourT = r.tab.fourT;
+    P.q = r.tab.q;
+    P.kcorr = r.tab.kcorr;
+    P.kconst = r.tab.kconst;
+    P.hclamp = r.hclamp;
+    P.bias_perm = r.bias ? ti->d_bias_perm : nullptr;
+    P.seed = r.seed;
+    P.trial_offset = r.trial_offset;
+    P.nchains = r.nchains;
+    P.dbuf = dbuf;
+    P.nlbuf = nlbuf;
+    P.out_spins = r.out_spins;
+    P.out_sum_sh = reinterpret_cast<unsigned long long*>(r.out_sum_sh);
+    P.out_sum_bs = reinterpret_cast<unsigned long long*>(r.out_sum_bs);
+    P.out_flips = reinterpret_cast<unsigned long long*>(r.out_flips);
+    P.out_trace = r.out_trace;
+    P.out_h = r.out_h;
+    P.err = err;
+    int rc = -1;
+    if (R == 8) rc = launch_t<8>(P, groups, mapA, mapB, st, why);
+    else if (R == 12) rc = launch_t<12>(P, groups, mapA, mapB, st, why);
+    else if (R == 16) rc = launch_t<16>(P, groups, mapA, mapB, st, why);
+    if (rc) return rc;
+    ti->last_err = err;
+    return 0;
+}
+
+int tensor_check_error(TensorInstance* ti, cudaStream_t st, std::string* why) {
+    if (!ti->last_err) return 0;
+    int h = 0;
+    cudaError_t e = cudaMemcpyAsync(&h, ti->last_err, 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        if (why) *why = std::string("error word: ") + cudaGetErrorString(e);
+        return -2;
+    }
+    if (h) {
+        if (why) *why = "a bounded device wait expired (code " + std::to_string(h) + ")";
+        return -3;
+    }
+    return 0;
 }
 
 void tensor_free_instance(TensorInstance* ti) {
-    if (ti && ti->d_J) cudaFree(ti->d_J);
-    if (ti) ti->d_J = nullptr;
+    if (!ti) return;
+    if (ti->d_J) cudaFree(ti->d_J);
+    if (ti->d_ws) cudaFree(ti->d_ws);
+    if (ti->d_bias_perm) cudaFree(ti->d_bias_perm);
+    ti->d_J = nullptr;
+    ti->d_ws = nullptr;
+    ti->d_bias_perm = nullptr;
+    ti->ws_bytes = 0;
 }
 
 }  // namespace anc
