@@ -19,7 +19,7 @@ EXPORTS = ("anc_instance_create", "anc_instance_create_csr", "anc_instance_get_i
            "anc_tables_create", "anc_tables_from_schedule", "anc_tables_steps", "anc_tables_read", "anc_tables_destroy",
            "anc_range_plan", "anc_schedule_tables", "anc_plan_ranges", "anc_spin_words", "anc_np", "anc_run",
            "anc_run_fields", "anc_run_device",
-           "anc_run_batch", "anc_last_device_ms", "anc_last_error", "anc_version")
+           "anc_run_batch", "anc_last_device_ms", "anc_last_error", "anc_last_profile", "anc_version")
 
 
 class AncError(RuntimeError):
@@ -37,7 +37,8 @@ class InstanceInfo(C.Structure):
 
 
 class RunOpts(C.Structure):
-    _fields_ = [("engine", C.c_int), ("wide", C.c_int), ("threads", C.c_int), ("reserved", C.c_int * 5)]
+    _fields_ = [("engine", C.c_int), ("wide", C.c_int), ("threads", C.c_int), ("profile", C.c_int),
+                ("reserved", C.c_int * 4)]
 
 
 class Job(C.Structure):
@@ -86,6 +87,7 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         L.anc_last_device_ms.restype = C.c_double
         L.anc_last_error.argtypes = []
         L.anc_last_error.restype = C.c_char_p
+        L.anc_last_profile.argtypes = [C.POINTER(C.c_double), C.c_int]
         L.anc_version.argtypes = []
         L.anc_version.restype = C.c_char_p
         _lib = L
@@ -98,9 +100,21 @@ def check(rc: int):
         raise AncError(rc, msg)
 
 
-def opts(engine: str = "auto", wide="auto") -> RunOpts:
+def opts(engine: str = "auto", wide="auto", profile: bool = False) -> RunOpts:
     o = RunOpts()
     o.engine = ENGINES[engine]
     o.wide = {"auto": -1, 0: 0, 1: 1, False: 0, True: 1, "0": 0, "1": 1}[wide]
     o.threads = 0
+    o.profile = int(bool(profile))
     return o
+
+
+PROFILE_FIELDS = ("wait_fields", "decide", "nlin_publish", "cluster_barrier", "nlin_read", "mma_wait_tma",
+                  "mma_phase", "tma_wait_stage", "step", "ctas", "cluster", "max_active_clusters")
+
+
+def last_profile() -> dict:
+    """Phase profile (SM cycles per step) of this thread's last profiled tensor-engine run."""
+    buf = (C.c_double * 12)()
+    k = load().anc_last_profile(buf, 12)
+    return {PROFILE_FIELDS[i]: buf[i] for i in range(k)}

@@ -19,6 +19,7 @@ namespace {
 
 thread_local std::string g_err;
 thread_local double g_dev_ms = 0.0;
+thread_local std::vector<double> g_prof;
 
 int fail(int code, const char* fmt, ...) {
     char buf[512];
@@ -74,6 +75,8 @@ struct anc_instance {
     DevBuf<uint32_t> w_spins;
     DevBuf<long long> w_sh, w_bs, w_fl;
     DevBuf<int32_t> w_trace, w_h;
+    DevBuf<long long> w_prof;                     // tensor-engine phase counters (opt-in)
+    int prof_ctas = 0, prof_S = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     int device = 0, sms = 0;
@@ -302,6 +305,18 @@ int run_device_impl(anc_instance* I, anc_tables* tb, uint64_t seed, uint32_t off
         r.out_flips = reinterpret_cast<int64_t*>(out.fl);
         r.out_trace = out.trace;
         r.out_h = out.h;
+        r.prof = nullptr;
+        I->prof_ctas = 0;
+        if (o && o->profile) {
+            anc::TensorGeometry geo;
+            if (anc::tensor_geometry(I->n, nchains, &geo) != 0) return fail(ANC_ECUDA, "tensor geometry query failed");
+            const int ctas = std::max(geo.ctas, 16 * ((nchains + 127) / 128));
+            CK(I->w_prof.ensure(size_t(ctas) * 16));
+            CK(cudaMemsetAsync(I->w_prof.p, 0, size_t(ctas) * 16 * sizeof(long long), st));
+            r.prof = I->w_prof.p;
+            I->prof_ctas = ctas;
+            I->prof_S = tb->S;
+        }
         std::string why;
         rc = anc::tensor_run(&I->tensor, r, st, &why);
         if (rc == -3) return fail(ANC_ETIMEOUT, "tensor engine: %s", why.c_str());
@@ -346,6 +361,22 @@ int run_host_impl(anc_instance* I, anc_tables* tb, uint64_t seed, uint32_t off, 
         if (rc == -3) return fail(ANC_ETIMEOUT, "tensor engine: %s", why.c_str());
         if (rc) return fail(ANC_ECUDA, "tensor engine: %s", why.c_str());
     }
+    if (I->prof_ctas > 0) {
+        std::vector<long long> h(size_t(I->prof_ctas) * 16);
+        CK(cudaMemcpy(h.data(), I->w_prof.p, h.size() * sizeof(long long), cudaMemcpyDeviceToHost));
+        g_prof.assign(12, 0.0);
+        for (int s = 0; s < 9; ++s) {
+            double acc = 0;
+            for (int b = 0; b < I->prof_ctas; ++b) acc += double(h[size_t(b) * 16 + s]);
+            g_prof[s] = acc / I->prof_ctas / std::max(1, I->prof_S);
+        }
+        anc::TensorGeometry geo;
+        anc::tensor_geometry(I->n, nchains, &geo);
+        g_prof[9] = geo.ctas;
+        g_prof[10] = geo.cluster;
+        g_prof[11] = geo.max_active_clusters;
+        I->prof_ctas = 0;
+    }
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, I->ev0, I->ev1));
     g_dev_ms = ms;
@@ -357,6 +388,12 @@ int run_host_impl(anc_instance* I, anc_tables* tb, uint64_t seed, uint32_t off, 
 extern "C" {
 
 const char* anc_last_error(void) { return g_err.c_str(); }
+
+int anc_last_profile(double* out, int max) {
+    const int k = std::min<int>(max, int(g_prof.size()));
+    for (int i = 0; i < k; ++i) out[i] = g_prof[i];
+    return k;
+}
 const char* anc_version(void) { return "anechoic-b200 0.1 (sm_100a)"; }
 double anc_last_device_ms(void) { return g_dev_ms; }
 int anc_np(int n) { return pad_np(n); }

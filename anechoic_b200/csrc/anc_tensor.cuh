@@ -32,7 +32,14 @@ struct TensorRun {
     int64_t* out_flips;
     int32_t* out_trace;
     int32_t* out_h;
+    long long* prof;          // device [grid][16] phase cycle totals, or null (profiling off)
 };
+
+// Launch geometry of a run: CTAs in the grid, CTAs per cluster, and how many clusters can be co-resident.
+struct TensorGeometry {
+    int ctas = 0, cluster = 0, max_active_clusters = 0;
+};
+int tensor_geometry(int n, int nchains, TensorGeometry* g);
 
 bool tensor_supported(int n, int K, int nchains);
 bool tensor_prefer(int n, int K, int nchains, int S);

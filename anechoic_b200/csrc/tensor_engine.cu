@@ -65,7 +65,14 @@ struct TensorParams {
     int32_t* out_trace;                 // [nchains][S] or null
     int32_t* out_h;                     // [nchains][n] or null
     int* err;                           // error word (zeroed)
+    long long* prof;                    // [gridDim.x][kProfSlots] clock64 phase totals, or null (off)
 };
+
+// opt-in phase profile (clock64 cycles summed over the steps, per CTA):
+//   0 decision warps waiting for h   1 TMEM load + decide + D store   2 named barrier + n_lin publish
+//   3 cluster barrier (decision warps)   4 n_lin read   5 MMA thread waiting for TMA stages
+//   6 MMA thread: barrier end -> last commit issued   7 TMA thread waiting for free stages   8 whole step loop
+constexpr int kProfSlots = 16;
 
 // ------------------------------------------------------------------------------------------------ PTX helpers
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return uint32_t(__cvta_generic_to_shared(p)); }
@@ -94,17 +101,38 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Bounded wait on phase `parity`; false (and the error word set) after kWaitNs.
+// Bounded wait on phase `parity`; false (and the error word set) after kWaitNs. The timer is read only every 256
+// polls: a %globaltimer read costs hundreds of cycles and would otherwise delay the wake-up.
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int* err, int code) {
     if (mbar_try_wait(bar, parity)) return true;
     const uint64_t t0 = globaltimer();
-    while (true) {
+    for (uint32_t k = 1;; ++k) {
         if (mbar_try_wait(bar, parity)) return true;
-        if (globaltimer() - t0 > kWaitNs) {
+        if ((k & 255u) == 0 && globaltimer() - t0 > kWaitNs) {
             atomicCAS(err, 0, code);
             return false;
         }
     }
+}
+
+// Bounded wait until the 32-bit flag at `p` (global, written with release semantics) reaches `target`.
+__device__ __forceinline__ bool flag_wait(const uint32_t* p, uint32_t target, int* err, int code) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    if (v >= target) return true;
+    const uint64_t t0 = globaltimer();
+    for (uint32_t k = 1;; ++k) {
+        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+        if (v >= target) return true;
+        if ((k & 255u) == 0 && globaltimer() - t0 > kWaitNs) {
+            atomicCAS(err, 0, code);
+            return false;
+        }
+    }
+}
+
+__device__ __forceinline__ void flag_publish(uint32_t* p, uint32_t v) {
+    asm volatile("fence.acq_rel.gpu;\n\tst.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
 __device__ __forceinline__ bool err_set(const int* err) { return *reinterpret_cast<const volatile int*>(err) != 0; }
@@ -289,12 +317,25 @@ __global__ void __launch_bounds__(kThreads, 1)
 
     // step index m = -1 (initial field), 0 .. S-1; after each: cluster barrier, then the MMA applies D(m)
     uint32_t stage_it = 0;                     // running stage counter (TMA and MMA threads)
+    const bool prof = P.prof != nullptr;
+    long long pr[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    long long tq = clock64();
+    const long long t_loop0 = tq;
+    auto mark = [&](int slot) {
+        if (prof) {
+            const long long now = clock64();
+            pr[slot] += now - tq;
+            tq = now;
+        }
+    };
     for (int m = -1; m < S; ++m) {
         const int par = m & 1;
         if (m >= 0 && warp < kDW) {
             // wait for h (after D(m-1)), read it, decide step m
+            if (prof) tq = clock64();
             if (!err_set(err)) mbar_wait(bar_h, uint32_t(m & 1), err, kErrHready);
             tc_fence_after();
+            mark(0);
             const int t = m;
             const int32_t fourT = __ldg(P.fourT + t), twoT = fourT >> 1, qv = __ldg(P.q + t);
             const int32_t corr = step_corr(nlin_prev, __ldg(P.kcorr + t), __ldg(P.kconst + t));
@@ -344,6 +385,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             for (int w = 0; w < COLS / 16; ++w)
                 reinterpret_cast<uint4*>(drow)[w] =
                     make_uint4(dbytes[4 * w], dbytes[4 * w + 1], dbytes[4 * w + 2], dbytes[4 * w + 3]);
+            mark(1);
             atomicAdd(&nl_s[r], nl);
             tc_fence_before();
             asm volatile("bar.sync 1, %0;" ::"r"(kDW * 32) : "memory");
@@ -352,9 +394,13 @@ __global__ void __launch_bounds__(kThreads, 1)
                 nl_s[r] = 0;
             }
             asm volatile("fence.proxy.async.global;" ::: "memory");
+            mark(2);
         }
+        if (prof) tq = clock64();
         cluster_sync();
         asm volatile("fence.proxy.async.global;" ::: "memory");
+        if (warp < kDW) mark(3);
+        else if (prof) tq = clock64();
         if (warp < kDW && m >= 0) {
             // n_lin of step m for replica r: sum of the 16 CTAs' partials
             const int32_t* nlp = P.nlbuf + (size_t(g) * 2 + par) * kC * kM + r;
@@ -363,6 +409,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             for (int cc = 0; cc < kC; ++cc) tot += __ldcg(nlp + cc * kM);
             nlin_prev = tot;
             if (c == 0 && qq == 0 && writer && P.out_trace) P.out_trace[size_t(chain) * S + m] = tot;
+            mark(4);
         }
         if (warp == kTmaWarp) {
             if (lane == 0) {
@@ -371,7 +418,9 @@ __global__ void __launch_bounds__(kThreads, 1)
                     const int s = int(stage_it % kStages);
                     const uint32_t ph = (stage_it / kStages) & 1u;
                     if (err_set(err)) continue;   // after a failed wait: issue nothing more
+                    const long long w0 = prof ? clock64() : 0;
                     if (stage_it >= kStages && !mbar_wait(bar_empty + 8 * s, ph ^ 1u, err, kErrEmpty)) continue;
+                    if (prof) pr[7] += clock64() - w0;
                     const uint32_t dst = smem_u32(stages + size_t(s) * STAGE);
                     mbar_arrive_expect_tx(bar_full + 8 * s, STAGE);
                     tma_load_2d(dst, &mapA, kc * kKChunk, ay, bar_full + 8 * s);
@@ -387,7 +436,9 @@ __global__ void __launch_bounds__(kThreads, 1)
                 for (int kc = 0; kc < NCHUNK; ++kc, ++stage_it) {
                     const int s = int(stage_it % kStages);
                     const uint32_t ph = (stage_it / kStages) & 1u;
+                    const long long w0 = prof ? clock64() : 0;
                     const bool ok = !err_set(err) && mbar_wait(bar_full + 8 * s, ph, err, kErrFull);
+                    if (prof) pr[5] += clock64() - w0;
                     tc_fence_after();
                     if (ok) {
                         const uint32_t a0 = smem_u32(stages + size_t(s) * STAGE), b0 = a0 + A_BYTES;
@@ -398,11 +449,20 @@ __global__ void __launch_bounds__(kThreads, 1)
                     mma_commit(bar_empty + 8 * s);     // frees the stage once the MMAs above have read it
                 }
                 mma_commit(bar_h);                     // h ready for the next decision
+                mark(6);
             } else {
                 stage_it += NCHUNK;
             }
             __syncwarp();
         }
+    }
+    if (prof) {
+        pr[8] = clock64() - t_loop0;
+        long long* dst = P.prof + size_t(blockIdx.x) * kProfSlots;
+        if (warp == 0 && lane == 0)
+            for (int s = 0; s < 5; ++s) dst[s] = pr[s];
+        if (warp == kMmaWarp && lane == 0) { dst[5] = pr[5]; dst[6] = pr[6]; dst[8] = pr[8]; }
+        if (warp == kTmaWarp && lane == 0) dst[7] = pr[7];
     }
 
     // ---------------- final fields and outputs ----------------
@@ -446,6 +506,370 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (warp == kMmaWarp) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+    }
+}
+
+// ------------------------------------------------------------------------------------------------ resident-J kernel
+// For NP = 2048 (n <= 2048): a cooperative persistent grid of 32 y-slices x P group-pairs. CTA (pair slot gp,
+// slice cs) owns spin slots with RNG lanes 8cs .. 8cs+7 (64 columns at permuted indices p = 8l + k) and keeps its
+// J column slice (2048 x 64 int8 = 128 KB, 128-byte swizzled) resident in shared memory for the whole launch.
+// It runs TWO replica groups of 128 (a pair) and alternates between them, so the decisions of one group overlap
+// the tensor-core update of the other:
+//   decision warps (16): for group g: wait "h ready", tcgen05.ld 16 field columns + the n_lin accumulator, decide,
+//     write D(m) (16 bytes) and the thread's n_lin partial (1 byte) to the exchange buffers, then one thread
+//     publishes flag[g][cs] = m + 2 (st.release.gpu).
+//   producer warps (4): for every K chunk (128 x-values = two source slices) wait for both slices' flags
+//     (ld.acquire.gpu), then TMA the 128 x 128-byte D tile into the stage ring; a 17th chunk carries the 128
+//     n_lin partials of all slices. Each warp issues every fourth chunk: one thread's bulk copies are serviced one
+//     at a time, so four issuers keep four copies in flight.
+//   MMA thread: per chunk 4 x tcgen05.mma.kind::i8 (M 128, N 64, K 32) into the group's field accumulator with B
+//     = the resident J chunk; the n_lin chunk is multiplied by a ones row (N 16) into a per-group accumulator,
+//     so sum_slices n_lin partials comes out of the tensor core with the fields.
+// No cluster barrier exists: the flags make the exchange a dataflow, chunks are consumed as slices finish.
+constexpr int kResSlices = 32;            // y-slices for NP = 2048
+constexpr int kResYS = 64;                // columns per slice (MMA N)
+constexpr int kResPW = 4;                 // producer warps
+constexpr int kResStages = 5;
+constexpr int kResMmaWarp = kDW + kResPW;
+constexpr int kResThreads = (kDW + kResPW + 1) * 32;
+constexpr int kResChunks = 17;            // 16 D chunks + 1 n_lin chunk per (step, group)
+constexpr int kErrFlag = 4, kErrJ = 5;
+
+struct ResParams {
+    int n, S, npairs;
+    const int32_t* fourT;
+    const int32_t* q;
+    const int64_t* kcorr;
+    const int32_t* kconst;
+    int32_t hclamp;
+    const int32_t* bias_perm;           // [2048] or null
+    uint64_t seed;
+    uint32_t trial_offset;
+    int nchains;
+    uint32_t* flags;                    // [2 * npairs][32] (zeroed)
+    int8_t* dbuf;                       // [2 * npairs][2][128][2048]
+    int8_t* nlx;                        // [2 * npairs][2][128][128]
+    uint32_t* out_spins;                // [nchains][64] (zeroed)
+    unsigned long long* out_sum_sh;
+    unsigned long long* out_sum_bs;
+    unsigned long long* out_flips;
+    int32_t* out_trace;
+    int32_t* out_h;
+    int* err;
+    long long* prof;
+};
+
+__global__ void __launch_bounds__(kResThreads, 1)
+    tensor_res_kernel(const __grid_constant__ CUtensorMap mapD, const __grid_constant__ CUtensorMap mapNL,
+                      const __grid_constant__ CUtensorMap mapJ, const __grid_constant__ ResParams P) {
+    constexpr int R = 8, NPAD = 2048;
+    constexpr uint32_t TILE = kM * kKChunk;                 // 16 KB D / n_lin tile
+    constexpr uint32_t JCHUNK = kResYS * kKChunk;           // 8 KB of resident J per K chunk
+    constexpr uint32_t IDESC_H = (2u << 4) | (1u << 7) | (1u << 10) | (uint32_t(kResYS >> 3) << 17) | (uint32_t(kM >> 4) << 24);
+    constexpr uint32_t IDESC_NL = (2u << 4) | (1u << 7) | (1u << 10) | (uint32_t(16 >> 3) << 17) | (uint32_t(kM >> 4) << 24);
+
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* jres = smem;                                   // 16 x 8 KB
+    uint8_t* ones = smem + 16 * JCHUNK;                     // 2 KB: row 0 = 128 x int8(1), rows 1..15 = 0
+    uint8_t* stages = ones + 2048;                          // kResStages x 16 KB (1024-aligned)
+    uint64_t* bars = reinterpret_cast<uint64_t*>(stages + kResStages * TILE);
+    // bars: full[5], empty[5], hready[2], jbar
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kResStages + 3);
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int cs = int(blockIdx.x % kResSlices);
+    const int gp0 = int(blockIdx.x / kResSlices), gstride = int(gridDim.x / kResSlices);
+    const int n = P.n, S = P.S;
+    int* err = P.err;
+    const uint32_t bar_full = smem_u32(bars), bar_empty = smem_u32(bars + kResStages);
+    const uint32_t bar_h0 = smem_u32(bars + 2 * kResStages), bar_j = smem_u32(bars + 2 * kResStages + 2);
+
+    if (tid == 0) {
+        for (int s = 0; s < kResStages; ++s) {
+            mbar_init(bar_full + 8 * s, 1);
+            mbar_init(bar_empty + 8 * s, 1);
+        }
+        mbar_init(bar_h0, 1);
+        mbar_init(bar_h0 + 8, 1);
+        mbar_init(bar_j, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    for (int i = tid; i < 2048; i += blockDim.x) ones[i] = i < 128 ? 1 : 0;
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (warp == kResMmaWarp) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(256)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    // resident J slice: rows cs*64 .. +64 of J_perm, 16 chunks of 128 columns
+    if (warp == kDW && lane == 0) {
+        mbar_arrive_expect_tx(bar_j, 16 * JCHUNK);
+        for (int kc = 0; kc < 16; ++kc) tma_load_2d(smem_u32(jres + kc * JCHUNK), &mapJ, kc * kKChunk, cs * kResYS, bar_j);
+    }
+
+    // decision-thread geometry: replica r (TMEM lane), column quarter qq: RNG lanes 8cs + 2qq + j, columns qq*16 ..
+    const int r = (warp & 3) * 32 + lane, qq = warp >> 2;
+    const uint32_t tl = uint32_t((warp & 3) * 32) << 16;
+    uint32_t hph[2] = {0u, 0u};            // decision side: completed "h ready" phases per group
+    uint32_t q = 0;                        // running chunk index (producers, MMA)
+    bool jready = false;
+    const bool prof = P.prof != nullptr;
+    long long pr[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    const long long t_loop0 = clock64();
+
+    for (int pw = gp0; pw < P.npairs; pw += gstride) {
+        const int G[2] = {2 * pw, 2 * pw + 1};
+        if (warp < kDW) {
+            // ---------------- decision warps ----------------
+            Xoshiro rng[2][2];
+            uint32_t sw[2], dw[2], nlacc_prev[2] = {0u, 0u};
+            int32_t nlin_prev[2] = {0, 0};
+            long long flips[2] = {0, 0};
+            const int chain[2] = {G[0] * kM + r, G[1] * kM + r};
+#pragma unroll
+            for (int g = 0; g < 2; ++g) {
+                sw[g] = 0u;
+                dw[g] = 0u;
+                uint32_t db[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    rng_seed(rng[g][j], P.seed, P.trial_offset + uint32_t(chain[g]), uint32_t(8 * cs + 2 * qq + j));
+#pragma unroll
+                    for (int k = 0; k < R; ++k) {
+                        const int col = j * R + k, i = k * 256 + 8 * cs + 2 * qq + j;
+                        const uint32_t rv = rng_next(rng[g][j]);
+                        const bool valid = i < n;
+                        const uint32_t up = valid ? (rv >> 31) : 1u;
+                        sw[g] |= up << col;
+                        if (valid && !up) dw[g] |= 1u << col;
+                        db[col >> 2] |= (valid ? (up ? 0x01u : 0xFFu) : 0u) << (8 * (col & 3));
+                    }
+                }
+                int8_t* drow = P.dbuf + ((size_t(G[g]) * 2 + 1) * kM + r) * NPAD + cs * kResYS + qq * 16;
+                *reinterpret_cast<uint4*>(drow) = make_uint4(db[0], db[1], db[2], db[3]);
+                P.nlx[((size_t(G[g]) * 2 + 1) * kM + r) * 128 + cs * 4 + qq] = 0;
+                // fields := bias, n_lin accumulator := 0
+                uint32_t v[16];
+#pragma unroll
+                for (int e = 0; e < 16; ++e)
+                    v[e] = P.bias_perm ? uint32_t(P.bias_perm[cs * kResYS + qq * 16 + e]) : 0u;
+                tmem_st16(tmem + tl + uint32_t(g * kResYS + qq * 16), v);
+                if (qq == 0) {
+#pragma unroll
+                    for (int e = 0; e < 16; ++e) v[e] = 0u;
+                    tmem_st16(tmem + tl + uint32_t(128 + g * 16), v);
+                }
+            }
+            tmem_wait_st();
+            asm volatile("fence.proxy.async.global;" ::: "memory");
+            tc_fence_before();
+            asm volatile("bar.sync 1, %0;" ::"r"(kDW * 32) : "memory");
+            if (tid == 0) {
+                flag_publish(P.flags + G[0] * kResSlices + cs, 1u);
+                flag_publish(P.flags + G[1] * kResSlices + cs, 1u);
+            }
+            for (int m = 0; m <= S; ++m) {
+#pragma unroll
+                for (int g = 0; g < 2; ++g) {
+                    long long t0 = prof ? clock64() : 0;
+                    if (!err_set(err)) mbar_wait(bar_h0 + 8 * g, hph[g] & 1u, err, kErrHready);
+                    ++hph[g];
+                    tc_fence_after();
+                    if (prof) { const long long t1 = clock64(); pr[0] += t1 - t0; t0 = t1; }
+                    uint32_t hv[16], nv;
+                    tmem_ld16(tmem + tl + uint32_t(g * kResYS + qq * 16), hv);
+                    asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];"
+                                 : "=r"(nv)
+                                 : "r"(tmem + tl + uint32_t(128 + g * 16)));
+                    tmem_wait_ld();
+                    const int32_t nlin = int32_t(nv - nlacc_prev[g]);   // n_lin of step m - 1 (0 before step 0)
+                    nlacc_prev[g] = nv;
+                    const bool writer = chain[g] < P.nchains;
+                    if (m >= 1 && writer && cs == 0 && qq == 0 && P.out_trace) P.out_trace[size_t(chain[g]) * S + (m - 1)] = nlin;
+                    nlin_prev[g] = nlin;
+                    if (m == S) {
+                        // final fields: outputs
+                        long long sh = 0, bs = 0;
+#pragma unroll
+                        for (int e = 0; e < 16; ++e) {
+                            const int j = e / R, k = e % R, i = k * 256 + 8 * cs + 2 * qq + j;
+                            if (i >= n) continue;
+                            const bool up = (sw[g] >> e) & 1u;
+                            const int32_t h = int32_t(hv[e]);
+                            sh += up ? h : -h;
+                            if (P.bias_perm) {
+                                const int32_t b = P.bias_perm[cs * kResYS + qq * 16 + e];
+                                bs += up ? b : -b;
+                            }
+                            if (writer) {
+                                if (up) atomicOr(P.out_spins + size_t(chain[g]) * 64 + (i >> 5), 1u << (i & 31));
+                                if (P.out_h) P.out_h[size_t(chain[g]) * n + i] = h;
+                            }
+                        }
+                        if (writer) {
+                            atomicAdd(P.out_sum_sh + chain[g], static_cast<unsigned long long>(sh));
+                            atomicAdd(P.out_sum_bs + chain[g], static_cast<unsigned long long>(bs));
+                            atomicAdd(P.out_flips + chain[g], static_cast<unsigned long long>(flips[g]));
+                        }
+                        continue;
+                    }
+                    const int t = m;
+                    const int32_t fourT = __ldg(P.fourT + t), twoT = fourT >> 1, qv = __ldg(P.q + t);
+                    const int32_t corr = step_corr(nlin_prev[g], __ldg(P.kcorr + t), __ldg(P.kconst + t));
+                    const uint32_t lw = uint32_t(2 * twoT - 1);
+                    const int32_t hcl = P.hclamp;
+                    uint32_t db[4] = {0u, 0u, 0u, 0u};
+                    uint32_t nsw = sw[g], ndw = 0u;
+                    int nl = 0;
+#pragma unroll
+                    for (int e = 0; e < 16; ++e) {
+                        const int j = e / R, k = e % R, i = k * 256 + 8 * cs + 2 * qq + j;
+                        const uint32_t u = rng_next(rng[g][j]);
+                        const bool valid = i < n;
+                        const bool up = (sw[g] >> e) & 1u, dif = (dw[g] >> e) & 1u;
+                        const int32_t h = int32_t(hv[e]);
+                        int32_t hs = up ? h : -h;
+                        if (hcl > 0) hs = max(-hcl, min(hs, hcl));
+                        const int32_t x = qv + (dif ? corr : -corr);
+                        const int32_t zt = hs * 65536 + x;
+                        const int32_t thr = threshold16(u, fourT);
+                        const bool fl = valid && (zt - thr < 0);
+                        nl += (valid && (uint32_t(zt + twoT - 1) < lw)) ? 1 : 0;
+                        if (fl) {
+                            nsw ^= 1u << e;
+                            ndw |= 1u << e;
+                            db[e >> 2] |= (up ? 0xFEu : 0x02u) << (8 * (e & 3));
+                            ++flips[g];
+                        }
+                    }
+                    sw[g] = nsw;
+                    dw[g] = ndw;
+                    const int par = m & 1;
+                    int8_t* drow = P.dbuf + ((size_t(G[g]) * 2 + par) * kM + r) * NPAD + cs * kResYS + qq * 16;
+                    *reinterpret_cast<uint4*>(drow) = make_uint4(db[0], db[1], db[2], db[3]);
+                    P.nlx[((size_t(G[g]) * 2 + par) * kM + r) * 128 + cs * 4 + qq] = int8_t(nl);
+                    asm volatile("fence.proxy.async.global;" ::: "memory");
+                    tc_fence_before();
+                    if (prof) { const long long t1 = clock64(); pr[1] += t1 - t0; t0 = t1; }
+                    asm volatile("bar.sync 1, %0;" ::"r"(kDW * 32) : "memory");
+                    if (tid == 0) flag_publish(P.flags + G[g] * kResSlices + cs, uint32_t(m + 2));
+                    if (prof) pr[2] += clock64() - t0;
+                }
+            }
+            tc_fence_before();
+        } else if (warp < kDW + kResPW) {
+            // ---------------- producer warps (all lanes poll the 32 slice flags at once; lane 0 issues) ----------
+            const int pwid = warp - kDW;
+            uint32_t ready = 0u;                   // slices known to have published (m, g)
+            for (int m = -1; m < S; ++m) {
+                const int par = m & 1;
+                for (int g = 0; g < 2; ++g) {
+                    const int ay = (G[g] * 2 + par) * kM;
+                    const uint32_t* fl = P.flags + G[g] * kResSlices;
+                    const uint32_t target = uint32_t(m + 2);
+                    ready = 0u;
+                    for (int c = 0; c < kResChunks; ++c, ++q) {
+                        if (int(q % kResPW) != pwid) continue;
+                        // every branch below is warp-uniform: lane 0 decides and broadcasts
+                        if (__shfl_sync(0xffffffffu, err_set(err) ? 1 : 0, 0)) continue;
+                        const int s = int(q % kResStages);
+                        const uint32_t u = q / kResStages;
+                        const long long w0 = prof ? clock64() : 0;
+                        if (u >= 1) {
+                            const int w = lane == 0 ? (mbar_wait(bar_empty + 8 * s, (u - 1) & 1u, err, kErrEmpty) ? 1 : 0) : 1;
+                            if (!__shfl_sync(0xffffffffu, w, 0)) continue;
+                        }
+                        const uint32_t need = c < 16 ? (3u << (2 * c)) : 0xffffffffu;
+                        bool ok = (ready & need) == need;
+                        if (!ok) {
+                            const uint64_t t0 = globaltimer();
+                            for (uint32_t k = 1;; ++k) {
+                                uint32_t v;
+                                asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(fl + lane) : "memory");
+                                ready = __ballot_sync(0xffffffffu, v >= target);
+                                if ((ready & need) == need) { ok = true; break; }
+                                if ((k & 63u) == 0 && __shfl_sync(0xffffffffu, globaltimer() - t0 > kWaitNs, 0)) {
+                                    if (lane == 0) atomicCAS(err, 0, kErrFlag);
+                                    break;
+                                }
+                            }
+                        }
+                        if (prof) pr[7] += clock64() - w0;
+                        if (!ok) continue;
+                        if (lane == 0) {
+                            asm volatile("fence.proxy.async.global;" ::: "memory");
+                            const uint32_t dst = smem_u32(stages + size_t(s) * TILE);
+                            mbar_arrive_expect_tx(bar_full + 8 * s, TILE);
+                            if (c < 16) tma_load_2d(dst, &mapD, c * kKChunk, ay, bar_full + 8 * s);
+                            else tma_load_2d(dst, &mapNL, 0, ay, bar_full + 8 * s);
+                        }
+                        __syncwarp();
+                    }
+                }
+            }
+        } else if (warp == kResMmaWarp) {
+            // ---------------- MMA thread ----------------
+            if (lane == 0) {
+                if (!jready) {
+                    if (!err_set(err)) mbar_wait(bar_j, 0u, err, kErrJ);
+                    jready = true;
+                }
+                for (int m = -1; m < S; ++m) {
+                    for (int g = 0; g < 2; ++g) {
+                        const long long t0 = prof ? clock64() : 0;
+                        for (int c = 0; c < kResChunks; ++c, ++q) {
+                            const int s = int(q % kResStages);
+                            const uint32_t u = q / kResStages;
+                            const long long w0 = prof ? clock64() : 0;
+                            const bool ok = !err_set(err) && mbar_wait(bar_full + 8 * s, u & 1u, err, kErrFull);
+                            if (prof) pr[5] += clock64() - w0;
+                            tc_fence_after();
+                            if (ok) {
+                                const uint32_t a0 = smem_u32(stages + size_t(s) * TILE);
+                                if (c < 16) {
+                                    const uint32_t b0 = smem_u32(jres + c * JCHUNK);
+#pragma unroll
+                                    for (int kk = 0; kk < kKChunk / 32; ++kk)
+                                        mma_i8(tmem + uint32_t(g * kResYS), sw128_desc(a0 + 32 * kk), sw128_desc(b0 + 32 * kk),
+                                               IDESC_H, 1u);
+                                } else {
+                                    const uint32_t b0 = smem_u32(ones);
+#pragma unroll
+                                    for (int kk = 0; kk < kKChunk / 32; ++kk)
+                                        mma_i8(tmem + uint32_t(128 + g * 16), sw128_desc(a0 + 32 * kk),
+                                               sw128_desc(b0 + 32 * kk), IDESC_NL, 1u);
+                                }
+                            }
+                            mma_commit(bar_empty + 8 * s);
+                        }
+                        mma_commit(bar_h0 + 8 * g);
+                        if (prof) pr[6] += clock64() - t0;
+                    }
+                }
+            } else {
+                q += uint32_t(S + 1) * 2 * kResChunks;
+            }
+            __syncwarp();
+        }
+    }
+    if (prof) {
+        long long* dst = P.prof + size_t(blockIdx.x) * kProfSlots;
+        if (warp == 0 && lane == 0) {
+            dst[0] = pr[0]; dst[1] = pr[1]; dst[2] = pr[2];
+        }
+        if (warp == kResMmaWarp && lane == 0) { dst[5] = pr[5]; dst[6] = pr[6]; dst[8] = clock64() - t_loop0; }
+        if (warp == kDW && lane == 0) dst[7] = pr[7];
+    }
+    __syncthreads();
+    if (warp == kResMmaWarp) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256) : "memory");
     }
 }
 
@@ -518,7 +942,66 @@ int launch_t(const TensorParams& P, int groups, const CUtensorMap& A, const CUte
     return 0;
 }
 
+template <int R>
+int max_clusters_t(int* out) {
+    auto fn = tensor_kernel<R>;
+    const size_t smem = smem_bytes_t<R>();
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = kC;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cfg.gridDim = dim3(kC);
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = smem;
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveClusters(out, fn, &cfg);
+    return int(e);
+}
+
+size_t res_smem_bytes() {
+    return 1024 + 16 * size_t(kResYS) * kKChunk + 2048 + size_t(kResStages) * kM * kKChunk + (2 * kResStages + 3) * 8 + 16;
+}
+
+// Concurrent pair slots of the resident kernel (32 co-resident CTAs each).
+int res_pair_slots(int npairs, int* out) {
+    auto fn = tensor_res_kernel;
+    const size_t smem = res_smem_bytes();
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    int per_sm = 0, dev = 0, sms = 0;
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kResThreads, smem);
+    if (e == cudaSuccess) e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return int(e);
+    *out = std::max(0, std::min(npairs, (per_sm * sms) / kResSlices));
+    return 0;
+}
+
 }  // namespace
+
+int tensor_geometry(int n, int nchains, TensorGeometry* g) {
+    const int np = std::max(2048, ((n + 255) / 256) * 256);
+    const int R = np / 256;
+    if (R == 8) {
+        const int npairs = ((nchains + kM - 1) / kM + 1) / 2;
+        int slots = 0;
+        const int rc = res_pair_slots(npairs, &slots);
+        g->cluster = 1;
+        g->ctas = kResSlices * slots;
+        g->max_active_clusters = g->ctas;
+        return rc;
+    }
+    g->cluster = kC;
+    g->ctas = kC * ((nchains + kM - 1) / kM);
+    if (R == 8) return max_clusters_t<8>(&g->max_active_clusters);
+    if (R == 12) return max_clusters_t<12>(&g->max_active_clusters);
+    if (R == 16) return max_clusters_t<16>(&g->max_active_clusters);
+    return int(cudaErrorInvalidValue);
+}
 
 bool tensor_supported(int n, int K, int nchains) {
     (void)K;
@@ -560,8 +1043,115 @@ int tensor_build_instance(const int8_t* J, int n, TensorInstance* out, std::stri
     return 0;
 }
 
+namespace {
+
+int res_run(TensorInstance* ti, const TensorRun& r, cudaStream_t st, std::string* why) {
+    const int npairs = ((r.nchains + kM - 1) / kM + 1) / 2;
+    const int ngroups = 2 * npairs;
+    int slots = 0;
+    int rc = res_pair_slots(npairs, &slots);
+    if (rc || slots < 1) {
+        if (why) *why = "the resident tensor kernel cannot be co-resident on this device";
+        return -2;
+    }
+    const size_t fbytes = size_t(ngroups) * kResSlices * 4;
+    const size_t dbytes = size_t(ngroups) * 2 * kM * 2048;
+    const size_t nbytes = size_t(ngroups) * 2 * kM * 128;
+    const size_t need = 256 + fbytes + dbytes + nbytes + 256;
+    cudaError_t e = cudaSuccess;
+    if (ti->ws_bytes < need) {
+        if (ti->d_ws) cudaFree(ti->d_ws);
+        ti->d_ws = nullptr;
+        ti->ws_bytes = 0;
+        e = cudaMalloc(&ti->d_ws, need);
+        if (e != cudaSuccess) {
+            if (why) *why = std::string("workspace: ") + cudaGetErrorString(e);
+            return -2;
+        }
+        ti->ws_bytes = need;
+    }
+    uint8_t* base = static_cast<uint8_t*>(ti->d_ws);
+    int* err = reinterpret_cast<int*>(base);
+    uint32_t* flags = reinterpret_cast<uint32_t*>(base + 256);
+    int8_t* dbuf = reinterpret_cast<int8_t*>(base + 256 + ((fbytes + 255) / 256) * 256);
+    int8_t* nlx = dbuf + dbytes;
+    if (r.bias && !ti->d_bias_perm) {
+        std::vector<int32_t> b(ti->n), bp(2048, 0);
+        e = cudaMemcpy(b.data(), r.bias, size_t(ti->n) * 4, cudaMemcpyDeviceToHost);
+        for (int i = 0; i < ti->n && e == cudaSuccess; ++i) bp[ti->perm[i]] = b[i];
+        if (e == cudaSuccess) e = cudaMalloc(&ti->d_bias_perm, 2048 * 4);
+        if (e == cudaSuccess) e = cudaMemcpy(ti->d_bias_perm, bp.data(), 2048 * 4, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            if (why) *why = std::string("bias: ") + cudaGetErrorString(e);
+            return -2;
+        }
+    }
+    CUtensorMap mapD, mapNL, mapJ;
+    if (!make_map(&mapD, dbuf, 2048, uint64_t(ngroups) * 2 * kM, kM) ||
+        !make_map(&mapNL, nlx, 128, uint64_t(ngroups) * 2 * kM, kM) || !make_map(&mapJ, ti->d_J, 2048, 2048, kResYS)) {
+        if (why) *why = "cuTensorMapEncodeTiled failed";
+        return -2;
+    }
+    e = cudaMemsetAsync(r.out_spins, 0, size_t(r.nchains) * 64 * 4, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(r.out_sum_sh, 0, size_t(r.nchains) * 8, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(r.out_sum_bs, 0, size_t(r.nchains) * 8, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(r.out_flips, 0, size_t(r.nchains) * 8, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(base, 0, 256 + fbytes, st);     // error word + flags
+    if (e != cudaSuccess) {
+        if (why) *why = std::string("memset: ") + cudaGetErrorString(e);
+        return -2;
+    }
+    ResParams P{};
+    P.n = ti->n;
+    P.S = r.tab.S;
+    P.npairs = npairs;
+    P.fourT = r.tab.fourT;
+    P.q = r.tab.q;
+    P.kcorr = r.tab.kcorr;
+    P.kconst = r.tab.kconst;
+    P.hclamp = r.hclamp;
+    P.bias_perm = r.bias ? ti->d_bias_perm : nullptr;
+    P.seed = r.seed;
+    P.trial_offset = r.trial_offset;
+    P.nchains = r.nchains;
+    P.flags = flags;
+    P.dbuf = dbuf;
+    P.nlx = nlx;
+    P.out_spins = r.out_spins;
+    P.out_sum_sh = reinterpret_cast<unsigned long long*>(r.out_sum_sh);
+    P.out_sum_bs = reinterpret_cast<unsigned long long*>(r.out_sum_bs);
+    P.out_flips = reinterpret_cast<unsigned long long*>(r.out_flips);
+    P.out_trace = r.out_trace;
+    P.out_h = r.out_h;
+    P.err = err;
+    P.prof = r.prof;
+    auto fn = tensor_res_kernel;
+    const size_t smem = res_smem_bytes();
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cfg.gridDim = dim3(kResSlices * slots);
+    cfg.blockDim = dim3(kResThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    if (e == cudaSuccess) e = cudaLaunchKernelEx(&cfg, fn, mapD, mapNL, mapJ, P);
+    if (e != cudaSuccess) {
+        if (why) *why = std::string("launch: ") + cudaGetErrorString(e);
+        return -2;
+    }
+    ti->last_err = err;
+    return 0;
+}
+
+}  // namespace
+
 int tensor_run(TensorInstance* ti, const TensorRun& r, cudaStream_t st, std::string* why) {
     const int np = ti->np, R = np / 256;
+    if (R == 8) return res_run(ti, r, st, why);
     const int groups = (r.nchains + kM - 1) / kM;
     // workspace: exchange buffers, permuted bias, error word
     const size_t dbytes = size_t(groups) * 2 * kM * np;
@@ -633,6 +1223,7 @@ int tensor_run(TensorInstance* ti, const TensorRun& r, cudaStream_t st, std::str
     P.out_trace = r.out_trace;
     P.out_h = r.out_h;
     P.err = err;
+    P.prof = r.prof;
     int rc = -1;
     if (R == 8) rc = launch_t<8>(P, groups, mapA, mapB, st, why);
     else if (R == 12) rc = launch_t<12>(P, groups, mapA, mapB, st, why);

@@ -190,6 +190,7 @@ class RunResult:
     trace: Optional[np.ndarray] = None
     fields: Optional[np.ndarray] = None
     device_ms: float = 0.0
+    profile: Optional[dict] = None
 
     def cuts(self, sumw: int) -> np.ndarray:
         """Device cut = (sumw + sum_sh / 2) / 2 with C++ truncating division (sca_ref.hpp:153)."""
@@ -207,8 +208,9 @@ def tdiv(a, b: int):
 
 
 def run(dev: DeviceInstance, tb: Tables, seed: int, trial_offset: int, nchains: int, trace: bool = False,
-        fields: bool = False, engine: str = "auto", wide="auto") -> RunResult:
-    """nchains anneals (trial ids trial_offset .. trial_offset + nchains - 1) in one launch."""
+        fields: bool = False, engine: str = "auto", wide="auto", profile: bool = False) -> RunResult:
+    """nchains anneals (trial ids trial_offset .. trial_offset + nchains - 1) in one launch. profile=True records
+    the tensor engine's per-phase cycle counters (RunResult.profile)."""
     L = load()
     n = dev.n
     W = spin_words(n)
@@ -217,15 +219,18 @@ def run(dev: DeviceInstance, tb: Tables, seed: int, trial_offset: int, nchains: 
     S = tb.S
     tr = np.zeros((nchains, S), np.int32) if trace else None
     hf = np.zeros((nchains, n), np.int32) if fields else None
-    o = _lib.opts(engine, wide)
+    o = _lib.opts(engine, wide, profile)
     args = (dev._h, tb._h, C.c_uint64(seed), C.c_uint32(trial_offset), nchains, C.byref(o), spins.ctypes.data,
             sh.ctypes.data, bs.ctypes.data, fl.ctypes.data, tr.ctypes.data if trace else None)
     if fields:
         check(L.anc_run_fields(*args, hf.ctypes.data))
     else:
         check(L.anc_run(*args))
-    return RunResult(n=n, trial_offset=trial_offset, spins=spins, sum_sh=sh, sum_bs=bs, flips=fl, trace=tr, fields=hf,
-                     device_ms=L.anc_last_device_ms())
+    res = RunResult(n=n, trial_offset=trial_offset, spins=spins, sum_sh=sh, sum_bs=bs, flips=fl, trace=tr, fields=hf,
+                    device_ms=L.anc_last_device_ms())
+    if profile:
+        res.profile = _lib.last_profile()
+    return res
 
 
 def run_batch(jobs: List[dict], engine: str = "auto", wide="auto") -> List[RunResult]:

@@ -103,8 +103,16 @@ typedef struct {
     int engine;      /* ANC_ENGINE_* */
     int wide;        /* -1 auto (clamp only if the plan needs it), 0 never (EINVAL if needed), 1 always */
     int threads;     /* host threads for rescoring; 0 = default */
-    int reserved[5];
+    int profile;     /* 1: record per-phase cycle counters of the tensor engine (anc_last_profile) */
+    int reserved[4];
 } anc_run_opts;
+
+/* Phase profile of the calling thread's last synchronous tensor-engine run with opts.profile = 1 (the counterpart
+ * of the reference's SCA_PROFILE build, sca_gpu.cu:163-168): out[0..8] = mean SM cycles per step of
+ *   0 wait for fields, 1 TMEM load + decide + update store, 2 n_lin publish, 3 cluster barrier, 4 n_lin read,
+ *   5 MMA waiting for TMA, 6 MMA phase (barrier to last commit), 7 TMA waiting for free stages, 8 whole step;
+ * out[9] = CTAs, out[10] = CTAs per cluster, out[11] = co-resident clusters. Returns the count written (<= max). */
+ANC_API int anc_last_profile(double* out, int max);
 
 /* Replaces one launch + readback of sca_gpu / sca_gpu_bias (sca_gpu.cu:699-713, sca_gpu_bias.cu:716-733) and
  * sca::run_trial / run_trial_bias per chain: nchains anneals with trial ids trial_offset + c.
