@@ -763,3 +763,121 @@ int anc_run_batch(int njobs, const anc_job* jobs, const anc_run_opts* o) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------------------------------------
+// Allocation-free batch entry point (anc_run_batch_noalloc). Its scratch lives in one file-scope device array; host
+// staging uses file-scope arrays, so no call here allocates.
+namespace {
+
+constexpr int kNaMaxJobs = ANC_NOALLOC_MAX_JOBS;
+constexpr int kNaMaxAnneals = ANC_NOALLOC_MAX_ANNEALS;
+constexpr size_t kNaJobsOff = 256;   // [0, 256): four work-queue counters (one per kernel kind)
+constexpr size_t kNaItemsOff = kNaJobsOff + ((size_t(kNaMaxJobs) * sizeof(anc::PlainJob) + 255) / 256) * 256;
+constexpr size_t kNaBytes = kNaItemsOff + size_t(kNaMaxAnneals) * sizeof(int2);
+static_assert(kNaBytes <= ANC_NOALLOC_SCRATCH_BYTES, "scratch larger than the size the header states");
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaBytes];
+
+std::mutex g_na_mu;                       // guards the host staging arrays and the address table
+void* g_na_addr[256] = {};                // device address of g_noalloc_scratch, per device ordinal
+anc::PlainJob g_na_jobs[kNaMaxJobs];
+int2 g_na_items[kNaMaxAnneals];
+
+}  // namespace
+
+extern "C" int anc_run_batch_noalloc(int njobs, const anc_device_job* jobs, void* stream) {
+    if (njobs < 1 || !jobs) return fail(ANC_EINVAL, "need 1 <= njobs and a job array");
+    if (njobs > kNaMaxJobs) return fail(ANC_EINVAL, "at most %d jobs per allocation-free call (got %d)", kNaMaxJobs, njobs);
+    long long total = 0;
+    for (int k = 0; k < njobs; ++k) {
+        const anc_device_job& j = jobs[k];
+        if (j.n < 1 || j.n > 65536) return fail(ANC_EINVAL, "job %d: n must be in 1..65536", k);
+        if (!(j.kbits == 0 || j.kbits == 1 || j.kbits == 2 || j.kbits == 4))
+            return fail(ANC_EINVAL, "job %d: kbits must be 0 (CSR), 1, 2 or 4", k);
+        if (j.kbits ? !j.planes : (!j.row_ptr || !j.adj)) return fail(ANC_EINVAL, "job %d: coupling pointers missing", k);
+        if (!j.fourT || !j.q || !j.kcorr || !j.kconst || j.S < 1) return fail(ANC_EINVAL, "job %d: tables missing", k);
+        if (!j.spins || !j.sum_sh || !j.sum_bs || !j.flips) return fail(ANC_EINVAL, "job %d: outputs missing", k);
+        if (j.nchains < 1 || j.hclamp < 0) return fail(ANC_EINVAL, "job %d: need nchains >= 1 and hclamp >= 0", k);
+        total += j.nchains;
+    }
+    if (total > kNaMaxAnneals)
+        return fail(ANC_EINVAL, "at most %d anneals per allocation-free call (got %lld)", kNaMaxAnneals, total);
+    std::lock_guard<std::mutex> lock(g_na_mu);
+    int dev = 0, sms = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 256) return fail(ANC_EINVAL, "device ordinal out of range");
+    if (!g_na_addr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+        g_na_addr[dev] = p;
+    }
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    uint8_t* base = static_cast<uint8_t*>(g_na_addr[dev]);
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    for (int k = 0; k < njobs; ++k) {
+        const anc_device_job& j = jobs[k];
+        anc::PlainJob& p = g_na_jobs[k];
+        p = anc::PlainJob{};
+        p.n = j.n;
+        p.np = pad_np(j.n);
+        p.nw = p.np / 32;
+        p.nwj = ((p.nw + 31) / 32) * 32;
+        p.K = j.kbits;
+        p.planes = j.planes;
+        p.row_ptr = j.row_ptr;
+        p.adj = j.adj;
+        p.bias = j.bias;
+        p.tab.fourT = j.fourT;
+        p.tab.q = j.q;
+        p.tab.kcorr = j.kcorr;
+        p.tab.kconst = j.kconst;
+        p.tab.S = j.S;
+        p.seed = j.seed;
+        p.trial_offset = j.trial_offset;
+        p.ntrials = j.nchains;
+        p.trace = j.trace != nullptr;
+        p.hclamp = j.hclamp;
+        p.out_spins = reinterpret_cast<uint32_t*>(j.spins);
+        p.out_sum_sh = j.sum_sh;
+        p.out_sum_bs = j.sum_bs;
+        p.out_flips = j.flips;
+        p.out_trace = j.trace;
+        p.out_h = nullptr;
+    }
+    CK(cudaMemcpyAsync(base + kNaJobsOff, g_na_jobs, sizeof(anc::PlainJob) * njobs, cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(base, 0, 256, st));   // the counters must start at zero on every call
+    const int kinds[4] = {0, 1, 2, 4};
+    int item_off = 0;
+    for (int ki = 0; ki < 4; ++ki) {
+        const int K = kinds[ki];
+        int cnt = 0, np_max = 0, nwj_max = 0;
+        for (int k = 0; k < njobs; ++k) {
+            if (g_na_jobs[k].K != K) continue;
+            np_max = std::max(np_max, g_na_jobs[k].np);
+            nwj_max = std::max(nwj_max, K == 0 ? g_na_jobs[k].nw : g_na_jobs[k].nwj);
+            for (int c = 0; c < jobs[k].nchains; ++c) g_na_items[item_off + cnt++] = make_int2(k, c);
+        }
+        if (!cnt) continue;
+        CK(cudaMemcpyAsync(base + kNaItemsOff + size_t(item_off) * sizeof(int2), g_na_items + item_off,
+                           size_t(cnt) * sizeof(int2), cudaMemcpyHostToDevice, st));
+        anc::PlainLaunch L{};
+        L.jobs = reinterpret_cast<const anc::PlainJob*>(base + kNaJobsOff);
+        L.items = reinterpret_cast<const int2*>(base + kNaItemsOff) + item_off;
+        L.nitems = cnt;
+        L.next_item = reinterpret_cast<int*>(base) + ki;
+        L.np_max = np_max;
+        L.nwj_max = nwj_max;
+        const int P = plain_P(np_max);
+        const size_t smem = anc::plain_smem_bytes(np_max, nwj_max, K, P);
+        if (smem > 227 * 1024) return fail(ANC_EINVAL, "instance too large for the plain engine");
+        int per_sm = 0;
+        int rc = anc::plain_max_blocks_per_sm(K, P, smem, &per_sm);
+        if (rc) return cuda_fail(cudaError_t(rc), "occupancy");
+        if (per_sm < 1) return fail(ANC_EINVAL, "plain engine cannot be resident");
+        rc = anc::plain_launch(L, K, P, std::max(1, std::min(cnt, per_sm * sms)), smem, st);
+        if (rc) return cuda_fail(cudaError_t(rc), "plain engine launch");
+        item_off += cnt;
+    }
+    return ANC_OK;
+}

@@ -155,6 +155,49 @@ typedef struct {
 /* Replaces running sca_gpu_bias once per instance (run_gsel.sh / run_bias.sh loops). */
 ANC_API int anc_run_batch(int njobs, const anc_job* jobs, const anc_run_opts* opts);
 
+/* No counterpart in the reference. Allocation-free batch run of the plain engine, for callers that cannot call
+ * cudaMalloc: applications that own every byte of device memory through their own pool or allocator (a serving
+ * runtime or framework caching allocator that has reserved the GPU), and callers with a fixed device-memory budget
+ * that must not grow. All inputs and outputs are DEVICE memory owned by the caller; the call allocates nothing
+ * (no cudaMalloc, no cudaFree, no allocating library routine). Its scratch -- job descriptors, the work-item queue
+ * and its counters -- is one file-scope device array of ANC_NOALLOC_SCRATCH_BYTES that every GPU loading the library
+ * holds until exit. The first call on a device looks that array up (cudaGetSymbolAddress) with the device current.
+ * Limits: at most ANC_NOALLOC_MAX_JOBS jobs and ANC_NOALLOC_MAX_ANNEALS anneals (sum of nchains) per call; larger
+ * requests return ANC_EINVAL. Every call reuses the same array and resets its counters: calls that overlap on the GPU
+ * (different streams, or several host threads) race; calls in order on one stream do not.
+ * Job layout:
+ *   kbits 1/2/4: planes = [kbits][NP][NWJ] uint32 with NP = anc_np(n), NWJ = ceil(NP/32) rounded up to a multiple of
+ *   32; word x*NWJ + y/32, bit y%32 of plane p describes J_xy: kbits 1 -> [J_xy = +1] (a +-1 complete graph);
+ *   kbits 2/4 -> plane 0 = [J_xy < 0], plane b = bit b-1 of |J_xy|. kbits 0: CSR row_ptr[n+1] and
+ *   adj[k] = (y << 8) | (uint8)J_xy for every nonzero of row x.
+ *   hclamp: 0 when anc_plan_ranges reports plain_ok, else its hclamp. Outputs as anc_run_device. */
+#define ANC_NOALLOC_MAX_JOBS 64
+#define ANC_NOALLOC_MAX_ANNEALS 16384
+#define ANC_NOALLOC_SCRATCH_BYTES (144 * 1024) /* upper bound of the device scratch array (139 KB used) */
+typedef struct {
+    int n;
+    int kbits;
+    const uint32_t* planes;
+    const int32_t* row_ptr;
+    const uint32_t* adj;
+    const int32_t* bias;      /* n entries or NULL */
+    const int32_t* fourT;     /* tables, S entries each */
+    const int32_t* q;
+    const int64_t* kcorr;
+    const int32_t* kconst;
+    int S;
+    int32_t hclamp;
+    uint64_t seed;
+    uint32_t trial_offset;
+    int nchains;
+    uint64_t* spins;          /* [nchains][anc_spin_words(n)] */
+    int64_t* sum_sh;          /* [nchains] */
+    int64_t* sum_bs;          /* [nchains] */
+    int64_t* flips;           /* [nchains] */
+    int32_t* trace;           /* [nchains][S] or NULL */
+} anc_device_job;
+ANC_API int anc_run_batch_noalloc(int njobs, const anc_device_job* jobs, void* stream);
+
 /* Last device time of a synchronous run on this thread (ms, CUDA events around the launch). */
 ANC_API double anc_last_device_ms(void);
 
