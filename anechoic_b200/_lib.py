@@ -14,12 +14,15 @@ LIB_PATH = os.path.join(PKG, "libanechoic.so")
 
 ANC_OK, ANC_EINVAL, ANC_ECUDA, ANC_ETIMEOUT, ANC_EMISMATCH = 0, -1, -2, -3, -4
 ENGINES = {"auto": 0, "plain": 1, "tensor": 2}
+TENSOR_KINDS = {"auto": 0, "int8": 1, "fp4": 2}
+KERNELS = {0: None, 1: "plain", 2: "tensor-int8", 3: "tensor-fp4"}
 
 EXPORTS = ("anc_instance_create", "anc_instance_create_csr", "anc_instance_get_info", "anc_instance_destroy",
            "anc_tables_create", "anc_tables_from_schedule", "anc_tables_steps", "anc_tables_read", "anc_tables_destroy",
            "anc_range_plan", "anc_schedule_tables", "anc_plan_ranges", "anc_spin_words", "anc_np", "anc_run",
            "anc_run_fields", "anc_run_device",
-           "anc_run_batch", "anc_last_device_ms", "anc_last_error", "anc_last_profile", "anc_version")
+           "anc_run_batch", "anc_last_device_ms", "anc_last_kernel", "anc_last_error", "anc_last_profile", "anc_version",
+           "anc_run_batch_noalloc")
 
 
 class AncError(RuntimeError):
@@ -38,7 +41,7 @@ class InstanceInfo(C.Structure):
 
 class RunOpts(C.Structure):
     _fields_ = [("engine", C.c_int), ("wide", C.c_int), ("threads", C.c_int), ("profile", C.c_int),
-                ("reserved", C.c_int * 4)]
+                ("tensor_kind", C.c_int), ("reserved", C.c_int * 3)]
 
 
 class Job(C.Structure):
@@ -85,6 +88,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         L.anc_run_batch.argtypes = [_i, C.POINTER(Job), C.POINTER(RunOpts)]
         L.anc_last_device_ms.argtypes = []
         L.anc_last_device_ms.restype = C.c_double
+        L.anc_last_kernel.argtypes = []
+        L.anc_last_kernel.restype = C.c_int
         L.anc_last_error.argtypes = []
         L.anc_last_error.restype = C.c_char_p
         L.anc_last_profile.argtypes = [C.POINTER(C.c_double), C.c_int]
@@ -100,9 +105,10 @@ def check(rc: int):
         raise AncError(rc, msg)
 
 
-def opts(engine: str = "auto", wide="auto", profile: bool = False) -> RunOpts:
+def opts(engine: str = "auto", wide="auto", profile: bool = False, tensor_kind: str = "auto") -> RunOpts:
     o = RunOpts()
     o.engine = ENGINES[engine]
+    o.tensor_kind = TENSOR_KINDS[tensor_kind]
     o.wide = {"auto": -1, 0: 0, 1: 1, False: 0, True: 1, "0": 0, "1": 1}[wide]
     o.threads = 0
     o.profile = int(bool(profile))
@@ -110,11 +116,17 @@ def opts(engine: str = "auto", wide="auto", profile: bool = False) -> RunOpts:
 
 
 PROFILE_FIELDS = ("wait_fields", "decide", "nlin_publish", "cluster_barrier", "nlin_read", "mma_wait_tma",
-                  "mma_phase", "tma_wait_stage", "step", "ctas", "cluster", "max_active_clusters")
+                  "mma_phase", "tma_wait_stage", "step", "ctas", "cluster", "max_active_clusters", "mma_issue",
+                  "mma_commit")
+
+
+def last_kernel():
+    """Kernel of this thread's last single-instance run: "plain", "tensor-int8", "tensor-fp4" (None before any)."""
+    return KERNELS[load().anc_last_kernel()]
 
 
 def last_profile() -> dict:
     """Phase profile (SM cycles per step) of this thread's last profiled tensor-engine run."""
-    buf = (C.c_double * 12)()
-    k = load().anc_last_profile(buf, 12)
+    buf = (C.c_double * 14)()
+    k = load().anc_last_profile(buf, 14)
     return {PROFILE_FIELDS[i]: buf[i] for i in range(k)}

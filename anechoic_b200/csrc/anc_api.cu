@@ -20,6 +20,7 @@ namespace {
 thread_local std::string g_err;
 thread_local double g_dev_ms = 0.0;
 thread_local std::vector<double> g_prof;
+thread_local int g_last_kernel = 0;
 
 int fail(int code, const char* fmt, ...) {
     char buf[512];
@@ -306,6 +307,7 @@ int run_device_impl(anc_instance* I, anc_tables* tb, uint64_t seed, uint32_t off
         r.out_trace = out.trace;
         r.out_h = out.h;
         r.prof = nullptr;
+        r.kind = o ? o->tensor_kind : ANC_TENSOR_AUTO;
         I->prof_ctas = 0;
         if (o && o->profile) {
             anc::TensorGeometry geo;
@@ -321,10 +323,13 @@ int run_device_impl(anc_instance* I, anc_tables* tb, uint64_t seed, uint32_t off
         rc = anc::tensor_run(&I->tensor, r, st, &why);
         if (rc == -3) return fail(ANC_ETIMEOUT, "tensor engine: %s", why.c_str());
         if (rc) return fail(rc == -2 ? ANC_ECUDA : ANC_EINVAL, "tensor engine: %s", why.c_str());
+        g_last_kernel = I->tensor.last_kind == anc::TENSOR_KIND_FP4 ? ANC_KERNEL_TENSOR_FP4 : ANC_KERNEL_TENSOR_INT8;
         return ANC_OK;
     }
     const anc::PlainJob job = make_job(I, tb, seed, off, nchains, hclamp, out);
-    return launch_plain_single(I, job, st);
+    rc = launch_plain_single(I, job, st);
+    if (rc == ANC_OK) g_last_kernel = ANC_KERNEL_PLAIN;
+    return rc;
 }
 
 int run_host_impl(anc_instance* I, anc_tables* tb, uint64_t seed, uint32_t off, int nchains, const anc_run_opts* o,
@@ -364,16 +369,17 @@ int run_host_impl(anc_instance* I, anc_tables* tb, uint64_t seed, uint32_t off, 
     if (I->prof_ctas > 0) {
         std::vector<long long> h(size_t(I->prof_ctas) * 16);
         CK(cudaMemcpy(h.data(), I->w_prof.p, h.size() * sizeof(long long), cudaMemcpyDeviceToHost));
-        g_prof.assign(12, 0.0);
-        for (int s = 0; s < 9; ++s) {
+        g_prof.assign(14, 0.0);
+        const int slot_of[11] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 12, 13};   // phase slot -> output index
+        for (int s = 0; s < 11; ++s) {
             double acc = 0;
             for (int b = 0; b < I->prof_ctas; ++b) acc += double(h[size_t(b) * 16 + s]);
-            g_prof[s] = acc / I->prof_ctas / std::max(1, I->prof_S);
+            g_prof[slot_of[s]] = acc / I->prof_ctas / std::max(1, I->prof_S);
         }
         anc::TensorGeometry geo;
         anc::tensor_geometry(I->n, nchains, &geo);
-        g_prof[9] = geo.ctas;
-        g_prof[10] = geo.cluster;
+        g_prof[9] = I->tensor.last_ctas;
+        g_prof[10] = I->tensor.last_cluster;
         g_prof[11] = geo.max_active_clusters;
         I->prof_ctas = 0;
     }
@@ -396,6 +402,7 @@ int anc_last_profile(double* out, int max) {
 }
 const char* anc_version(void) { return "anechoic-b200 0.1 (sm_100a)"; }
 double anc_last_device_ms(void) { return g_dev_ms; }
+int anc_last_kernel(void) { return g_last_kernel; }
 int anc_np(int n) { return pad_np(n); }
 int anc_spin_words(int n) { return pad_np(n) / 64; }
 

@@ -16,8 +16,16 @@ struct TensorInstance {
     void* d_ws = nullptr;        // exchange buffers + error word
     size_t ws_bytes = 0;
     int32_t* d_bias_perm = nullptr;
+    int64_t bias_absmax = 0;     // max |b_i| (set with d_bias_perm)
+    uint8_t* d_J4 = nullptr;     // J_perm as packed e2m1 [2048][1024] when NP = 2048 and every |J_xy| <= 1, else null
+    int64_t rowsum_max = 0;      // max_y sum_x |J_xy|
     int* last_err = nullptr;     // error word of the last launch
+    int last_kind = 0;           // kernel of the last launch: TENSOR_KIND_INT8 or TENSOR_KIND_FP4
+    int last_ctas = 0, last_cluster = 0;
 };
+
+// Operand format of the field update: int8 (any |J| <= 127) or packed fp4 e2m1 (|J| <= 1, NP = 2048).
+constexpr int TENSOR_KIND_AUTO = 0, TENSOR_KIND_INT8 = 1, TENSOR_KIND_FP4 = 2;
 
 struct TensorRun {
     DevTables tab;
@@ -33,6 +41,7 @@ struct TensorRun {
     int32_t* out_trace;
     int32_t* out_h;
     long long* prof;          // device [grid][16] phase cycle totals, or null (profiling off)
+    int kind;                 // TENSOR_KIND_*
 };
 
 // Launch geometry of a run: CTAs in the grid, CTAs per cluster, and how many clusters can be co-resident.
@@ -45,6 +54,9 @@ bool tensor_supported(int n, int K, int nchains);
 bool tensor_prefer(int n, int K, int nchains, int S);
 int tensor_build_instance(const int8_t* J, int n, TensorInstance* out, std::string* why);
 int tensor_run(TensorInstance* ti, const TensorRun& r, cudaStream_t st, std::string* why);
+// Whether the fp4 kernel can run this instance with this bias bound exactly (the fields stay far inside the range
+// where fp32 accumulation of integers is exact).
+bool tensor_fp4_eligible(const TensorInstance* ti, int64_t bias_absmax);
 // After the stream has reached the launch: -3 if a bounded device wait expired, 0 otherwise.
 int tensor_check_error(TensorInstance* ti, cudaStream_t st, std::string* why);
 void tensor_free_instance(TensorInstance* ti);

@@ -620,7 +620,7 @@ __global__ void __launch_bounds__(kResThreads, 1)
     uint32_t q = 0;                        // running chunk index (producers, MMA)
     bool jready = false;
     const bool prof = P.prof != nullptr;
-    long long pr[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    long long pr[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     const long long t_loop0 = clock64();
 
     for (int pw = gp0; pw < P.npairs; pw += gstride) {
@@ -830,6 +830,7 @@ __global__ void __launch_bounds__(kResThreads, 1)
                             const bool ok = !err_set(err) && mbar_wait(bar_full + 8 * s, u & 1u, err, kErrFull);
                             if (prof) pr[5] += clock64() - w0;
                             tc_fence_after();
+                            const long long i0 = prof ? clock64() : 0;
                             if (ok) {
                                 const uint32_t a0 = smem_u32(stages + size_t(s) * TILE);
                                 if (c < 16) {
@@ -846,7 +847,9 @@ __global__ void __launch_bounds__(kResThreads, 1)
                                                sw128_desc(b0 + 32 * kk), IDESC_NL, 1u);
                                 }
                             }
+                            const long long i1 = prof ? clock64() : 0;
                             mma_commit(bar_empty + 8 * s);
+                            if (prof) { const long long i2 = clock64(); pr[9] += i1 - i0; pr[10] += i2 - i1; }
                         }
                         mma_commit(bar_h0 + 8 * g);
                         if (prof) pr[6] += clock64() - t0;
@@ -863,11 +866,387 @@ __global__ void __launch_bounds__(kResThreads, 1)
         if (warp == 0 && lane == 0) {
             dst[0] = pr[0]; dst[1] = pr[1]; dst[2] = pr[2];
         }
-        if (warp == kResMmaWarp && lane == 0) { dst[5] = pr[5]; dst[6] = pr[6]; dst[8] = clock64() - t_loop0; }
+        if (warp == kResMmaWarp && lane == 0) {
+            dst[5] = pr[5]; dst[6] = pr[6]; dst[8] = clock64() - t_loop0; dst[9] = pr[9]; dst[10] = pr[10];
+        }
         if (warp == kDW && lane == 0) dst[7] = pr[7];
     }
     __syncthreads();
     if (warp == kResMmaWarp) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256) : "memory");
+    }
+}
+
+// ------------------------------------------------------------------------------------------------ fp4 kernel
+// For NP = 2048 and couplings in {-1, 0, +1}: J and D are exact in e2m1 (packed fp4, two per byte), so the update
+// runs as tcgen05.mma.kind::mxf4.block_scale (M 128, N 128, K 64) with every block scale 1.0 (ue8m0 0x7F) and fp32
+// accumulation, exact for these integer fields. A cooperative persistent grid of 16 y-slices x G replica groups:
+// CTA (group slot, slice cs) owns RNG lanes 16cs .. 16cs+15 (128 columns at p = 8l + k), keeps its J slice
+// (128 rows x 2048 fp4 = 128 KB) resident, and runs one group of 128 replicas at a time:
+//   16 decision warps: thread (replica r, quarter qq) owns lanes 16cs + 4qq + j (j < 4) x 8 rounds = 32 slots =
+//     TMEM columns qq*32 + j*8 + k; it decides (lanes interleaved for ILP), writes its 32 D nibbles (16 bytes) and
+//     its n_lin partial byte, and one thread publishes flag[g][cs] = m + 2.
+//   4 producer warps poll the 16 slice flags warp-wide and TMA each 128 x 128-byte D tile (256 K values = two
+//     source slices) as both slices publish; a 9th tile carries the n_lin partials.
+//   the MMA thread: 4 x mxf4 MMAs per D tile into the fp32 field accumulator, 2 x i8 MMAs (N 16) of the partials
+//     against a ones row into an int32 n_lin accumulator.
+constexpr int kF4Slices = 16;
+constexpr int kF4YS = 128;
+constexpr int kF4PW = 4;
+constexpr int kF4Stages = 5;
+constexpr int kF4MmaWarp = kDW + kF4PW;
+constexpr int kF4Threads = (kDW + kF4PW + 1) * 32;
+constexpr int kF4Chunks = 9;              // 8 D tiles (2048 fp4 = 1024 bytes per row) + 1 n_lin tile per step
+constexpr int kF4SfCol = 160;             // TMEM columns 144..255 hold scale factors 0x7F (1.0)
+
+struct F4Params {
+    int n, S, ngroups;
+    const int32_t* fourT;
+    const int32_t* q;
+    const int64_t* kcorr;
+    const int32_t* kconst;
+    int32_t hclamp;
+    const int32_t* bias_perm;           // [2048] or null
+    uint64_t seed;
+    uint32_t trial_offset;
+    int nchains;
+    uint32_t* flags;                    // [ngroups][16] (zeroed)
+    uint8_t* dbuf;                      // [ngroups][2][128][1024] packed e2m1
+    int8_t* nlx;                        // [ngroups][2][128][128]
+    uint32_t* out_spins;                // [nchains][64] (zeroed)
+    unsigned long long* out_sum_sh;
+    unsigned long long* out_sum_bs;
+    unsigned long long* out_flips;
+    int32_t* out_trace;
+    int32_t* out_h;
+    int* err;
+    long long* prof;
+};
+
+__device__ __forceinline__ void mma_mxf4(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t sfa,
+                                         uint32_t sfb) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, 1, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::mxf4.block_scale.block32 [%0], %1, %2, %3, [%4], [%5], p;\n\t}"
+        ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(sfa), "r"(sfb));
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,"
+        "%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+          "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]),
+          "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
+          "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+        : "r"(taddr));
+}
+
+__global__ void __launch_bounds__(kF4Threads, 1)
+    tensor_fp4_kernel(const __grid_constant__ CUtensorMap mapD, const __grid_constant__ CUtensorMap mapNL,
+                      const __grid_constant__ CUtensorMap mapJ, const __grid_constant__ F4Params P) {
+    constexpr int R = 8, ROWB = 1024;                       // rounds; bytes per packed D / J row
+    constexpr uint32_t TILE = kM * kKChunk;                 // 16 KB tile (128 rows x 128 bytes)
+    constexpr uint32_t IDESC_F4 = (1u << 7) | (1u << 10) | (uint32_t(kF4YS >> 3) << 17) | (1u << 23) | (uint32_t(kM >> 4) << 24);
+    constexpr uint32_t IDESC_NL = (2u << 4) | (1u << 7) | (1u << 10) | (uint32_t(16 >> 3) << 17) | (uint32_t(kM >> 4) << 24);
+
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* jres = smem;                                   // 8 x 16 KB
+    uint8_t* ones = smem + 8 * TILE;                        // 2 KB: row 0 = 128 x int8(1)
+    uint8_t* stages = ones + 2048;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(stages + kF4Stages * TILE);   // full[5], empty[5], hready, jbar
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kF4Stages + 2);
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int cs = int(blockIdx.x % kF4Slices);
+    const int gs0 = int(blockIdx.x / kF4Slices), gstride = int(gridDim.x / kF4Slices);
+    const int n = P.n, S = P.S;
+    int* err = P.err;
+    const uint32_t bar_full = smem_u32(bars), bar_empty = smem_u32(bars + kF4Stages);
+    const uint32_t bar_h = smem_u32(bars + 2 * kF4Stages), bar_j = smem_u32(bars + 2 * kF4Stages + 1);
+
+    if (tid == 0) {
+        for (int s = 0; s < kF4Stages; ++s) {
+            mbar_init(bar_full + 8 * s, 1);
+            mbar_init(bar_empty + 8 * s, 1);
+        }
+        mbar_init(bar_h, 1);
+        mbar_init(bar_j, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    for (int i = tid; i < 2048; i += blockDim.x) ones[i] = i < 128 ? 1 : 0;
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (warp == kF4MmaWarp) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(256)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    if (warp == kDW && lane == 0) {
+        mbar_arrive_expect_tx(bar_j, 8 * TILE);
+        for (int kc = 0; kc < 8; ++kc) tma_load_2d(smem_u32(jres + kc * TILE), &mapJ, kc * kKChunk, cs * kF4YS, bar_j);
+    }
+    // scale factors: columns 144..255 of every lane := 0x7F7F7F7F (ue8m0 1.0); warps 0..3 cover the 128 lanes
+    const uint32_t tl = uint32_t((warp & 3) * 32) << 16;
+    if (warp < 4) {
+        uint32_t v[16];
+#pragma unroll
+        for (int e = 0; e < 16; ++e) v[e] = 0x7F7F7F7Fu;
+        for (int c0 = 144; c0 < 256; c0 += 16) tmem_st16(tmem + tl + uint32_t(c0), v);
+        tmem_wait_st();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+
+    const int r = (warp & 3) * 32 + lane, qq = warp >> 2;
+    uint32_t hph = 0u, q = 0;
+    bool jready = false;
+    const bool prof = P.prof != nullptr;
+    long long pr[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    const long long t_loop0 = clock64();
+
+    for (int g = gs0; g < P.ngroups; g += gstride) {
+        if (warp < kDW) {
+            // ---------------- decision warps ----------------
+            const int chain = g * kM + r;
+            const bool writer = chain < P.nchains;
+            Xoshiro rng[4];
+            uint32_t sw = 0u, dw = 0u, nlacc_prev = 0u;
+            int32_t nlin_prev = 0;
+            long long flips = 0;
+            {
+                uint32_t db[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+                for (int j = 0; j < 4; ++j) rng_seed(rng[j], P.seed, P.trial_offset + uint32_t(chain), uint32_t(16 * cs + 4 * qq + j));
+#pragma unroll
+                for (int k = 0; k < R; ++k)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const int col = j * R + k, i = k * 256 + 16 * cs + 4 * qq + j;
+                        const uint32_t rv = rng_next(rng[j]);
+                        const bool valid = i < n;
+                        const uint32_t up = valid ? (rv >> 31) : 1u;
+                        sw |= up << col;
+                        if (valid && !up) dw |= 1u << col;
+                        db[col >> 3] |= (valid ? (up ? 0x2u : 0xAu) : 0u) << (4 * (col & 7));   // e2m1 +1 / -1
+                    }
+                uint8_t* drow = P.dbuf + ((size_t(g) * 2 + 1) * kM + r) * ROWB + cs * 64 + qq * 16;
+                *reinterpret_cast<uint4*>(drow) = make_uint4(db[0], db[1], db[2], db[3]);
+                P.nlx[((size_t(g) * 2 + 1) * kM + r) * 128 + cs * 4 + qq] = 0;
+                uint32_t v[16];
+#pragma unroll
+                for (int h2 = 0; h2 < 2; ++h2) {
+#pragma unroll
+                    for (int e = 0; e < 16; ++e)
+                        v[e] = __float_as_uint(P.bias_perm ? float(P.bias_perm[cs * kF4YS + qq * 32 + h2 * 16 + e]) : 0.f);
+                    tmem_st16(tmem + tl + uint32_t(qq * 32 + h2 * 16), v);
+                }
+                if (qq == 0) {
+#pragma unroll
+                    for (int e = 0; e < 16; ++e) v[e] = 0u;
+                    tmem_st16(tmem + tl + 128u, v);
+                }
+                tmem_wait_st();
+            }
+            asm volatile("fence.proxy.async.global;" ::: "memory");
+            tc_fence_before();
+            asm volatile("bar.sync 1, %0;" ::"r"(kDW * 32) : "memory");
+            if (tid == 0) flag_publish(P.flags + g * kF4Slices + cs, 1u);
+            for (int m = 0; m <= S; ++m) {
+                long long t0 = prof ? clock64() : 0;
+                if (!err_set(err)) mbar_wait(bar_h, hph & 1u, err, kErrHready);
+                ++hph;
+                tc_fence_after();
+                if (prof) { const long long t1 = clock64(); pr[0] += t1 - t0; t0 = t1; }
+                uint32_t hv[32], nv;
+                tmem_ld32(tmem + tl + uint32_t(qq * 32), hv);
+                asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];" : "=r"(nv) : "r"(tmem + tl + 128u));
+                tmem_wait_ld();
+                const int32_t nlin = int32_t(nv - nlacc_prev);
+                nlacc_prev = nv;
+                if (m >= 1 && writer && cs == 0 && qq == 0 && P.out_trace) P.out_trace[size_t(chain) * S + (m - 1)] = nlin;
+                nlin_prev = nlin;
+                if (m == S) {
+                    long long sh = 0, bs = 0;
+#pragma unroll
+                    for (int col = 0; col < 32; ++col) {
+                        const int j = col / R, k = col % R, i = k * 256 + 16 * cs + 4 * qq + j;
+                        if (i >= n) continue;
+                        const bool up = (sw >> col) & 1u;
+                        const int32_t h = __float2int_rn(__uint_as_float(hv[col]));
+                        sh += up ? h : -h;
+                        if (P.bias_perm) {
+                            const int32_t b = P.bias_perm[cs * kF4YS + qq * 32 + col];
+                            bs += up ? b : -b;
+                        }
+                        if (writer) {
+                            if (up) atomicOr(P.out_spins + size_t(chain) * 64 + (i >> 5), 1u << (i & 31));
+                            if (P.out_h) P.out_h[size_t(chain) * n + i] = h;
+                        }
+                    }
+                    if (writer) {
+                        atomicAdd(P.out_sum_sh + chain, static_cast<unsigned long long>(sh));
+                        atomicAdd(P.out_sum_bs + chain, static_cast<unsigned long long>(bs));
+                        atomicAdd(P.out_flips + chain, static_cast<unsigned long long>(flips));
+                    }
+                    continue;
+                }
+                const int t = m;
+                const int32_t fourT = __ldg(P.fourT + t), twoT = fourT >> 1, qv = __ldg(P.q + t);
+                const int32_t corr = step_corr(nlin_prev, __ldg(P.kcorr + t), __ldg(P.kconst + t));
+                const uint32_t lw = uint32_t(2 * twoT - 1);
+                const int32_t xs = qv - corr, xd = qv + corr, c1 = twoT - 1;
+                const int32_t hcl = P.hclamp;
+                uint32_t db[4] = {0u, 0u, 0u, 0u};
+                uint32_t nsw = sw, ndw = 0u;
+                int nl = 0;
+#pragma unroll
+                for (int k = 0; k < R; ++k)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const int col = j * R + k, i = k * 256 + 16 * cs + 4 * qq + j;
+                        const uint32_t u = rng_next(rng[j]);
+                        const bool valid = i < n;
+                        const bool up = (sw >> col) & 1u, dif = (dw >> col) & 1u;
+                        const int32_t h = __float2int_rn(__uint_as_float(hv[col]));
+                        int32_t hs = up ? h : -h;
+                        if (hcl > 0) hs = max(-hcl, min(hs, hcl));
+                        const int32_t zt = hs * 65536 + (dif ? xd : xs);
+                        // floor((u16 - 32768) * 4T / 65536) = mulhi((u16 - 32768) << 16, 4T)
+                        const int32_t thr = __mulhi(int32_t((u & 0xffff0000u) ^ 0x80000000u), fourT);
+                        const bool fl = valid && (zt < thr);
+                        nl += (valid && (uint32_t(zt + c1) < lw)) ? 1 : 0;
+                        if (fl) {
+                            nsw ^= 1u << col;
+                            ndw |= 1u << col;
+                            db[col >> 3] |= (up ? 0xCu : 0x4u) << (4 * (col & 7));   // e2m1 -2 / +2
+                        }
+                    }
+                flips += __popc(ndw);
+                sw = nsw;
+                dw = ndw;
+                const int par = m & 1;
+                uint8_t* drow = P.dbuf + ((size_t(g) * 2 + par) * kM + r) * ROWB + cs * 64 + qq * 16;
+                *reinterpret_cast<uint4*>(drow) = make_uint4(db[0], db[1], db[2], db[3]);
+                P.nlx[((size_t(g) * 2 + par) * kM + r) * 128 + cs * 4 + qq] = int8_t(nl);
+                asm volatile("fence.proxy.async.global;" ::: "memory");
+                tc_fence_before();
+                if (prof) { const long long t1 = clock64(); pr[1] += t1 - t0; t0 = t1; }
+                asm volatile("bar.sync 1, %0;" ::"r"(kDW * 32) : "memory");
+                if (tid == 0) flag_publish(P.flags + g * kF4Slices + cs, uint32_t(m + 2));
+                if (prof) pr[2] += clock64() - t0;
+            }
+            tc_fence_before();
+        } else if (warp < kDW + kF4PW) {
+            // ---------------- producer warps ----------------
+            const int pwid = warp - kDW;
+            const uint32_t* fl = P.flags + g * kF4Slices;
+            for (int m = -1; m < S; ++m) {
+                const int ay = (g * 2 + (m & 1)) * kM;
+                const uint32_t target = uint32_t(m + 2);
+                uint32_t ready = 0u;
+                for (int c = 0; c < kF4Chunks; ++c, ++q) {
+                    if (int(q % kF4PW) != pwid) continue;
+                    if (__shfl_sync(0xffffffffu, err_set(err) ? 1 : 0, 0)) continue;
+                    const int s = int(q % kF4Stages);
+                    const uint32_t u = q / kF4Stages;
+                    const long long w0 = prof ? clock64() : 0;
+                    if (u >= 1) {
+                        const int w = lane == 0 ? (mbar_wait(bar_empty + 8 * s, (u - 1) & 1u, err, kErrEmpty) ? 1 : 0) : 1;
+                        if (!__shfl_sync(0xffffffffu, w, 0)) continue;
+                    }
+                    const uint32_t need = c < 8 ? (3u << (2 * c)) : 0xffffu;
+                    bool ok = (ready & need) == need;
+                    if (!ok) {
+                        const uint64_t t0 = globaltimer();
+                        for (uint32_t k = 1;; ++k) {
+                            uint32_t v = 0xffffffffu;
+                            if (lane < kF4Slices)
+                                asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(fl + lane) : "memory");
+                            ready = __ballot_sync(0xffffffffu, v >= target);
+                            if ((ready & need) == need) { ok = true; break; }
+                            if ((k & 63u) == 0 && __shfl_sync(0xffffffffu, globaltimer() - t0 > kWaitNs, 0)) {
+                                if (lane == 0) atomicCAS(err, 0, kErrFlag);
+                                break;
+                            }
+                        }
+                    }
+                    if (prof) pr[7] += clock64() - w0;
+                    if (!ok) continue;
+                    if (lane == 0) {
+                        asm volatile("fence.proxy.async.global;" ::: "memory");
+                        const uint32_t dst = smem_u32(stages + size_t(s) * TILE);
+                        mbar_arrive_expect_tx(bar_full + 8 * s, TILE);
+                        if (c < 8) tma_load_2d(dst, &mapD, c * kKChunk, ay, bar_full + 8 * s);
+                        else tma_load_2d(dst, &mapNL, 0, ay, bar_full + 8 * s);
+                    }
+                    __syncwarp();
+                }
+            }
+        } else if (warp == kF4MmaWarp) {
+            // ---------------- MMA thread ----------------
+            if (lane == 0) {
+                if (!jready) {
+                    if (!err_set(err)) mbar_wait(bar_j, 0u, err, kErrJ);
+                    jready = true;
+                }
+                for (int m = -1; m < S; ++m) {
+                    const long long t0 = prof ? clock64() : 0;
+                    for (int c = 0; c < kF4Chunks; ++c, ++q) {
+                        const int s = int(q % kF4Stages);
+                        const uint32_t u = q / kF4Stages;
+                        const long long w0 = prof ? clock64() : 0;
+                        const bool ok = !err_set(err) && mbar_wait(bar_full + 8 * s, u & 1u, err, kErrFull);
+                        if (prof) pr[5] += clock64() - w0;
+                        tc_fence_after();
+                        const long long i0 = prof ? clock64() : 0;
+                        if (ok) {
+                            const uint32_t a0 = smem_u32(stages + size_t(s) * TILE);
+                            if (c < 8) {
+                                const uint32_t b0 = smem_u32(jres + c * TILE);
+#pragma unroll
+                                for (int kk = 0; kk < kKChunk / 32; ++kk)
+                                    mma_mxf4(tmem, sw128_desc(a0 + 32 * kk), sw128_desc(b0 + 32 * kk), IDESC_F4,
+                                             tmem + uint32_t(kF4SfCol), tmem + uint32_t(kF4SfCol + 32));
+                            } else {
+                                const uint32_t b0 = smem_u32(ones);
+#pragma unroll
+                                for (int kk = 0; kk < 2; ++kk)
+                                    mma_i8(tmem + 128u, sw128_desc(a0 + 32 * kk), sw128_desc(b0 + 32 * kk), IDESC_NL, 1u);
+                            }
+                        }
+                        const long long i1 = prof ? clock64() : 0;
+                        mma_commit(bar_empty + 8 * s);
+                        if (prof) { const long long i2 = clock64(); pr[9] += i1 - i0; pr[10] += i2 - i1; }
+                    }
+                    mma_commit(bar_h);
+                    if (prof) pr[6] += clock64() - t0;
+                }
+            } else {
+                q += uint32_t(S + 1) * kF4Chunks;
+            }
+            __syncwarp();
+        }
+    }
+    if (prof) {
+        long long* dst = P.prof + size_t(blockIdx.x) * kProfSlots;
+        if (warp == 0 && lane == 0) {
+            dst[0] = pr[0]; dst[1] = pr[1]; dst[2] = pr[2];
+        }
+        if (warp == kF4MmaWarp && lane == 0) {
+            dst[5] = pr[5]; dst[6] = pr[6]; dst[8] = clock64() - t_loop0; dst[9] = pr[9]; dst[10] = pr[10];
+        }
+        if (warp == kDW && lane == 0) dst[7] = pr[7];
+    }
+    __syncthreads();
+    if (warp == kF4MmaWarp) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256) : "memory");
     }
@@ -1028,13 +1407,36 @@ int tensor_build_instance(const int8_t* J, int n, TensorInstance* out, std::stri
         p[i] = cc * nc + jl * R + k;
     }
     std::vector<int8_t> Jp(size_t(np) * np, 0);
-    for (int x = 0; x < n; ++x)
-        for (int y = 0; y < n; ++y) Jp[size_t(p[y]) * np + p[x]] = J[size_t(x) * n + y];   // row = y (N), col = x (K)
+    bool unit = true;
+    int64_t rowmax = 0;
+    for (int x = 0; x < n; ++x) {
+        int64_t rs = 0;
+        for (int y = 0; y < n; ++y) {
+            const int8_t v = J[size_t(x) * n + y];
+            Jp[size_t(p[y]) * np + p[x]] = v;   // row = y (N), col = x (K)
+            rs += v < 0 ? -v : v;
+            unit = unit && v >= -1 && v <= 1;
+        }
+        rowmax = std::max(rowmax, rs);
+    }
     out->n = n;
     out->np = np;
     out->perm.assign(p.begin(), p.end());
+    out->rowsum_max = rowmax;
     cudaError_t e = cudaMalloc(&out->d_J, Jp.size());
     if (e == cudaSuccess) e = cudaMemcpy(out->d_J, Jp.data(), Jp.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && unit && R == 8) {
+        // packed e2m1, two per byte (even K index in the low nibble): +1 -> 0x2, -1 -> 0xA, 0 -> 0x0
+        std::vector<uint8_t> J4(size_t(np) * np / 2, 0);
+        for (size_t y = 0; y < size_t(np); ++y)
+            for (size_t x = 0; x < size_t(np); ++x) {
+                const int8_t v = Jp[y * np + x];
+                const uint8_t code = v > 0 ? 0x2 : (v < 0 ? 0xA : 0x0);
+                J4[(y * np + x) >> 1] |= uint8_t(code << (4 * (x & 1)));
+            }
+        e = cudaMalloc(&out->d_J4, J4.size());
+        if (e == cudaSuccess) e = cudaMemcpy(out->d_J4, J4.data(), J4.size(), cudaMemcpyHostToDevice);
+    }
     if (e != cudaSuccess) {
         if (why) *why = std::string("upload J: ") + cudaGetErrorString(e);
         return -2;
@@ -1043,7 +1445,145 @@ int tensor_build_instance(const int8_t* J, int n, TensorInstance* out, std::stri
     return 0;
 }
 
+// Largest |h| the fp4 kernel may meet is bias_absmax + rowsum_max; it stays below 2^14, where every partial sum of
+// the fp32 accumulator is an integer held exactly with 10 bits to spare.
+bool tensor_fp4_eligible(const TensorInstance* ti, int64_t bias_absmax) {
+    return ti->d_J4 != nullptr && ti->np == 2048 && ti->rowsum_max + bias_absmax < (int64_t(1) << 14);
+}
+
 namespace {
+
+// Permuted bias on the device (built once per instance from the caller's device bias) and its max |b|.
+int ensure_bias_perm(TensorInstance* ti, const int32_t* bias, std::string* why) {
+    if (!bias || ti->d_bias_perm) return 0;
+    std::vector<int32_t> b(ti->n), bp(ti->np, 0);
+    cudaError_t e = cudaMemcpy(b.data(), bias, size_t(ti->n) * 4, cudaMemcpyDeviceToHost);
+    int64_t mx = 0;
+    for (int i = 0; i < ti->n && e == cudaSuccess; ++i) {
+        bp[ti->perm[i]] = b[i];
+        mx = std::max<int64_t>(mx, b[i] < 0 ? -int64_t(b[i]) : int64_t(b[i]));
+    }
+    if (e == cudaSuccess) e = cudaMalloc(&ti->d_bias_perm, size_t(ti->np) * 4);
+    if (e == cudaSuccess) e = cudaMemcpy(ti->d_bias_perm, bp.data(), size_t(ti->np) * 4, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        if (why) *why = std::string("bias: ") + cudaGetErrorString(e);
+        return -2;
+    }
+    ti->bias_absmax = mx;
+    return 0;
+}
+
+size_t f4_smem_bytes() {
+    return 1024 + 8 * size_t(kM) * kKChunk + 2048 + size_t(kF4Stages) * kM * kKChunk + (2 * kF4Stages + 2) * 8 + 16;
+}
+
+// Concurrent group slots of the fp4 kernel (16 co-resident CTAs each).
+int f4_group_slots(int ngroups, int* out) {
+    auto fn = tensor_fp4_kernel;
+    const size_t smem = f4_smem_bytes();
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    int per_sm = 0, dev = 0, sms = 0;
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kF4Threads, smem);
+    if (e == cudaSuccess) e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return int(e);
+    *out = std::max(0, std::min(ngroups, (per_sm * sms) / kF4Slices));
+    return 0;
+}
+
+int f4_run(TensorInstance* ti, const TensorRun& r, cudaStream_t st, std::string* why) {
+    const int ngroups = (r.nchains + kM - 1) / kM;
+    int slots = 0;
+    int rc = f4_group_slots(ngroups, &slots);
+    if (rc || slots < 1) {
+        if (why) *why = "the fp4 tensor kernel cannot be co-resident on this device";
+        return -2;
+    }
+    const size_t fbytes = ((size_t(ngroups) * kF4Slices * 4 + 255) / 256) * 256;
+    const size_t dbytes = size_t(ngroups) * 2 * kM * 1024;
+    const size_t nbytes = size_t(ngroups) * 2 * kM * 128;
+    const size_t need = 256 + fbytes + dbytes + nbytes;
+    cudaError_t e = cudaSuccess;
+    if (ti->ws_bytes < need) {
+        if (ti->d_ws) cudaFree(ti->d_ws);
+        ti->d_ws = nullptr;
+        ti->ws_bytes = 0;
+        e = cudaMalloc(&ti->d_ws, need);
+        if (e != cudaSuccess) {
+            if (why) *why = std::string("workspace: ") + cudaGetErrorString(e);
+            return -2;
+        }
+        ti->ws_bytes = need;
+    }
+    uint8_t* base = static_cast<uint8_t*>(ti->d_ws);
+    int* err = reinterpret_cast<int*>(base);
+    uint32_t* flags = reinterpret_cast<uint32_t*>(base + 256);
+    uint8_t* dbuf = base + 256 + fbytes;
+    int8_t* nlx = reinterpret_cast<int8_t*>(dbuf + dbytes);
+    CUtensorMap mapD, mapNL, mapJ;
+    if (!make_map(&mapD, dbuf, 1024, uint64_t(ngroups) * 2 * kM, kM) ||
+        !make_map(&mapNL, nlx, 128, uint64_t(ngroups) * 2 * kM, kM) || !make_map(&mapJ, ti->d_J4, 1024, 2048, kF4YS)) {
+        if (why) *why = "cuTensorMapEncodeTiled failed";
+        return -2;
+    }
+    e = cudaMemsetAsync(r.out_spins, 0, size_t(r.nchains) * 64 * 4, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(r.out_sum_sh, 0, size_t(r.nchains) * 8, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(r.out_sum_bs, 0, size_t(r.nchains) * 8, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(r.out_flips, 0, size_t(r.nchains) * 8, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(base, 0, 256 + fbytes, st);     // error word + flags
+    if (e == cudaSuccess) e = cudaMemsetAsync(nlx, 0, nbytes, st);            // partial bytes 64..127 stay zero
+    if (e != cudaSuccess) {
+        if (why) *why = std::string("memset: ") + cudaGetErrorString(e);
+        return -2;
+    }
+    F4Params P{};
+    P.n = ti->n;
+    P.S = r.tab.S;
+    P.ngroups = ngroups;
+    P.fourT = r.tab.fourT;
+    P.q = r.tab.q;
+    P.kcorr = r.tab.kcorr;
+    P.kconst = r.tab.kconst;
+    P.hclamp = r.hclamp;
+    P.bias_perm = r.bias ? ti->d_bias_perm : nullptr;
+    P.seed = r.seed;
+    P.trial_offset = r.trial_offset;
+    P.nchains = r.nchains;
+    P.flags = flags;
+    P.dbuf = dbuf;
+    P.nlx = nlx;
+    P.out_spins = r.out_spins;
+    P.out_sum_sh = reinterpret_cast<unsigned long long*>(r.out_sum_sh);
+    P.out_sum_bs = reinterpret_cast<unsigned long long*>(r.out_sum_bs);
+    P.out_flips = reinterpret_cast<unsigned long long*>(r.out_flips);
+    P.out_trace = r.out_trace;
+    P.out_h = r.out_h;
+    P.err = err;
+    P.prof = r.prof;
+    auto fn = tensor_fp4_kernel;
+    const size_t smem = f4_smem_bytes();
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cfg.gridDim = dim3(kF4Slices * slots);
+    cfg.blockDim = dim3(kF4Threads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    if (e == cudaSuccess) e = cudaLaunchKernelEx(&cfg, fn, mapD, mapNL, mapJ, P);
+    if (e != cudaSuccess) {
+        if (why) *why = std::string("launch: ") + cudaGetErrorString(e);
+        return -2;
+    }
+    ti->last_err = err;
+    ti->last_kind = TENSOR_KIND_FP4;
+    ti->last_ctas = kF4Slices * slots;
+    ti->last_cluster = 1;
+    return 0;
+}
 
 int res_run(TensorInstance* ti, const TensorRun& r, cudaStream_t st, std::string* why) {
     const int npairs = ((r.nchains + kM - 1) / kM + 1) / 2;
@@ -1075,17 +1615,6 @@ int res_run(TensorInstance* ti, const TensorRun& r, cudaStream_t st, std::string
     uint32_t* flags = reinterpret_cast<uint32_t*>(base + 256);
     int8_t* dbuf = reinterpret_cast<int8_t*>(base + 256 + ((fbytes + 255) / 256) * 256);
     int8_t* nlx = dbuf + dbytes;
-    if (r.bias && !ti->d_bias_perm) {
-        std::vector<int32_t> b(ti->n), bp(2048, 0);
-        e = cudaMemcpy(b.data(), r.bias, size_t(ti->n) * 4, cudaMemcpyDeviceToHost);
-        for (int i = 0; i < ti->n && e == cudaSuccess; ++i) bp[ti->perm[i]] = b[i];
-        if (e == cudaSuccess) e = cudaMalloc(&ti->d_bias_perm, 2048 * 4);
-        if (e == cudaSuccess) e = cudaMemcpy(ti->d_bias_perm, bp.data(), 2048 * 4, cudaMemcpyHostToDevice);
-        if (e != cudaSuccess) {
-            if (why) *why = std::string("bias: ") + cudaGetErrorString(e);
-            return -2;
-        }
-    }
     CUtensorMap mapD, mapNL, mapJ;
     if (!make_map(&mapD, dbuf, 2048, uint64_t(ngroups) * 2 * kM, kM) ||
         !make_map(&mapNL, nlx, 128, uint64_t(ngroups) * 2 * kM, kM) || !make_map(&mapJ, ti->d_J, 2048, 2048, kResYS)) {
@@ -1144,6 +1673,9 @@ int res_run(TensorInstance* ti, const TensorRun& r, cudaStream_t st, std::string
         return -2;
     }
     ti->last_err = err;
+    ti->last_kind = TENSOR_KIND_INT8;
+    ti->last_ctas = kResSlices * slots;
+    ti->last_cluster = 1;
     return 0;
 }
 
@@ -1151,6 +1683,14 @@ int res_run(TensorInstance* ti, const TensorRun& r, cudaStream_t st, std::string
 
 int tensor_run(TensorInstance* ti, const TensorRun& r, cudaStream_t st, std::string* why) {
     const int np = ti->np, R = np / 256;
+    int rc0 = ensure_bias_perm(ti, r.bias, why);
+    if (rc0) return rc0;
+    const bool fp4 = tensor_fp4_eligible(ti, r.bias ? ti->bias_absmax : 0);
+    if (r.kind == TENSOR_KIND_FP4 && !fp4) {
+        if (why) *why = "the fp4 kernel needs NP = 2048, |J| <= 1 and max|b| + max_y sum_x |J_xy| < 16384";
+        return -1;
+    }
+    if (fp4 && r.kind != TENSOR_KIND_INT8) return f4_run(ti, r, st, why);
     if (R == 8) return res_run(ti, r, st, why);
     const int groups = (r.nchains + kM - 1) / kM;
     // workspace: exchange buffers, permuted bias, error word
@@ -1171,18 +1711,6 @@ int tensor_run(TensorInstance* ti, const TensorRun& r, cudaStream_t st, std::str
     int8_t* dbuf = static_cast<int8_t*>(ti->d_ws);
     int32_t* nlbuf = reinterpret_cast<int32_t*>(static_cast<uint8_t*>(ti->d_ws) + dbytes);
     int* err = reinterpret_cast<int*>(static_cast<uint8_t*>(ti->d_ws) + dbytes + nlbytes);
-    if (r.bias && !ti->d_bias_perm) {
-        // permuted bias (host copy of the caller's device bias)
-        std::vector<int32_t> b(ti->n), bp(np, 0);
-        e = cudaMemcpy(b.data(), r.bias, size_t(ti->n) * 4, cudaMemcpyDeviceToHost);
-        for (int i = 0; i < ti->n && e == cudaSuccess; ++i) bp[ti->perm[i]] = b[i];
-        if (e == cudaSuccess) e = cudaMalloc(&ti->d_bias_perm, size_t(np) * 4);
-        if (e == cudaSuccess) e = cudaMemcpy(ti->d_bias_perm, bp.data(), size_t(np) * 4, cudaMemcpyHostToDevice);
-        if (e != cudaSuccess) {
-            if (why) *why = std::string("bias: ") + cudaGetErrorString(e);
-            return -2;
-        }
-    }
     CUtensorMap mapA, mapB;
     if (!make_map(&mapA, dbuf, uint64_t(np), uint64_t(groups) * 2 * kM, kM) ||
         !make_map(&mapB, ti->d_J, uint64_t(np), uint64_t(np), uint32_t(16 * R))) {
@@ -1230,6 +1758,9 @@ int tensor_run(TensorInstance* ti, const TensorRun& r, cudaStream_t st, std::str
     else if (R == 16) rc = launch_t<16>(P, groups, mapA, mapB, st, why);
     if (rc) return rc;
     ti->last_err = err;
+    ti->last_kind = TENSOR_KIND_INT8;
+    ti->last_ctas = kC * groups;
+    ti->last_cluster = kC;
     return 0;
 }
 
@@ -1254,6 +1785,8 @@ void tensor_free_instance(TensorInstance* ti) {
     if (ti->d_J) cudaFree(ti->d_J);
     if (ti->d_ws) cudaFree(ti->d_ws);
     if (ti->d_bias_perm) cudaFree(ti->d_bias_perm);
+    if (ti->d_J4) cudaFree(ti->d_J4);
+    ti->d_J4 = nullptr;
     ti->d_J = nullptr;
     ti->d_ws = nullptr;
     ti->d_bias_perm = nullptr;

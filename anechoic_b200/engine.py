@@ -191,6 +191,7 @@ class RunResult:
     fields: Optional[np.ndarray] = None
     device_ms: float = 0.0
     profile: Optional[dict] = None
+    kernel: Optional[str] = None     # "plain", "tensor-int8" or "tensor-fp4"
 
     def cuts(self, sumw: int) -> np.ndarray:
         """Device cut = (sumw + sum_sh / 2) / 2 with C++ truncating division (sca_ref.hpp:153)."""
@@ -208,9 +209,11 @@ def tdiv(a, b: int):
 
 
 def run(dev: DeviceInstance, tb: Tables, seed: int, trial_offset: int, nchains: int, trace: bool = False,
-        fields: bool = False, engine: str = "auto", wide="auto", profile: bool = False) -> RunResult:
+        fields: bool = False, engine: str = "auto", wide="auto", profile: bool = False,
+        tensor_kind: str = "auto") -> RunResult:
     """nchains anneals (trial ids trial_offset .. trial_offset + nchains - 1) in one launch. profile=True records
-    the tensor engine's per-phase cycle counters (RunResult.profile)."""
+    the tensor engine's per-phase cycle counters (RunResult.profile); tensor_kind picks the tensor engine's operand
+    format ("auto", "int8", "fp4")."""
     L = load()
     n = dev.n
     W = spin_words(n)
@@ -219,7 +222,7 @@ def run(dev: DeviceInstance, tb: Tables, seed: int, trial_offset: int, nchains: 
     S = tb.S
     tr = np.zeros((nchains, S), np.int32) if trace else None
     hf = np.zeros((nchains, n), np.int32) if fields else None
-    o = _lib.opts(engine, wide, profile)
+    o = _lib.opts(engine, wide, profile, tensor_kind)
     args = (dev._h, tb._h, C.c_uint64(seed), C.c_uint32(trial_offset), nchains, C.byref(o), spins.ctypes.data,
             sh.ctypes.data, bs.ctypes.data, fl.ctypes.data, tr.ctypes.data if trace else None)
     if fields:
@@ -227,7 +230,7 @@ def run(dev: DeviceInstance, tb: Tables, seed: int, trial_offset: int, nchains: 
     else:
         check(L.anc_run(*args))
     res = RunResult(n=n, trial_offset=trial_offset, spins=spins, sum_sh=sh, sum_bs=bs, flips=fl, trace=tr, fields=hf,
-                    device_ms=L.anc_last_device_ms())
+                    device_ms=L.anc_last_device_ms(), kernel=_lib.last_kernel())
     if profile:
         res.profile = _lib.last_profile()
     return res

@@ -8,7 +8,8 @@ Target cut: 0.995 x the best cut of 1000 long anneals (S = 5000, same correction
 exact engine outside the timed region. TTS99: primary t_batch ln(0.01)/ln(1 - P_batch), secondary
 t_batch ln(0.01)/(B ln(1 - p)) (reference estimators, gpu/onsager_v2_20261007/src/analyze.py:15-47).
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--engine auto|plain|tensor] [--impl ours|reference]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--engine auto|plain|tensor] [--tensor-kind auto|int8|fp4]
+                  [--impl ours|reference]
 
 --impl reference times the reference's own CPU golden model (sca::run_trial_bias compiled unmodified into
 oracle/_ref/libscaref.so) on all host threads over a bounded sample of the same workload.
@@ -193,6 +194,35 @@ def cpu_baseline_sample(budget_s: float = 15.0):
 
 
 # ------------------------------------------------------------------------------------------------------ our arm
+KERNEL_NAMES = {"plain": "plain_kernel", "tensor-int8": "tensor_res_kernel", "tensor-fp4": "tensor_fp4_kernel"}
+
+
+def roofline(kernel: str, t_launch_ms: float, B: int, S: int, mean_flips: float, np_pad: int):
+    """Roofline of the dominant kernel for one launch of B anneals x S steps.
+    plain: algorithmic bytes = B x (flipped rows x ceil(N/8) B of 1-bit couplings + S x (8 N B of fields + N/4 B of
+    spin bits)), against the measured HBM copy bandwidth (J is L2-resident, so HBM is a lower bound of the roof).
+    tensor: dense contraction ops = 2 x NP^2 x B x (S + 1) (every column of dS, the initial field included), against
+    the sm_100 dense rate of the operand format relative to the measured bf16 GEMM: int8 2x, fp4 (e2m1) 4x."""
+    hbm, bf16, peak_kind = measured_peaks()
+    if kernel == "plain":
+        alg = B * (mean_flips * math.ceil(N_SPINS / 8) + S * (8 * N_SPINS + N_SPINS / 4))
+        ach = alg / (t_launch_ms / 1000.0) / 1e9
+        return {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                "traffic": profile_traffic(KERNEL_NAMES[kernel]), "peak_kind": peak_kind,
+                "algorithmic_per_launch": alg, "kernel": KERNEL_NAMES[kernel],
+                "note": "bit-column algorithmic bytes; J is L2-resident so the HBM copy peak is a lower bound of the roof"}
+    mult = 4.0 if kernel == "tensor-fp4" else 2.0
+    ops = 2.0 * np_pad * np_pad * B * (S + 1)
+    ach = ops / (t_launch_ms / 1000.0) / 1e12
+    peak = mult * bf16
+    return {"bound": "tensor", "achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak,
+            "traffic": profile_traffic(KERNEL_NAMES[kernel]), "peak_kind": f"{peak_kind} bf16 x {mult:g}",
+            "algorithmic_per_launch": ops, "kernel": KERNEL_NAMES[kernel],
+            "useful_fraction": mean_flips / (N_SPINS * S),
+            "note": f"{'fp4' if mult == 4 else 'int8'} dense ops (tera-ops/s), 2 NP^2 per replica-step; peak = "
+                    f"{mult:g} x measured bf16 GEMM (sm_100 dense rate ratio)"}
+
+
 def bench_ours(args, ws, rank, local):
     import numpy as np
     import torch
@@ -211,15 +241,14 @@ def bench_ours(args, ws, rank, local):
     dev = A.DeviceInstance(inst)
     sumw = dev.info["sumw"]
     tb = A.Tables.from_schedule(A.Schedule(**SCHED))
-    engine = args.engine
+    engine, kind = args.engine, args.tensor_kind
 
     # target cut (outside the timed region): best of 1000 long anneals on the exact engine
     ttb = A.Tables.from_schedule(A.Schedule(**TARGET_SCHED))
-    tr = A.run(dev, ttb, RUN_SEED, 0xE0000000, TARGET_ANNEALS, engine=engine)
+    tr = A.run(dev, ttb, RUN_SEED, 0xE0000000, TARGET_ANNEALS, engine=engine, tensor_kind=kind)
     best = int(tr.cuts(sumw).max())
     target = math.ceil(0.995 * best)
 
-    # device-resident outputs for the timed loop
     W = A.spin_words(N_SPINS)
     d_sp = torch.empty((CHAINS, W), dtype=torch.int64, device="cuda")
     d_sh = torch.empty(CHAINS, dtype=torch.int64, device="cuda")
@@ -227,63 +256,85 @@ def bench_ours(args, ws, rank, local):
     d_fl = torch.empty(CHAINS, dtype=torch.int64, device="cuda")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.int32, device="cuda")   # > L2 (126 MB)
     L = _lib.load()
-    o = _lib.opts(engine)
     stream = torch.cuda.current_stream()
     trial_base = rank << 20
 
-    def launch(step):
-        _lib.check(L.anc_run_device(dev._h, tb._h, RUN_SEED, trial_base + step * CHAINS, CHAINS, o,
-                                    d_sp.data_ptr(), d_sh.data_ptr(), d_bs.data_ptr(), d_fl.data_ptr(), None,
-                                    stream.cuda_stream))
+    def timed(eng, knd, steps, warmup, clocks=False):
+        """Device-timed launches (inputs resident, outputs on the device); returns per-launch ms and the kernel."""
+        o = _lib.opts(eng, tensor_kind=knd)
 
-    for w in range(args.warmup):
-        launch(1000 + w)
-    torch.cuda.synchronize()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    succ_batches, succ, flips_total = 0, 0, 0
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(dev_index) as clk:
-        for k in range(args.steps):
+        def launch(step):
+            _lib.check(L.anc_run_device(dev._h, tb._h, RUN_SEED, trial_base + step * CHAINS, CHAINS, o,
+                                        d_sp.data_ptr(), d_sh.data_ptr(), d_bs.data_ptr(), d_fl.data_ptr(), None,
+                                        stream.cuda_stream))
+
+        for w in range(warmup):
+            launch(1000 + w)
+        torch.cuda.synchronize()
+        kernel = _lib.last_kernel()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        clk = ClockSampler(dev_index) if clocks else None
+        if clk:
+            clk.__enter__()
+        for k in range(steps):
             flush.fill_(k)                         # L2 flush between timed iterations (not timed)
             ev[k][0].record(stream)
             launch(k)
             ev[k][1].record(stream)
         torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    ms = [a.elapsed_time(b) for a, b in ev]
-    # success statistics of the timed batches (rerun readback: results of the last batch are on the device; recompute
-    # all batches' cuts through the host API so that every timed batch is scored)
-    for k in range(args.steps):
-        r = A.run(dev, tb, RUN_SEED, trial_base + k * CHAINS, CHAINS, engine=engine)
-        c = r.cuts(sumw)
-        s = int((c >= target).sum())
-        succ += s; succ_batches += int(s > 0); flips_total += int(r.flips.sum())
-    t_batch_ms = sum(ms) / len(ms)
-    if dist:
-        t = torch.tensor([t_batch_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_batch_ms = float(t.item())
+        if clk:
+            clk.__exit__(None, None, None)
+        if dist:
+            dist.barrier()
+        return [a.elapsed_time(b) for a, b in ev], kernel, clk
 
-    # e2e: the same batch through the public C ABI with host outputs (tables uploaded from host each step,
-    # results read back to host each step)
-    fourT_np = tb.arrays()
+    def scored(eng, knd, steps):
+        """Success statistics of the timed batches, recomputed through the host API (same trial ids)."""
+        succ, succ_batches, flips_total = 0, 0, 0
+        for k in range(steps):
+            r = A.run(dev, tb, RUN_SEED, trial_base + k * CHAINS, CHAINS, engine=eng, tensor_kind=knd)
+            c = r.cuts(sumw)
+            s_ = int((c >= target).sum())
+            succ += s_; succ_batches += int(s_ > 0); flips_total += int(r.flips.sum())
+        return succ, succ_batches, flips_total
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    ms, kernel, clk = timed(engine, kind, args.steps, args.warmup, clocks=True)
+    t_batch_ms = max_over_ranks(sum(ms) / len(ms))
+    succ, succ_batches, flips_total = scored(engine, kind, args.steps)
+
+    # the plain (bit-column) engine on the same batches, for the batched-vs-plain comparison of the metric
+    plain = None
+    if kernel != "plain" and not args.no_plain:
+        pms, _, _ = timed("plain", "auto", args.steps, args.warmup)
+        p_ms = max_over_ranks(sum(pms) / len(pms))
+        p_succ, p_sb, _ = scored("plain", "auto", args.steps)
+        plain = {"anneals_per_s": CHAINS * ws / (p_ms / 1000.0), "ms_per_step": p_ms,
+                 "tts99_us_primary": 1000.0 * tts99(p_sb / args.steps, p_ms),
+                 "tts99_us_secondary": 1000.0 * tts99_secondary(p_succ / (CHAINS * args.steps), CHAINS, p_ms)}
+
+    # e2e: the same batch through the public C ABI with host buffers -- schedule tables uploaded from host memory
+    # and results (spins, sum s*h, sum b*s, flips) read back to host memory inside every timed step
+    arrays = tb.arrays()
     e2e_ms = []
     torch.cuda.synchronize()
     for k in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        tbk = A.Tables.from_arrays(**fourT_np)
-        r = A.run(dev, tbk, RUN_SEED, trial_base + k * CHAINS, CHAINS, engine=engine)
+        tbk = A.Tables.from_arrays(**arrays)
+        A.run(dev, tbk, RUN_SEED, trial_base + k * CHAINS, CHAINS, engine=engine, tensor_kind=kind)
         dt = time.perf_counter() - t0
         if k >= args.warmup:
             e2e_ms.append(1000.0 * dt)
-    e2e_t = sum(e2e_ms) / len(e2e_ms)
-    if dist:
-        t = torch.tensor([e2e_t], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_t = float(t.item())
+    e2e_t = max_over_ranks(sum(e2e_ms) / len(e2e_ms))
     h2d = SCHED["S"] * (4 + 4 + 8 + 4)
     d2h = CHAINS * (W * 8 + 8 * 3)
 
@@ -294,31 +345,26 @@ def bench_ours(args, ws, rank, local):
     S = SCHED["S"]
     anneals = CHAINS * ws
     value = anneals / (t_batch_ms / 1000.0)
-    B = CHAINS
-    nb = args.steps
+    B, nb = CHAINS, args.steps
     P_batch = succ_batches / nb
     p = succ / (B * nb)
-    # roofline: algorithmic bytes of the bit-column update per launch (flipped rows x ceil(N/8) bytes, K = 1) plus
-    # fields (8 B/spin/step) and spins (N/4 B/step), per anneal-step, summed over the batch
-    mean_flips = flips_total / (B * nb)              # per anneal (whole schedule)
-    alg_bytes = B * (mean_flips * math.ceil(N_SPINS / 8) + S * (8 * N_SPINS + N_SPINS / 4))
-    hbm, _, peak_kind = measured_peaks()
-    achieved = alg_bytes / (t_batch_ms / 1000.0) / 1e9
+    mean_flips = flips_total / (B * nb)
     line = {
         "metric": METRIC, "value": value, "unit": "anneals/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_batch_ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "vs_baseline": None, "dtype": "int32" if kernel == "plain" else ("fp4-e2m1/f32" if kernel == "tensor-fp4"
+                                                                         else "int8/int32"),
+        "data": "synthetic",
         "config": {"workload": f"N={N_SPINS} +-1 complete graph (seed {INSTANCE_SEED}), {CHAINS} concurrent anneals "
                                f"per GPU, S={S} counted Onsager lambda 1.05 ramp, t0 30 t1 5 q 4",
-                   "engine": engine, "n": N_SPINS, "anneals_per_gpu": CHAINS, "S": S, "l2": "flushed between steps",
-                   "parallelism": f"replicas x{ws}"},
+                   "engine": engine, "kernel": kernel, "n": N_SPINS, "anneals_per_gpu": CHAINS, "S": S,
+                   "l2": "flushed between steps", "parallelism": f"replicas x{ws}"},
         "tts99_us": {"primary": 1000.0 * tts99(P_batch, t_batch_ms), "secondary": 1000.0 * tts99_secondary(p, B, t_batch_ms),
                      "target_cut": target, "best_cut": best, "p": p, "P_batch": P_batch, "t_batch_us": 1000 * t_batch_ms},
+        "plain_engine": plain,
         "us_per_anneal_step": 1000.0 * t_batch_ms / S, "ns_per_chain_step": 1e6 * t_batch_ms / (S * B),
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": profile_traffic(f"plain_{engine}"), "peak_kind": peak_kind,
-                     "note": "bit-column algorithmic bytes; J is L2-resident so the HBM copy peak is a lower bound "
-                             "of the roof"},
+        "ms_per_step_spread": [min(ms), max(ms)],
+        "roofline": roofline(kernel, t_batch_ms, B, S, mean_flips, L.anc_np(N_SPINS)),
         "e2e": {"value": anneals / (e2e_t / 1000.0), "unit": "anneals/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_t},
         "gpu_launches": args.steps,
@@ -339,7 +385,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--engine", default="auto", choices=["auto", "plain", "tensor"])
+    ap.add_argument("--tensor-kind", default="auto", choices=["auto", "int8", "fp4"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain-engine comparison run")
     args = ap.parse_args()
     ws, rank, local = dist_env()
     if args.impl == "reference":

@@ -39,6 +39,11 @@ extern "C" {
 #define ANC_ENGINE_PLAIN 1  /* bit-column engine: one CTA per anneal, bit-packed couplings, flipped columns only */
 #define ANC_ENGINE_TENSOR 2 /* batched engine: replicas sharing J, tcgen05 int8 J * dS update */
 
+#define ANC_TENSOR_AUTO 0   /* fp4 when exact for the instance (NP = 2048, |J| <= 1, small fields), else int8 */
+#define ANC_TENSOR_INT8 1   /* tcgen05.mma kind::i8, int32 accumulation (any K) */
+#define ANC_TENSOR_FP4 2    /* tcgen05.mma kind::mxf4 on packed e2m1 with unit block scales, fp32 accumulation;
+                              exact because J in {-1,0,1}, dS in {0,+-1,+-2} and |h| < 2^14 (EINVAL otherwise) */
+
 typedef struct anc_instance anc_instance;
 typedef struct anc_tables anc_tables;
 
@@ -104,14 +109,16 @@ typedef struct {
     int wide;        /* -1 auto (clamp only if the plan needs it), 0 never (EINVAL if needed), 1 always */
     int threads;     /* host threads for rescoring; 0 = default */
     int profile;     /* 1: record per-phase cycle counters of the tensor engine (anc_last_profile) */
-    int reserved[4];
+    int tensor_kind; /* ANC_TENSOR_*: operand format of the tensor engine's field update */
+    int reserved[3];
 } anc_run_opts;
 
 /* Phase profile of the calling thread's last synchronous tensor-engine run with opts.profile = 1 (the counterpart
  * of the reference's SCA_PROFILE build, sca_gpu.cu:163-168): out[0..8] = mean SM cycles per step of
  *   0 wait for fields, 1 TMEM load + decide + update store, 2 n_lin publish, 3 cluster barrier, 4 n_lin read,
  *   5 MMA waiting for TMA, 6 MMA phase (barrier to last commit), 7 TMA waiting for free stages, 8 whole step;
- * out[9] = CTAs, out[10] = CTAs per cluster, out[11] = co-resident clusters. Returns the count written (<= max). */
+ * out[9] = CTAs, out[10] = CTAs per cluster, out[11] = co-resident clusters, out[12] = MMA issue, out[13] = MMA
+ * commits (cycles per step). Returns the count written (<= max). */
 ANC_API int anc_last_profile(double* out, int max);
 
 /* Replaces one launch + readback of sca_gpu / sca_gpu_bias (sca_gpu.cu:699-713, sca_gpu_bias.cu:716-733) and
@@ -200,6 +207,12 @@ ANC_API int anc_run_batch_noalloc(int njobs, const anc_device_job* jobs, void* s
 
 /* Last device time of a synchronous run on this thread (ms, CUDA events around the launch). */
 ANC_API double anc_last_device_ms(void);
+
+/* Kernel used by this thread's last anc_run / anc_run_fields / anc_run_device: ANC_KERNEL_* (0 if none yet). */
+#define ANC_KERNEL_PLAIN 1        /* bit-column engine */
+#define ANC_KERNEL_TENSOR_INT8 2  /* tcgen05 kind::i8 engine */
+#define ANC_KERNEL_TENSOR_FP4 3   /* tcgen05 kind::mxf4 engine */
+ANC_API int anc_last_kernel(void);
 
 /* Message of the calling thread's last failure ("" if none). */
 ANC_API const char* anc_last_error(void);
