@@ -117,7 +117,9 @@ def opts(engine: str = "auto", wide="auto", profile: bool = False, tensor_kind: 
 
 PROFILE_FIELDS = ("wait_fields", "decide", "nlin_publish", "cluster_barrier", "nlin_read", "mma_wait_tma",
                   "mma_phase", "tma_wait_stage", "step", "ctas", "cluster", "max_active_clusters", "mma_issue",
-                  "mma_commit")
+                  "mma_commit", "first_tile_after_publish", "last_tile_after_publish", "nlin_tile_after_publish",
+                  "fields_commit_after_publish", "tile0_flags_after_publish", "tile7_flags_after_publish",
+                  "tile0_tma_after_publish", "tile7_tma_after_publish")
 
 
 def last_kernel():
@@ -127,6 +129,6 @@ def last_kernel():
 
 def last_profile() -> dict:
     """Phase profile (SM cycles per step) of this thread's last profiled tensor-engine run."""
-    buf = (C.c_double * 14)()
-    k = load().anc_last_profile(buf, 14)
+    buf = (C.c_double * len(PROFILE_FIELDS))()
+    k = load().anc_last_profile(buf, len(PROFILE_FIELDS))
     return {PROFILE_FIELDS[i]: buf[i] for i in range(k)}

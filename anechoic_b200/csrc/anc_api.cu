@@ -313,8 +313,8 @@ int run_device_impl(anc_instance* I, anc_tables* tb, uint64_t seed, uint32_t off
             anc::TensorGeometry geo;
             if (anc::tensor_geometry(I->n, nchains, &geo) != 0) return fail(ANC_ECUDA, "tensor geometry query failed");
             const int ctas = std::max(geo.ctas, 16 * ((nchains + 127) / 128));
-            CK(I->w_prof.ensure(size_t(ctas) * 16));
-            CK(cudaMemsetAsync(I->w_prof.p, 0, size_t(ctas) * 16 * sizeof(long long), st));
+            CK(I->w_prof.ensure(size_t(ctas) * anc::kTensorProfSlots));
+            CK(cudaMemsetAsync(I->w_prof.p, 0, size_t(ctas) * anc::kTensorProfSlots * sizeof(long long), st));
             r.prof = I->w_prof.p;
             I->prof_ctas = ctas;
             I->prof_S = tb->S;
@@ -367,13 +367,14 @@ int run_host_impl(anc_instance* I, anc_tables* tb, uint64_t seed, uint32_t off, 
         if (rc) return fail(ANC_ECUDA, "tensor engine: %s", why.c_str());
     }
     if (I->prof_ctas > 0) {
-        std::vector<long long> h(size_t(I->prof_ctas) * 16);
+        const size_t ns = anc::kTensorProfSlots;
+        std::vector<long long> h(size_t(I->prof_ctas) * ns);
         CK(cudaMemcpy(h.data(), I->w_prof.p, h.size() * sizeof(long long), cudaMemcpyDeviceToHost));
-        g_prof.assign(14, 0.0);
-        const int slot_of[11] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 12, 13};   // phase slot -> output index
-        for (int s = 0; s < 11; ++s) {
+        g_prof.assign(22, 0.0);
+        const int slot_of[19] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 12, 13, 14, 15, 16, 17, 18, 19, 20, 21};   // slot -> output
+        for (int s = 0; s < 19; ++s) {
             double acc = 0;
-            for (int b = 0; b < I->prof_ctas; ++b) acc += double(h[size_t(b) * 16 + s]);
+            for (int b = 0; b < I->prof_ctas; ++b) acc += double(h[size_t(b) * ns + s]);
             g_prof[slot_of[s]] = acc / I->prof_ctas / std::max(1, I->prof_S);
         }
         anc::TensorGeometry geo;

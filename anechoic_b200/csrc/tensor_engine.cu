@@ -70,9 +70,13 @@ struct TensorParams {
 
 // opt-in phase profile (clock64 cycles summed over the steps, per CTA):
 //   0 decision warps waiting for h   1 TMEM load + decide + D store   2 named barrier + n_lin publish
-//   3 cluster barrier (decision warps)   4 n_lin read   5 MMA thread waiting for TMA stages
-//   6 MMA thread: barrier end -> last commit issued   7 TMA thread waiting for free stages   8 whole step loop
-constexpr int kProfSlots = 16;
+//   3 cluster barrier (decision warps; fp4 kernel: flag publish alone)   4 n_lin read (fp4 kernel: fields ready
+//     minus own publish)   5 MMA thread waiting for TMA stages   6 MMA thread: barrier end -> last commit issued
+//   7 TMA thread waiting for free stages   8 whole step loop   9 MMA issue   10 MMA commits
+//   fp4 kernel, measured from this CTA's own publish: 11 first D tile in shared memory, 12 last D tile, 13 n_lin
+//     tile, 14 fields-ready commit issued, 15 / 16 flags of D tile 0 / 7 seen by the producer, 17 / 18 TMA of D tile
+//     0 / 7 issued
+constexpr int kProfSlots = kTensorProfSlots;
 
 // ------------------------------------------------------------------------------------------------ PTX helpers
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return uint32_t(__cvta_generic_to_shared(p)); }
@@ -115,24 +119,14 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int* er
     }
 }
 
-// Bounded wait until the 32-bit flag at `p` (global, written with release semantics) reaches `target`.
-__device__ __forceinline__ bool flag_wait(const uint32_t* p, uint32_t target, int* err, int code) {
-    uint32_t v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    if (v >= target) return true;
-    const uint64_t t0 = globaltimer();
-    for (uint32_t k = 1;; ++k) {
-        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-        if (v >= target) return true;
-        if ((k & 255u) == 0 && globaltimer() - t0 > kWaitNs) {
-            atomicCAS(err, 0, code);
-            return false;
-        }
-    }
-}
-
 __device__ __forceinline__ void flag_publish(uint32_t* p, uint32_t v) {
     asm volatile("fence.acq_rel.gpu;\n\tst.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Release store alone: the writes of the CTA's other threads are ordered before it by the preceding bar.sync, and
+// release is cumulative over them.
+__device__ __forceinline__ void flag_release(uint32_t* p, uint32_t v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
 __device__ __forceinline__ bool err_set(const int* err) { return *reinterpret_cast<const volatile int*>(err) != 0; }
@@ -893,7 +887,7 @@ __global__ void __launch_bounds__(kResThreads, 1)
 //     against a ones row into an int32 n_lin accumulator.
 constexpr int kF4Slices = 16;
 constexpr int kF4YS = 128;
-constexpr int kF4PW = 4;
+constexpr int kF4PW = 3;               // producer warps (20 warps in all: 96 registers per thread)
 constexpr int kF4Stages = 5;
 constexpr int kF4MmaWarp = kDW + kF4PW;
 constexpr int kF4Threads = (kDW + kF4PW + 1) * 32;
@@ -943,6 +937,35 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
         : "r"(taddr));
 }
 
+// One decision pass of a thread's 32 columns (column = 8 j + k: RNG lane j of the thread, round k), interleaving the
+// four lanes' streams. Outputs the flip mask and the mask of slots inside the linear band -2T < z < 2T.
+//   s*h: the field in f32 with its sign flipped for s = -1 (bit 31 of ~sw), clamped when the range plan asks;
+//   z = s*h*65536 + q -/+ corr through the exact conversion 1.5*2^23 + x (|x| < 2^22): the low 16 bits of that
+//   encoding are x, so encoding << 16 = x * 65536 modulo 2^32;
+//   r = floor((u16 - 32768) * 4T / 65536) = mulhi((u16 - 32768) << 16, 4T).
+template <bool CLAMP>
+__device__ __forceinline__ void f4_decide(Xoshiro (&rng)[4], const uint32_t (&hv)[32], uint32_t downs, uint32_t dw,
+                                          int32_t xs, int32_t twocorr, int32_t fourT, int32_t c1, uint32_t lw,
+                                          float hclf, uint32_t& fm, uint32_t& lm) {
+    fm = 0u;
+    lm = 0u;
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int col = j * 8 + k;
+            const uint32_t u = rng_next(rng[j]);
+            float hsf = __uint_as_float(hv[col] ^ ((downs << (31 - col)) & 0x80000000u));
+            if (CLAMP) hsf = fminf(fmaxf(hsf, -hclf), hclf);
+            const int32_t zb = __float_as_int(hsf + 12582912.0f);
+            int32_t zt = (zb << 16) + xs;
+            if ((dw >> col) & 1u) zt += twocorr;
+            const int32_t thr = __mulhi(int32_t((u & 0xffff0000u) ^ 0x80000000u), fourT);
+            if (zt < thr) fm |= 1u << col;
+            if (uint32_t(zt + c1) < lw) lm |= 1u << col;
+        }
+}
+
 __global__ void __launch_bounds__(kF4Threads, 1)
     tensor_fp4_kernel(const __grid_constant__ CUtensorMap mapD, const __grid_constant__ CUtensorMap mapNL,
                       const __grid_constant__ CUtensorMap mapJ, const __grid_constant__ F4Params P) {
@@ -958,6 +981,7 @@ __global__ void __launch_bounds__(kF4Threads, 1)
     uint8_t* stages = ones + 2048;
     uint64_t* bars = reinterpret_cast<uint64_t*>(stages + kF4Stages * TILE);   // full[5], empty[5], hready, jbar
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kF4Stages + 2);
+    __shared__ volatile long long s_pub[2];      // profiling: clock64 of this CTA's flag publish, by step parity
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int cs = int(blockIdx.x % kF4Slices);
@@ -1009,7 +1033,7 @@ __global__ void __launch_bounds__(kF4Threads, 1)
     uint32_t hph = 0u, q = 0;
     bool jready = false;
     const bool prof = P.prof != nullptr;
-    long long pr[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    long long pa = 0, pb = 0, pc = 0, pd = 0;   // phase cycle totals; meaning depends on the warp's role
     const long long t_loop0 = clock64();
 
     for (int g = gs0; g < P.ngroups; g += gstride) {
@@ -1018,7 +1042,7 @@ __global__ void __launch_bounds__(kF4Threads, 1)
             const int chain = g * kM + r;
             const bool writer = chain < P.nchains;
             Xoshiro rng[4];
-            uint32_t sw = 0u, dw = 0u, nlacc_prev = 0u;
+            uint32_t sw = 0u, dw = 0u, vmask = 0u, nlacc_prev = 0u;
             int32_t nlin_prev = 0;
             long long flips = 0;
             {
@@ -1034,6 +1058,7 @@ __global__ void __launch_bounds__(kF4Threads, 1)
                         const bool valid = i < n;
                         const uint32_t up = valid ? (rv >> 31) : 1u;
                         sw |= up << col;
+                        if (valid) vmask |= 1u << col;
                         if (valid && !up) dw |= 1u << col;
                         db[col >> 3] |= (valid ? (up ? 0x2u : 0xAu) : 0u) << (4 * (col & 7));   // e2m1 +1 / -1
                     }
@@ -1058,13 +1083,24 @@ __global__ void __launch_bounds__(kF4Threads, 1)
             asm volatile("fence.proxy.async.global;" ::: "memory");
             tc_fence_before();
             asm volatile("bar.sync 1, %0;" ::"r"(kDW * 32) : "memory");
-            if (tid == 0) flag_publish(P.flags + g * kF4Slices + cs, 1u);
+            if (tid == 0) flag_release(P.flags + g * kF4Slices + cs, 1u);
+            const float hclf = float(P.hclamp);
+            long long last_pub = 0, p_pub = 0, p_wake = 0;   // profiling (thread 0): publish cost, wake - publish
             for (int m = 0; m <= S; ++m) {
                 long long t0 = prof ? clock64() : 0;
+                // this step's table entries, loaded before the wait for the fields
+                const int t = m < S ? m : S - 1;
+                const int32_t fourT = __ldg(P.fourT + t), qv = __ldg(P.q + t), kconst = __ldg(P.kconst + t);
+                const int64_t kcorr = __ldg(P.kcorr + t);
                 if (!err_set(err)) mbar_wait(bar_h, hph & 1u, err, kErrHready);
                 ++hph;
                 tc_fence_after();
-                if (prof) { const long long t1 = clock64(); pr[0] += t1 - t0; t0 = t1; }
+                if (prof) {
+                    const long long t1 = clock64();
+                    pa += t1 - t0;
+                    t0 = t1;
+                    if (m >= 1) p_wake += t1 - last_pub;
+                }
                 uint32_t hv[32], nv;
                 tmem_ld32(tmem + tl + uint32_t(qq * 32), hv);
                 asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];" : "=r"(nv) : "r"(tmem + tl + 128u));
@@ -1098,56 +1134,58 @@ __global__ void __launch_bounds__(kF4Threads, 1)
                     }
                     continue;
                 }
-                const int t = m;
-                const int32_t fourT = __ldg(P.fourT + t), twoT = fourT >> 1, qv = __ldg(P.q + t);
-                const int32_t corr = step_corr(nlin_prev, __ldg(P.kcorr + t), __ldg(P.kconst + t));
+                const int32_t twoT = fourT >> 1;
+                const int32_t corr = step_corr(nlin_prev, kcorr, kconst);
                 const uint32_t lw = uint32_t(2 * twoT - 1);
-                const int32_t xs = qv - corr, xd = qv + corr, c1 = twoT - 1;
-                const int32_t hcl = P.hclamp;
-                uint32_t db[4] = {0u, 0u, 0u, 0u};
-                uint32_t nsw = sw, ndw = 0u;
-                int nl = 0;
+                const int32_t xs = qv - corr, c1 = twoT - 1, twocorr = 2 * corr;
+                const uint32_t downs = ~sw;           // bit set: s = -1, the field's sign flips
+                uint32_t fm, lm;                      // flip mask, linear-band mask
+                if (P.hclamp > 0) f4_decide<true>(rng, hv, downs, dw, xs, twocorr, fourT, c1, lw, hclf, fm, lm);
+                else f4_decide<false>(rng, hv, downs, dw, xs, twocorr, fourT, c1, lw, hclf, fm, lm);
+                fm &= vmask;
+                lm &= vmask;
+                const int nl = __popc(lm);
+                flips += __popc(fm);
+                // dS nibbles: flipped down->up = +2 (0x4), up->down = -2 (0xC); word w holds columns 8w .. 8w+7
+                const uint32_t fdn = fm & sw;
+                uint32_t db[4];
 #pragma unroll
-                for (int k = 0; k < R; ++k)
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        const int col = j * R + k, i = k * 256 + 16 * cs + 4 * qq + j;
-                        const uint32_t u = rng_next(rng[j]);
-                        const bool valid = i < n;
-                        const bool up = (sw >> col) & 1u, dif = (dw >> col) & 1u;
-                        const int32_t h = __float2int_rn(__uint_as_float(hv[col]));
-                        int32_t hs = up ? h : -h;
-                        if (hcl > 0) hs = max(-hcl, min(hs, hcl));
-                        const int32_t zt = hs * 65536 + (dif ? xd : xs);
-                        // floor((u16 - 32768) * 4T / 65536) = mulhi((u16 - 32768) << 16, 4T)
-                        const int32_t thr = __mulhi(int32_t((u & 0xffff0000u) ^ 0x80000000u), fourT);
-                        const bool fl = valid && (zt < thr);
-                        nl += (valid && (uint32_t(zt + c1) < lw)) ? 1 : 0;
-                        if (fl) {
-                            nsw ^= 1u << col;
-                            ndw |= 1u << col;
-                            db[col >> 3] |= (up ? 0xCu : 0x4u) << (4 * (col & 7));   // e2m1 -2 / +2
-                        }
-                    }
-                flips += __popc(ndw);
-                sw = nsw;
-                dw = ndw;
+                for (int w = 0; w < 4; ++w) {
+                    uint32_t a8 = (fm >> (8 * w)) & 0xFFu, b8 = (fdn >> (8 * w)) & 0xFFu;
+                    a8 = (a8 | (a8 << 12)) & 0x000F000Fu; a8 = (a8 | (a8 << 6)) & 0x03030303u; a8 = (a8 | (a8 << 3)) & 0x11111111u;
+                    b8 = (b8 | (b8 << 12)) & 0x000F000Fu; b8 = (b8 | (b8 << 6)) & 0x03030303u; b8 = (b8 | (b8 << 3)) & 0x11111111u;
+                    db[w] = (a8 << 2) | (b8 << 3);
+                }
+                sw ^= fm;
+                dw = fm;
                 const int par = m & 1;
                 uint8_t* drow = P.dbuf + ((size_t(g) * 2 + par) * kM + r) * ROWB + cs * 64 + qq * 16;
                 *reinterpret_cast<uint4*>(drow) = make_uint4(db[0], db[1], db[2], db[3]);
                 P.nlx[((size_t(g) * 2 + par) * kM + r) * 128 + cs * 4 + qq] = int8_t(nl);
                 asm volatile("fence.proxy.async.global;" ::: "memory");
                 tc_fence_before();
-                if (prof) { const long long t1 = clock64(); pr[1] += t1 - t0; t0 = t1; }
+                if (prof) { const long long t1 = clock64(); pb += t1 - t0; t0 = t1; }
                 asm volatile("bar.sync 1, %0;" ::"r"(kDW * 32) : "memory");
-                if (tid == 0) flag_publish(P.flags + g * kF4Slices + cs, uint32_t(m + 2));
-                if (prof) pr[2] += clock64() - t0;
+                const long long tb = prof ? clock64() : 0;
+                if (tid == 0) flag_release(P.flags + g * kF4Slices + cs, uint32_t(m + 2));
+                if (prof) {
+                    last_pub = clock64();
+                    pc += last_pub - t0;
+                    p_pub += last_pub - tb;
+                    if (tid == 0) s_pub[m & 1] = last_pub;
+                }
             }
             tc_fence_before();
+            if (prof && tid == 0) {
+                long long* dst = P.prof + size_t(blockIdx.x) * kProfSlots;
+                dst[3] += p_pub;
+                dst[4] += p_wake;
+            }
         } else if (warp < kDW + kF4PW) {
             // ---------------- producer warps ----------------
             const int pwid = warp - kDW;
             const uint32_t* fl = P.flags + g * kF4Slices;
+            long long p_rdy = 0, p_iss = 0;      // profiling: flags seen / TMA issued after the own publish (tiles 0, 7)
             for (int m = -1; m < S; ++m) {
                 const int ay = (g * 2 + (m & 1)) * kM;
                 const uint32_t target = uint32_t(m + 2);
@@ -1169,7 +1207,7 @@ __global__ void __launch_bounds__(kF4Threads, 1)
                         for (uint32_t k = 1;; ++k) {
                             uint32_t v = 0xffffffffu;
                             if (lane < kF4Slices)
-                                asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(fl + lane) : "memory");
+                                asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(fl + lane) : "memory");
                             ready = __ballot_sync(0xffffffffu, v >= target);
                             if ((ready & need) == need) { ok = true; break; }
                             if ((k & 63u) == 0 && __shfl_sync(0xffffffffu, globaltimer() - t0 > kWaitNs, 0)) {
@@ -1177,8 +1215,13 @@ __global__ void __launch_bounds__(kF4Threads, 1)
                                 break;
                             }
                         }
+                        // acquire: relaxed reads that saw the release stores, then a fence; __syncwarp orders every
+                        // lane's acquire before lane 0's copy
+                        asm volatile("fence.acq_rel.gpu;" ::: "memory");
+                        __syncwarp();
                     }
-                    if (prof) pr[7] += clock64() - w0;
+                    const long long w1 = prof ? clock64() : 0;
+                    if (prof) pa += w1 - w0;
                     if (!ok) continue;
                     if (lane == 0) {
                         asm volatile("fence.proxy.async.global;" ::: "memory");
@@ -1186,9 +1229,19 @@ __global__ void __launch_bounds__(kF4Threads, 1)
                         mbar_arrive_expect_tx(bar_full + 8 * s, TILE);
                         if (c < 8) tma_load_2d(dst, &mapD, c * kKChunk, ay, bar_full + 8 * s);
                         else tma_load_2d(dst, &mapNL, 0, ay, bar_full + 8 * s);
+                        if (prof && m >= 0 && (c == 0 || c == 7)) {
+                            const long long pub = s_pub[m & 1];
+                            p_rdy += w1 - pub;
+                            p_iss += clock64() - pub;
+                        }
                     }
                     __syncwarp();
                 }
+            }
+            if (prof && lane == 0 && (pwid == 0 || pwid == 7 % kF4PW)) {
+                long long* dst = P.prof + size_t(blockIdx.x) * kProfSlots;
+                dst[pwid == 0 ? 15 : 16] += p_rdy;
+                dst[pwid == 0 ? 17 : 18] += p_iss;
             }
         } else if (warp == kF4MmaWarp) {
             // ---------------- MMA thread ----------------
@@ -1197,6 +1250,7 @@ __global__ void __launch_bounds__(kF4Threads, 1)
                     if (!err_set(err)) mbar_wait(bar_j, 0u, err, kErrJ);
                     jready = true;
                 }
+                long long p_first = 0, p_last = 0, p_nl = 0, p_h = 0, tf0 = 0, tf7 = 0, tf8 = 0;
                 for (int m = -1; m < S; ++m) {
                     const long long t0 = prof ? clock64() : 0;
                     for (int c = 0; c < kF4Chunks; ++c, ++q) {
@@ -1204,7 +1258,13 @@ __global__ void __launch_bounds__(kF4Threads, 1)
                         const uint32_t u = q / kF4Stages;
                         const long long w0 = prof ? clock64() : 0;
                         const bool ok = !err_set(err) && mbar_wait(bar_full + 8 * s, u & 1u, err, kErrFull);
-                        if (prof) pr[5] += clock64() - w0;
+                        if (prof) {
+                            const long long w1 = clock64();
+                            pa += w1 - w0;
+                            if (c == 0) tf0 = w1;
+                            if (c == 7) tf7 = w1;
+                            if (c == 8) tf8 = w1;
+                        }
                         tc_fence_after();
                         const long long i0 = prof ? clock64() : 0;
                         if (ok) {
@@ -1224,10 +1284,27 @@ __global__ void __launch_bounds__(kF4Threads, 1)
                         }
                         const long long i1 = prof ? clock64() : 0;
                         mma_commit(bar_empty + 8 * s);
-                        if (prof) { const long long i2 = clock64(); pr[9] += i1 - i0; pr[10] += i2 - i1; }
+                        if (prof) { const long long i2 = clock64(); pc += i1 - i0; pd += i2 - i1; }
                     }
                     mma_commit(bar_h);
-                    if (prof) pr[6] += clock64() - t0;
+                    if (prof) {
+                        const long long th = clock64();
+                        pb += th - t0;
+                        if (m >= 0) {
+                            const long long pub = s_pub[m & 1];
+                            p_first += tf0 - pub;
+                            p_last += tf7 - pub;
+                            p_nl += tf8 - pub;
+                            p_h += th - pub;
+                        }
+                    }
+                }
+                if (prof) {
+                    long long* dst = P.prof + size_t(blockIdx.x) * kProfSlots;
+                    dst[11] += p_first;
+                    dst[12] += p_last;
+                    dst[13] += p_nl;
+                    dst[14] += p_h;
                 }
             } else {
                 q += uint32_t(S + 1) * kF4Chunks;
@@ -1238,12 +1315,12 @@ __global__ void __launch_bounds__(kF4Threads, 1)
     if (prof) {
         long long* dst = P.prof + size_t(blockIdx.x) * kProfSlots;
         if (warp == 0 && lane == 0) {
-            dst[0] = pr[0]; dst[1] = pr[1]; dst[2] = pr[2];
+            dst[0] = pa; dst[1] = pb; dst[2] = pc;
         }
         if (warp == kF4MmaWarp && lane == 0) {
-            dst[5] = pr[5]; dst[6] = pr[6]; dst[8] = clock64() - t_loop0; dst[9] = pr[9]; dst[10] = pr[10];
+            dst[5] = pa; dst[6] = pb; dst[8] = clock64() - t_loop0; dst[9] = pc; dst[10] = pd;
         }
-        if (warp == kDW && lane == 0) dst[7] = pr[7];
+        if (warp == kDW && lane == 0) dst[7] = pa;
     }
     __syncthreads();
     if (warp == kF4MmaWarp) {
@@ -1281,8 +1358,6 @@ bool make_map(CUtensorMap* map, void* base, uint64_t cols, uint64_t rows, uint32
               CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
-
-int rounds_of(int np) { return np / 256; }
 
 template <int R>
 size_t smem_bytes_t() {

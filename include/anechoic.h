@@ -118,7 +118,10 @@ typedef struct {
  *   0 wait for fields, 1 TMEM load + decide + update store, 2 n_lin publish, 3 cluster barrier, 4 n_lin read,
  *   5 MMA waiting for TMA, 6 MMA phase (barrier to last commit), 7 TMA waiting for free stages, 8 whole step;
  * out[9] = CTAs, out[10] = CTAs per cluster, out[11] = co-resident clusters, out[12] = MMA issue, out[13] = MMA
- * commits (cycles per step). Returns the count written (<= max). */
+ * commits (cycles per step); fp4 kernel, cycles after the CTA's own publish: out[14] first update tile in shared
+ * memory, out[15] last update tile, out[16] n_lin tile, out[17] fields-ready commit, out[18] / out[19] flags of
+ * update tile 0 / 7 seen, out[20] / out[21] TMA of tile 0 / 7 issued (slot 3 there is the flag publish alone and
+ * slot 4 the fields-ready wake-up after the own publish). Returns the count written (<= max). */
 ANC_API int anc_last_profile(double* out, int max);
 
 /* Replaces one launch + readback of sca_gpu / sca_gpu_bias (sca_gpu.cu:699-713, sca_gpu_bias.cu:716-733) and
