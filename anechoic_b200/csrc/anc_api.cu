@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "../../include/anechoic.h"
+#include "anc_meanfield.cuh"
 #include "anc_plain.cuh"
 #include "anc_tensor.cuh"
 
@@ -395,6 +396,58 @@ int run_host_impl(anc_instance* I, anc_tables* tb, uint64_t seed, uint32_t off, 
 extern "C" {
 
 const char* anc_last_error(void) { return g_err.c_str(); }
+
+// ---- mean-field relaxation ----
+struct anc_meanfield {
+    anc::MfContext* ctx = nullptr;
+};
+
+int anc_mf_create(const int8_t* J, int n, const int32_t* bias, anc_meanfield** out) {
+    if (!J || n < 1 || !out) return fail(ANC_EINVAL, "anc_mf_create: J, n >= 1 and out are required");
+    std::string why;
+    anc::MfContext* c = nullptr;
+    const int rc = anc::mf_create(J, bias, n, &c, &why);
+    if (rc) return fail(rc == -2 ? ANC_ECUDA : ANC_EINVAL, "mean-field setup: %s", why.c_str());
+    *out = new anc_meanfield{c};
+    return ANC_OK;
+}
+
+int anc_mf_npad(const anc_meanfield* mf) { return mf && mf->ctx ? anc::mf_npad(mf->ctx) : 0; }
+
+int anc_mf_forward(anc_meanfield* mf, int S, const float* sched, const float* m0, const float* mprev, float* ckpt,
+                   float* m_out, void* stream) {
+    if (!mf || !mf->ctx || S < 1 || !sched) return fail(ANC_EINVAL, "anc_mf_forward: invalid arguments");
+    std::string why;
+    const int rc = anc::mf_forward(mf->ctx, S, sched, sched + S, sched + 2 * size_t(S), sched + 3 * size_t(S), m0,
+                                   mprev, ckpt, m_out, static_cast<cudaStream_t>(stream), &why);
+    if (rc) return fail(rc == -2 ? ANC_ECUDA : ANC_EINVAL, "mean-field forward: %s", why.c_str());
+    return ANC_OK;
+}
+
+int anc_mf_backward(anc_meanfield* mf, int S, const float* sched, const float* ckpt, const float* g_m, float* gsched,
+                    void* stream) {
+    if (!mf || !mf->ctx || S < 1 || !sched) return fail(ANC_EINVAL, "anc_mf_backward: invalid arguments");
+    std::string why;
+    const int rc = anc::mf_backward(mf->ctx, S, sched, sched + S, sched + 2 * size_t(S), sched + 3 * size_t(S), ckpt,
+                                    g_m, gsched, static_cast<cudaStream_t>(stream), &why);
+    if (rc) return fail(rc == -2 ? ANC_ECUDA : ANC_EINVAL, "mean-field adjoint: %s", why.c_str());
+    return ANC_OK;
+}
+
+int anc_mf_check(anc_meanfield* mf, void* stream) {
+    if (!mf || !mf->ctx) return fail(ANC_EINVAL, "anc_mf_check: null handle");
+    std::string why;
+    const int rc = anc::mf_check_error(mf->ctx, static_cast<cudaStream_t>(stream), &why);
+    if (rc == -3) return fail(ANC_ETIMEOUT, "%s", why.c_str());
+    if (rc) return fail(ANC_ECUDA, "%s", why.c_str());
+    return ANC_OK;
+}
+
+void anc_mf_destroy(anc_meanfield* mf) {
+    if (!mf) return;
+    anc::mf_destroy(mf->ctx);
+    delete mf;
+}
 
 int anc_last_profile(double* out, int max) {
     const int k = std::min<int>(max, int(g_prof.size()));

@@ -1,0 +1,512 @@
+// Mean-field relaxation kernels (see anc_meanfield.cuh for the recurrence): the J x m GEMM on tcgen05 (kind::f16,
+// BF16 operands, f32 accumulation in TMEM) and the fused forward / adjoint elementwise steps.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "anc_meanfield.cuh"
+#include "anc_ptx.cuh"
+
+namespace anc {
+
+struct MfContext {
+    int n = 0, npad = 0;
+    __nv_bfloat16* J = nullptr;       // [npad][npad] (zero padded)
+    float* bias = nullptr;            // [npad]
+    float* partial = nullptr;         // [npad / 256][64][npad] split-K partial products
+    float* mring = nullptr;           // forward ring: 3 x [64][npad]
+    __nv_bfloat16* xm = nullptr;      // [2][64][npad]: hi / lo of the m operand
+    __nv_bfloat16* xp = nullptr;      // [2][64][npad]: hi / lo of the adjoint operand
+    float* seg_m = nullptr;           // [kMfCheckpoint + 2][64][npad]: m_{t0-1} .. m_{t0+16} of a segment
+    float* seg_P = nullptr;           // [kMfCheckpoint][64][npad]
+    float* pbar = nullptr;            // [3][64][npad] ring of pbar_t
+    float* svec = nullptr;            // [3][64] ring of s_t
+    float* nbuf = nullptr;            // [S + 1][64] soft counts n_t
+    int nbuf_steps = 0;
+    int* err = nullptr;               // device error word
+    CUtensorMap mapJ, mapXmh, mapXml, mapXph, mapXpl;
+};
+
+namespace {
+
+using namespace ptx;
+
+constexpr int kRows = 128;                 // rows of J per CTA (MMA M)
+constexpr int kRep = kMfReplicas;          // MMA N
+constexpr int kKC = 256;                   // K per CTA: 4 swizzle atoms of 64 BF16
+constexpr int kGemmThreads = 128;
+constexpr int kElemThreads = 256;
+constexpr int kErrFull = 11, kErrDone = 12;
+constexpr uint32_t kATile = kRows * 128;   // 16 KB: 128 rows x 64 BF16
+constexpr uint32_t kBTile = kRep * 128;    // 8 KB: 64 rows x 64 BF16
+
+size_t gemm_smem() { return 1024 + 4 * size_t(kATile) + 8 * size_t(kBTile) + 64; }
+
+// partial[ks][r][y] = sum_{x in [256 ks, 256 ks + 256)} J[y][x] * (Xh[r][x] + Xl[r][x]); grid (npad / 128, npad / 256).
+__global__ void __launch_bounds__(kGemmThreads, 1)
+    mf_gemm_kernel(const __grid_constant__ CUtensorMap mapJ, const __grid_constant__ CUtensorMap mapXh,
+                   const __grid_constant__ CUtensorMap mapXl, float* __restrict__ partial, int npad, int* err) {
+    // kind::f16 instruction descriptor: f32 accumulator, BF16 A and B, both K-major, N = 64, M = 128
+    constexpr uint32_t IDESC =
+        (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(kRep >> 3) << 17) | (uint32_t(kRows >> 4) << 24);
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* sa = smem;
+    uint8_t* sbh = sa + 4 * kATile;
+    uint8_t* sbl = sbh + 4 * kBTile;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sbl + 4 * kBTile);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 2);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int y0 = blockIdx.x * kRows, k0 = blockIdx.y * kKC;
+    const uint32_t bar_full = smem_u32(bars), bar_done = smem_u32(bars + 1);
+    if (tid == 0) {
+        mbar_init(bar_full, 1);
+        mbar_init(bar_done, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)), "r"(64)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+    if (tid == 0) {
+        mbar_arrive_expect_tx(bar_full, 4 * (kATile + 2 * kBTile));
+        for (int a = 0; a < 4; ++a) {
+            tma_load_2d(smem_u32(sa + a * kATile), &mapJ, k0 + 64 * a, y0, bar_full);
+            tma_load_2d(smem_u32(sbh + a * kBTile), &mapXh, k0 + 64 * a, 0, bar_full);
+            tma_load_2d(smem_u32(sbl + a * kBTile), &mapXl, k0 + 64 * a, 0, bar_full);
+        }
+        const bool ok = mbar_wait(bar_full, 0u, err, kErrFull);
+        tc_fence_after();
+        if (ok) {
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int kk = 0; kk < 4; ++kk)
+                    mma_f16(tmem, sw128_desc(smem_u32(sa + a * kATile) + 32 * kk),
+                            sw128_desc(smem_u32(sbh + a * kBTile) + 32 * kk), IDESC, (a | kk) != 0 ? 1u : 0u);
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int kk = 0; kk < 4; ++kk)
+                    mma_f16(tmem, sw128_desc(smem_u32(sa + a * kATile) + 32 * kk),
+                            sw128_desc(smem_u32(sbl + a * kBTile) + 32 * kk), IDESC, 1u);
+        }
+        mma_commit(bar_done);
+    }
+    __syncwarp();
+    mbar_wait(bar_done, 0u, err, kErrDone);
+    tc_fence_after();
+    // warp w reads TMEM lanes 32w .. 32w + 31 = rows y0 + 32w + lane; columns = replicas
+    const int y = y0 + warp * 32 + lane;
+    float* dst = partial + size_t(blockIdx.y) * kRep * npad + y;
+    uint32_t v[32];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        tmem_ld32(tmem + (uint32_t(warp * 32) << 16) + uint32_t(32 * h), v);
+        tmem_wait_ld();
+#pragma unroll
+        for (int e = 0; e < 32; ++e) dst[size_t(32 * h + e) * npad] = __uint_as_float(v[e]);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(64) : "memory");
+    }
+}
+
+__device__ __forceinline__ void split_bf16(float v, __nv_bfloat16& hi, __nv_bfloat16& lo) {
+    hi = __float2bfloat16_rn(v);
+    lo = __float2bfloat16_rn(v - __bfloat162float(hi));
+}
+
+// Deterministic block sum (fixed shuffle tree, then warp 0 over the warp partials); the result is valid in warp 0.
+template <int NV>
+__device__ __forceinline__ void block_sum(float (&v)[NV], float* red) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+    }
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) red[k * 32 + warp] = v[k];
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            float x = lane < nw ? red[k * 32 + lane] : 0.f;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+            v[k] = x;
+        }
+    }
+}
+
+// Soft counts n[r] = sum_{i < n} (1 - m[r,i]^2) and the BF16 split of m; one block per replica.
+__global__ void __launch_bounds__(kElemThreads) mf_prep_kernel(const float* __restrict__ m, int n, int npad,
+                                                               float* __restrict__ nout, __nv_bfloat16* __restrict__ xh,
+                                                               __nv_bfloat16* __restrict__ xl) {
+    __shared__ float red[32];
+    const int r = blockIdx.x;
+    float acc[1] = {0.f};
+    for (int i = threadIdx.x; i < npad; i += blockDim.x) {
+        const size_t idx = size_t(r) * npad + i;
+        const float v = m[idx];
+        split_bf16(v, xh[idx], xl[idx]);
+        if (i < n) acc[0] += 1.f - v * v;
+    }
+    block_sum(acc, red);
+    if (threadIdx.x == 0) nout[r] = acc[0];
+}
+
+struct FwdArgs {
+    const float* partial;
+    int ksplit, npad, n, t;
+    const float* bias;
+    const float *beta, *q, *u, *w;
+    const float* m_cur;
+    const float* m_prev;
+    const float* n_cur;      // [64]
+    float* m_next;
+    __nv_bfloat16 *xh, *xl;  // split of m_next
+    float* n_next;           // [64]
+    float* P_out;            // [64][npad] or null
+};
+
+__global__ void __launch_bounds__(kElemThreads) mf_fwd_kernel(const FwdArgs a) {
+    __shared__ float red[32];
+    const int r = blockIdx.x, npad = a.npad;
+    const float beta = a.beta[a.t], q = a.q[a.t];
+    const float gamma = a.u[a.t] * a.n_cur[r] + a.w[a.t];
+    float acc[1] = {0.f};
+    for (int i = threadIdx.x; i < npad; i += blockDim.x) {
+        const size_t idx = size_t(r) * npad + i;
+        float H = 0.f;
+        for (int ks = 0; ks < a.ksplit; ++ks) H += a.partial[(size_t(ks) * kRep + r) * npad + i];
+        const float P = H + a.bias[i] + q * a.m_cur[idx] - gamma * a.m_prev[idx];
+        const float mn = i < a.n ? tanhf(beta * P) : 0.f;
+        a.m_next[idx] = mn;
+        split_bf16(mn, a.xh[idx], a.xl[idx]);
+        if (a.P_out) a.P_out[idx] = P;
+        if (i < a.n) acc[0] += 1.f - mn * mn;
+    }
+    block_sum(acc, red);
+    if (threadIdx.x == 0) a.n_next[r] = acc[0];
+}
+
+struct BwdArgs {
+    const float* partial;      // J pbar_{t+1} split-K partials, or null when t = S - 1
+    int ksplit, npad, n, t, S;
+    const float* g_final;      // dL/dm_S (used when t = S - 1)
+    const float* pbar_next;    // pbar_{t+1} or null
+    const float* pbar_next2;   // pbar_{t+2} or null
+    const float* s_next;       // s_{t+1} [64] or null
+    const float* n_next2;      // n_{t+2} [64] or null
+    const float *beta, *q, *u, *w;
+    const float* m_next;       // m_{t+1}
+    const float* m_cur;        // m_t
+    const float* m_prev;       // m_{t-1}
+    const float* P;            // P_t
+    const float* n_cur;        // n_t [64]
+    float* pbar;               // out: pbar_t
+    __nv_bfloat16 *xh, *xl;    // out: split of pbar_t
+    float* s_out;              // out: s_t [64]
+    float* gsched;             // out: [S][4][64]
+};
+
+// One adjoint step t:
+//   G      = dL/dm_{t+1} = J pbar_{t+1} + q_{t+1} pbar_{t+1} + 2 u_{t+1} s_{t+1} m_{t+1} - gamma_{t+2} pbar_{t+2}
+//            (dL/dm_S given at t = S - 1)
+//   abar_t = G (1 - m_{t+1}^2),  pbar_t = beta_t abar_t,  s_t = sum_i pbar_t m_{t-1}
+//   dL/dbeta_t += sum abar_t P_t, dL/dq_t += sum pbar_t m_t, dL/du_t += -s_t n_t, dL/dw_t += -s_t
+__global__ void __launch_bounds__(kElemThreads) mf_bwd_kernel(const BwdArgs a) {
+    __shared__ float red[3 * 32];
+    const int r = blockIdx.x, npad = a.npad, t = a.t;
+    const float beta = a.beta[t];
+    const bool last = t == a.S - 1;
+    const float q1 = last ? 0.f : a.q[t + 1];
+    const float us = last ? 0.f : 2.f * a.u[t + 1] * a.s_next[r];
+    const float g2 = a.pbar_next2 ? a.u[t + 2] * a.n_next2[r] + a.w[t + 2] : 0.f;
+    float acc[3] = {0.f, 0.f, 0.f};   // sum abar * P, sum pbar * m_t, sum pbar * m_{t-1}
+    for (int i = threadIdx.x; i < npad; i += blockDim.x) {
+        const size_t idx = size_t(r) * npad + i;
+        float G;
+        if (last) {
+            G = a.g_final[idx];
+        } else {
+            float H = 0.f;
+            for (int ks = 0; ks < a.ksplit; ++ks) H += a.partial[(size_t(ks) * kRep + r) * npad + i];
+            G = H + q1 * a.pbar_next[idx] + us * a.m_next[idx];
+            if (a.pbar_next2) G -= g2 * a.pbar_next2[idx];
+        }
+        const float mn = a.m_next[idx];
+        const float abar = i < a.n ? G * (1.f - mn * mn) : 0.f;
+        const float pb = beta * abar;
+        a.pbar[idx] = pb;
+        split_bf16(pb, a.xh[idx], a.xl[idx]);
+        acc[0] += abar * a.P[idx];
+        acc[1] += pb * a.m_cur[idx];
+        acc[2] += pb * a.m_prev[idx];
+    }
+    block_sum(acc, red);
+    if (threadIdx.x == 0) {
+        a.s_out[r] = acc[2];
+        float* g = a.gsched + size_t(t) * 4 * kRep;
+        g[0 * kRep + r] = acc[0];
+        g[1 * kRep + r] = acc[1];
+        g[2 * kRep + r] = -acc[2] * a.n_cur[r];
+        g[3 * kRep + r] = -acc[2];
+    }
+}
+
+bool check(cudaError_t e, const char* what, std::string* why) {
+    if (e == cudaSuccess) return true;
+    if (why) *why = std::string(what) + ": " + cudaGetErrorString(e);
+    return false;
+}
+
+int gemm(MfContext* c, const CUtensorMap& mh, const CUtensorMap& ml, cudaStream_t st, std::string* why) {
+    const size_t smem = gemm_smem();
+    cudaError_t e = cudaFuncSetAttribute(mf_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e == cudaSuccess) {
+        mf_gemm_kernel<<<dim3(c->npad / kRows, c->npad / kKC), kGemmThreads, smem, st>>>(c->mapJ, mh, ml, c->partial,
+                                                                                        c->npad, c->err);
+        e = cudaGetLastError();
+    }
+    return check(e, "mean-field GEMM launch", why) ? 0 : -2;
+}
+
+float* mslot(float* base, int k, int npad) { return base + size_t(k) * kRep * npad; }
+
+// Forward steps t = t0 .. t1 - 1: m_t = cur(t), m_{t-1} = prev(t); writes m_{t+1} to next(t) and P_t to pout(t)
+// when that is not null. The BF16 split of m_t must already be in c->xm.
+template <class CurFn, class PrevFn, class NextFn, class PFn>
+int run_steps(MfContext* c, int t0, int t1, const float* beta, const float* q, const float* u, const float* w,
+              CurFn cur, PrevFn prev, NextFn next, PFn pout, cudaStream_t st, std::string* why) {
+    const int npad = c->npad;
+    for (int t = t0; t < t1; ++t) {
+        int rc = gemm(c, c->mapXmh, c->mapXml, st, why);
+        if (rc) return rc;
+        FwdArgs a{};
+        a.partial = c->partial;
+        a.ksplit = npad / kKC;
+        a.npad = npad;
+        a.n = c->n;
+        a.t = t;
+        a.bias = c->bias;
+        a.beta = beta;
+        a.q = q;
+        a.u = u;
+        a.w = w;
+        a.m_cur = cur(t);
+        a.m_prev = prev(t);
+        a.n_cur = c->nbuf + size_t(t) * kRep;
+        a.m_next = next(t);
+        a.xh = c->xm;
+        a.xl = c->xm + size_t(kRep) * npad;
+        a.n_next = c->nbuf + size_t(t + 1) * kRep;
+        a.P_out = pout(t);
+        mf_fwd_kernel<<<kRep, kElemThreads, 0, st>>>(a);
+        if (!check(cudaGetLastError(), "mean-field forward step", why)) return -2;
+    }
+    return 0;
+}
+
+int ensure_steps(MfContext* c, int S, std::string* why) {
+    if (S <= c->nbuf_steps) return 0;
+    if (c->nbuf) cudaFree(c->nbuf);
+    c->nbuf = nullptr;
+    c->nbuf_steps = 0;
+    if (!check(cudaMalloc(&c->nbuf, size_t(S + 1) * kRep * sizeof(float)), "cudaMalloc", why)) return -2;
+    c->nbuf_steps = S;
+    return 0;
+}
+
+}  // namespace
+
+int mf_npad(const MfContext* c) { return c->npad; }
+
+int mf_create(const int8_t* J, const int32_t* bias, int n, MfContext** out, std::string* why) {
+    if (!J || n < 1 || !out) {
+        if (why) *why = "J, n >= 1 and an output handle are required";
+        return -1;
+    }
+    auto* c = new MfContext();
+    c->n = n;
+    c->npad = ((n + 255) / 256) * 256;
+    const int npad = c->npad;
+    std::vector<__nv_bfloat16> Jh(size_t(npad) * npad, __float2bfloat16(0.f));
+    for (int x = 0; x < n; ++x)
+        for (int y = 0; y < n; ++y) Jh[size_t(y) * npad + x] = __float2bfloat16(float(J[size_t(x) * n + y]));
+    std::vector<float> bh(npad, 0.f);
+    if (bias)
+        for (int i = 0; i < n; ++i) bh[i] = float(bias[i]);
+    const size_t plane = size_t(kRep) * npad;
+    bool ok = check(cudaMalloc(&c->J, Jh.size() * sizeof(__nv_bfloat16)), "cudaMalloc", why) &&
+              check(cudaMemcpy(c->J, Jh.data(), Jh.size() * sizeof(__nv_bfloat16), cudaMemcpyHostToDevice), "upload J",
+                    why) &&
+              check(cudaMalloc(&c->bias, npad * sizeof(float)), "cudaMalloc", why) &&
+              check(cudaMemcpy(c->bias, bh.data(), npad * sizeof(float), cudaMemcpyHostToDevice), "upload bias", why) &&
+              check(cudaMalloc(&c->partial, size_t(npad / kKC) * plane * sizeof(float)), "cudaMalloc", why) &&
+              check(cudaMalloc(&c->mring, 3 * plane * sizeof(float)), "cudaMalloc", why) &&
+              check(cudaMalloc(&c->xm, 2 * plane * sizeof(__nv_bfloat16)), "cudaMalloc", why) &&
+              check(cudaMalloc(&c->xp, 2 * plane * sizeof(__nv_bfloat16)), "cudaMalloc", why) &&
+              check(cudaMalloc(&c->seg_m, (kMfCheckpoint + 2) * plane * sizeof(float)), "cudaMalloc", why) &&
+              check(cudaMalloc(&c->seg_P, kMfCheckpoint * plane * sizeof(float)), "cudaMalloc", why) &&
+              check(cudaMalloc(&c->pbar, 3 * plane * sizeof(float)), "cudaMalloc", why) &&
+              check(cudaMalloc(&c->svec, 3 * kRep * sizeof(float)), "cudaMalloc", why) &&
+              check(cudaMalloc(&c->err, sizeof(int)), "cudaMalloc", why) &&
+              check(cudaMemset(c->err, 0, sizeof(int)), "cudaMemset", why);
+    if (ok) {
+        ok = make_map_2d(&c->mapJ, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, c->J, npad, npad, 64, kRows) &&
+             make_map_2d(&c->mapXmh, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, c->xm, npad, kRep, 64, kRep) &&
+             make_map_2d(&c->mapXml, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, c->xm + plane, npad, kRep, 64, kRep) &&
+             make_map_2d(&c->mapXph, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, c->xp, npad, kRep, 64, kRep) &&
+             make_map_2d(&c->mapXpl, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, c->xp + plane, npad, kRep, 64, kRep);
+        if (!ok && why) *why = "cuTensorMapEncodeTiled failed";
+    }
+    if (!ok) {
+        mf_destroy(c);
+        return -2;
+    }
+    *out = c;
+    return 0;
+}
+
+int mf_forward(MfContext* c, int S, const float* beta, const float* q, const float* u, const float* w, const float* m0,
+               const float* mprev, float* ckpt, float* m_out, cudaStream_t st, std::string* why) {
+    if (!c || S < 1 || !beta || !q || !u || !w || !m0 || !mprev || !ckpt || !m_out) {
+        if (why) *why = "invalid mean-field forward arguments";
+        return -1;
+    }
+    int rc = ensure_steps(c, S, why);
+    if (rc) return rc;
+    const int npad = c->npad;
+    const size_t plane = size_t(kRep) * npad;
+    float* ring = c->mring;
+    if (!check(cudaMemcpyAsync(mslot(ring, 0, npad), mprev, plane * 4, cudaMemcpyDeviceToDevice, st), "copy", why) ||
+        !check(cudaMemcpyAsync(mslot(ring, 1, npad), m0, plane * 4, cudaMemcpyDeviceToDevice, st), "copy", why))
+        return -2;
+    mf_prep_kernel<<<kRep, kElemThreads, 0, st>>>(mslot(ring, 1, npad), c->n, npad, c->nbuf, c->xm, c->xm + plane);
+    if (!check(cudaGetLastError(), "mean-field prep", why)) return -2;
+    // m_t lives in ring slot (t + 1) % 3, m_{t-1} in slot t % 3
+    for (int t0 = 0; t0 < S; t0 += kMfCheckpoint) {
+        float* ck = ckpt + size_t(t0 / kMfCheckpoint) * 2 * plane;
+        if (!check(cudaMemcpyAsync(ck, mslot(ring, t0 % 3, npad), plane * 4, cudaMemcpyDeviceToDevice, st), "ckpt",
+                   why) ||
+            !check(cudaMemcpyAsync(ck + plane, mslot(ring, (t0 + 1) % 3, npad), plane * 4, cudaMemcpyDeviceToDevice, st),
+                   "ckpt", why))
+            return -2;
+        const int t1 = std::min(S, t0 + kMfCheckpoint);
+        rc = run_steps(
+            c, t0, t1, beta, q, u, w, [&](int t) { return mslot(ring, (t + 1) % 3, npad); },
+            [&](int t) { return mslot(ring, t % 3, npad); }, [&](int t) { return mslot(ring, (t + 2) % 3, npad); },
+            [](int) { return static_cast<float*>(nullptr); }, st, why);
+        if (rc) return rc;
+    }
+    if (!check(cudaMemcpyAsync(m_out, mslot(ring, (S + 1) % 3, npad), plane * 4, cudaMemcpyDeviceToDevice, st), "copy",
+               why))
+        return -2;
+    return 0;
+}
+
+int mf_backward(MfContext* c, int S, const float* beta, const float* q, const float* u, const float* w,
+                const float* ckpt, const float* g_m, float* gsched, cudaStream_t st, std::string* why) {
+    if (!c || S < 1 || !beta || !q || !u || !w || !ckpt || !g_m || !gsched) {
+        if (why) *why = "invalid mean-field backward arguments";
+        return -1;
+    }
+    int rc = ensure_steps(c, S, why);
+    if (rc) return rc;
+    const int npad = c->npad;
+    const size_t plane = size_t(kRep) * npad;
+    const int nseg = (S + kMfCheckpoint - 1) / kMfCheckpoint;
+    for (int seg = nseg - 1; seg >= 0; --seg) {
+        const int t0 = seg * kMfCheckpoint, t1 = std::min(S, t0 + kMfCheckpoint);
+        // segment buffer slot k holds m_{t0 - 1 + k}
+        const float* ck = ckpt + size_t(seg) * 2 * plane;
+        if (!check(cudaMemcpyAsync(mslot(c->seg_m, 0, npad), ck, 2 * plane * 4, cudaMemcpyDeviceToDevice, st), "copy",
+                   why))
+            return -2;
+        mf_prep_kernel<<<kRep, kElemThreads, 0, st>>>(mslot(c->seg_m, 1, npad), c->n, npad,
+                                                     c->nbuf + size_t(t0) * kRep, c->xm, c->xm + plane);
+        if (!check(cudaGetLastError(), "mean-field prep", why)) return -2;
+        rc = run_steps(
+            c, t0, t1, beta, q, u, w, [&](int t) { return mslot(c->seg_m, t - t0 + 1, npad); },
+            [&](int t) { return mslot(c->seg_m, t - t0, npad); },
+            [&](int t) { return mslot(c->seg_m, t - t0 + 2, npad); },
+            [&](int t) { return mslot(c->seg_P, t - t0, npad); }, st, why);
+        if (rc) return rc;
+        for (int t = t1 - 1; t >= t0; --t) {
+            const bool last = t == S - 1;
+            if (!last) {
+                rc = gemm(c, c->mapXph, c->mapXpl, st, why);
+                if (rc) return rc;
+            }
+            BwdArgs a{};
+            a.partial = last ? nullptr : c->partial;
+            a.ksplit = npad / kKC;
+            a.npad = npad;
+            a.n = c->n;
+            a.t = t;
+            a.S = S;
+            a.g_final = g_m;
+            a.pbar_next = last ? nullptr : mslot(c->pbar, (t + 1) % 3, npad);
+            a.pbar_next2 = t + 2 < S ? mslot(c->pbar, (t + 2) % 3, npad) : nullptr;
+            a.s_next = last ? nullptr : c->svec + ((t + 1) % 3) * kRep;
+            a.n_next2 = t + 2 < S ? c->nbuf + size_t(t + 2) * kRep : nullptr;
+            a.beta = beta;
+            a.q = q;
+            a.u = u;
+            a.w = w;
+            a.m_next = mslot(c->seg_m, t - t0 + 2, npad);
+            a.m_cur = mslot(c->seg_m, t - t0 + 1, npad);
+            a.m_prev = mslot(c->seg_m, t - t0, npad);
+            a.P = mslot(c->seg_P, t - t0, npad);
+            a.n_cur = c->nbuf + size_t(t) * kRep;
+            a.pbar = mslot(c->pbar, t % 3, npad);
+            a.xh = c->xp;
+            a.xl = c->xp + plane;
+            a.s_out = c->svec + (t % 3) * kRep;
+            a.gsched = gsched;
+            mf_bwd_kernel<<<kRep, kElemThreads, 0, st>>>(a);
+            if (!check(cudaGetLastError(), "mean-field adjoint step", why)) return -2;
+        }
+    }
+    return 0;
+}
+
+int mf_check_error(MfContext* c, cudaStream_t st, std::string* why) {
+    int h = 0;
+    cudaError_t e = cudaMemcpyAsync(&h, c->err, 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (!check(e, "mean-field error word", why)) return -2;
+    if (h) {
+        if (why) *why = "a bounded device wait expired in the mean-field GEMM (code " + std::to_string(h) + ")";
+        cudaMemsetAsync(c->err, 0, 4, st);
+        return -3;
+    }
+    return 0;
+}
+
+void mf_destroy(MfContext* c) {
+    if (!c) return;
+    for (void* p : {static_cast<void*>(c->J), static_cast<void*>(c->bias), static_cast<void*>(c->partial),
+                    static_cast<void*>(c->mring), static_cast<void*>(c->xm), static_cast<void*>(c->xp),
+                    static_cast<void*>(c->seg_m), static_cast<void*>(c->seg_P), static_cast<void*>(c->pbar),
+                    static_cast<void*>(c->svec), static_cast<void*>(c->nbuf), static_cast<void*>(c->err)})
+        if (p) cudaFree(p);
+    delete c;
+}
+
+}  // namespace anc

@@ -208,6 +208,31 @@ typedef struct {
 } anc_device_job;
 ANC_API int anc_run_batch_noalloc(int njobs, const anc_device_job* jobs, void* stream);
 
+/* ---------------------------------------------------------------------------------------------------------------
+ * Differentiable mean-field relaxation (new; the reference has no differentiable path). Soft surrogate of the
+ * corrected dynamics, per replica r and step t = 0 .. S-1:
+ *   P_t = J m_t + b + q_t m_t - gamma_t m_{t-1},  gamma_t[r] = u_t sum_i (1 - m_t[r,i]^2) + w_t,  m_{t+1} = tanh(beta_t P_t)
+ * with beta_t = 1/(2 T_t), u_t = lambda_t / (2 T_{t-1}) (counted Onsager gain), w_t the constant correction
+ * (kappa T_{t-1} temperature-scaled, -jv constant): the tanh form of the reference's effective process
+ * (research/dmft_sca_20261004/dmft_torch.py:38-57) and the soft version of sca_ref.hpp:118-131.
+ * J in BF16 (exact for the integer couplings), f32 magnetisations and accumulation (tcgen05 kind::f16 GEMM with m
+ * split into BF16 hi + lo), checkpoints every 16 steps in the adjoint. All pointers below are DEVICE pointers;
+ * calls are asynchronous on `stream` (NULL = default); anc_mf_check synchronises and reports a device wait timeout.
+ *   sched:  [4][S] f32 rows beta, q, u, w
+ *   m0, mprev, m_out: [64][npad] f32 (rows = replicas; unused rows and columns i >= n stay zero)
+ *   ckpt:   [ceil(S/16)][2][64][npad] f32 (written by forward, read by backward)
+ *   g_m:    dL/dm_S [64][npad];  gsched: [S][4][64] per-replica partials of dL/d(beta, q, u, w)_t
+ * --------------------------------------------------------------------------------------------------------------- */
+typedef struct anc_meanfield anc_meanfield;
+ANC_API int anc_mf_create(const int8_t* J, int n, const int32_t* bias, anc_meanfield** out);
+ANC_API int anc_mf_npad(const anc_meanfield* mf);
+ANC_API int anc_mf_forward(anc_meanfield* mf, int S, const float* sched, const float* m0, const float* mprev,
+                           float* ckpt, float* m_out, void* stream);
+ANC_API int anc_mf_backward(anc_meanfield* mf, int S, const float* sched, const float* ckpt, const float* g_m,
+                            float* gsched, void* stream);
+ANC_API int anc_mf_check(anc_meanfield* mf, void* stream);
+ANC_API void anc_mf_destroy(anc_meanfield* mf);
+
 /* Last device time of a synchronous run on this thread (ms, CUDA events around the launch). */
 ANC_API double anc_last_device_ms(void);
 

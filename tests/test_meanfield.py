@@ -1,0 +1,118 @@
+"""GPU checks of the mean-field relaxation kernels (tcgen05 BF16 J x m GEMM, fused forward / adjoint steps,
+checkpoints every 16 steps) against the FP64 oracle (oracle/meanfield_ref.py, torch float64 autograd) and central
+finite differences; and exact-engine parity under a tuned (q-ramped) schedule.
+
+Stated error (floating point, so tolerances are written here): the kernels hold m in f32 and feed it to the tensor
+cores as a BF16 hi + lo pair (about 16 significant bits); J is exact in BF16.
+  forward  max |m_S - m_S(fp64)| <= 2e-3 (64 replicas x 200 steps on the N=2000 +-1 instance)
+  gradient relative error of each of the five schedule derivatives <= 2e-2 against FP64 autograd
+"""
+import math
+
+import pytest
+import torch
+
+import anechoic_b200 as A
+from anechoic_b200 import instances as I
+from anechoic_b200.meanfield import MeanField, SoftSchedule, initial_magnetisations, relax, soft_cut
+from oracle.meanfield_ref import relax64, soft_cut64
+from tests.golden.make_golden import SEED
+from tests.test_parity_plain import assert_same
+
+pytestmark = pytest.mark.gpu
+
+THETA0 = (30.0, math.log(6.0), 4.0, 0.0, 1.05)     # reference default schedule, counted Onsager lambda 1.05
+
+
+def _case(inst, S, R, mode, theta, seed=1):
+    mf = MeanField(inst)
+    sch = SoftSchedule(S=S, mode=mode)
+    m0r = initial_magnetisations(inst.n, R, seed)
+    J64 = torch.as_tensor(inst.to_dense(), dtype=torch.float64, device="cuda")
+    b64 = torch.zeros(inst.n, dtype=torch.float64, device="cuda") if inst.bias is None else \
+        torch.as_tensor(inst.bias, dtype=torch.float64, device="cuda")
+    sumw = inst.stats()["sumw"]
+    th = torch.tensor(theta, dtype=torch.float64, device="cuda", requires_grad=True)
+    beta, q, u, w = sch.vectors(th)
+    mS = relax(mf, beta, q, u, w, mf.pad(m0r))
+    cut = soft_cut(inst, mS[:R, : inst.n].double()).mean()
+    cut.backward()
+    th64 = torch.tensor(theta, dtype=torch.float64, device="cuda", requires_grad=True)
+    b_, q_, u_, w_ = sch.vectors(th64)
+    m0 = m0r.double().cuda()
+    m64 = relax64(J64, b64, b_, q_, u_, w_, m0, torch.ones_like(m0))
+    cut64 = soft_cut64(J64, sumw, m64).mean()
+    cut64.backward()
+    return dict(mS=mS[:R, : inst.n].double(), m64=m64.detach(), g=th.grad.detach(), g64=th64.grad.detach(),
+                cut=float(cut), cut64=float(cut64))
+
+
+def _rel(g, g64):
+    nz = g64.abs() > 1e-12
+    return ((g - g64).abs()[nz] / g64.abs()[nz].clamp_min(1e-3 * float(g64.abs().max()))).max().item()
+
+
+@pytest.fixture(scope="module")
+def pm1(cuda):
+    return I.complete_pm1(2000, SEED)
+
+
+def test_config4_forward_and_gradient_vs_fp64(pm1):
+    """N=2000 +-1, 64 replicas, 200 unrolled steps, counted Onsager: forward and the five schedule gradients."""
+    r = _case(pm1, 200, 64, "counted", THETA0)
+    err = (r["mS"] - r["m64"]).abs().max().item()
+    assert err <= 2e-3, err
+    rel = _rel(r["g"], r["g64"])
+    assert rel <= 2e-2, (rel, r["g"].tolist(), r["g64"].tolist())
+    assert abs(r["cut"] - r["cut64"]) <= 1e-3 * abs(r["cut64"])
+
+
+@pytest.mark.parametrize("mode", ["tecT", "none"])
+def test_other_corrections_and_ragged_checkpoints(cuda, mode):
+    """K=2 couplings with bias, n = 700 (npad 768), S = 37 (two full checkpoint segments and a ragged one)."""
+    inst = I.random_kbit(700, 2, 44, pzero=0.4, bmax=3)
+    r = _case(inst, 37, 40, mode, (12.0, math.log(8.0), 1.0, 0.5, 1.5))
+    err = (r["mS"] - r["m64"]).abs().max().item()
+    assert err <= 2e-3, err
+    rel = _rel(r["g"], r["g64"])
+    assert rel <= 2e-2, (rel, r["g"].tolist(), r["g64"].tolist())
+
+
+def test_kernel_gradient_vs_central_differences(pm1):
+    """dL/dtheta from the adjoint kernels against central differences of the kernels' own forward."""
+    S, R = 48, 64
+    mf = MeanField(pm1)
+    sch = SoftSchedule(S=S, mode="counted")
+    m0 = mf.pad(initial_magnetisations(pm1.n, R, 5))
+
+    def loss(theta):
+        beta, q, u, w = sch.vectors(theta)
+        return soft_cut(pm1, relax(mf, beta, q, u, w, m0)[:R, : pm1.n].double()).mean()
+
+    th = torch.tensor(THETA0, dtype=torch.float64, device="cuda", requires_grad=True)
+    loss(th).backward()
+    for k in range(5):
+        h = 2e-3 * max(1.0, abs(THETA0[k]))
+        tp = torch.tensor(THETA0, dtype=torch.float64, device="cuda")
+        tm = tp.clone()
+        tp[k] += h
+        tm[k] -= h
+        with torch.no_grad():
+            fd = (loss(tp) - loss(tm)).item() / (2 * h)
+        g = th.grad[k].item()
+        assert abs(fd - g) <= 5e-2 * max(abs(fd), abs(g), 1.0), (k, fd, g)
+
+
+def test_tuned_schedule_runs_bit_exact_on_the_engine(pm1, oracle):
+    """A few tuning steps, then the tuned (q-ramped) tables on the exact engine: parity with the golden-model
+    restatement for every spin and n_lin step (the relaxation never alters the integer engine)."""
+    from anechoic_b200.meanfield import tune
+    theta, hist = tune(pm1, S=100, R=64, theta0=(30.0, math.log(6.0), 4.0, 0.5, 1.05), iters=3)
+    assert len(hist) == 3 and all(math.isfinite(h[1]) for h in hist)
+    arrays = SoftSchedule(S=100, mode="counted").table_arrays(theta)
+    tb = A.Tables.from_arrays(**arrays)
+    dev = A.DeviceInstance(pm1)
+    r = A.run(dev, tb, 9, 0, 130, trace=True, engine="tensor")
+    ref = oracle.run_batch(2000, arrays, 9, 0, 130, dense=pm1.dense)
+    for c in range(130):
+        assert_same(r, {k: v[c] for k, v in ref.items()}, c, f"chain {c}")
