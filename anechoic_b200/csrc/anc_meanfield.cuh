@@ -10,8 +10,8 @@
 // expected number of slots inside the linear band).
 //
 // J is held in BF16 (exact for |J| <= 256); J m is a tcgen05 kind::f16 GEMM (M 128 rows of J, N 64 replicas,
-// K split over CTAs) with m given as a BF16 hi + lo pair (about 16 significant bits), f32 accumulation, and the
-// split-K partials summed in a fixed order by the elementwise kernels (deterministic).
+// K split over CTAs) with m given as three BF16 terms (24 significant bits, so every product is the f32 product),
+// f32 accumulation, and the split-K partials summed in a fixed order by the elementwise kernels (deterministic).
 //
 // The adjoint runs the recurrence backwards from dL/dm_S with activation checkpoints every 16 steps (each segment
 // recomputed once) and returns per-step sums dL/dbeta_t, dL/dq_t, dL/du_t, dL/dw_t (one value per replica, summed

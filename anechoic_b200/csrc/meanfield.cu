@@ -18,8 +18,8 @@ struct MfContext {
     float* bias = nullptr;            // [npad]
     float* partial = nullptr;         // [npad / 256][64][npad] split-K partial products
     float* mring = nullptr;           // forward ring: 3 x [64][npad]
-    __nv_bfloat16* xm = nullptr;      // [2][64][npad]: hi / lo of the m operand
-    __nv_bfloat16* xp = nullptr;      // [2][64][npad]: hi / lo of the adjoint operand
+    __nv_bfloat16* xm = nullptr;      // [3][64][npad]: hi / mid / lo of the m operand
+    __nv_bfloat16* xp = nullptr;      // [3][64][npad]: hi / mid / lo of the adjoint operand
     float* seg_m = nullptr;           // [kMfCheckpoint + 2][64][npad]: m_{t0-1} .. m_{t0+16} of a segment
     float* seg_P = nullptr;           // [kMfCheckpoint][64][npad]
     float* pbar = nullptr;            // [3][64][npad] ring of pbar_t
@@ -27,7 +27,7 @@ struct MfContext {
     float* nbuf = nullptr;            // [S + 1][64] soft counts n_t
     int nbuf_steps = 0;
     int* err = nullptr;               // device error word
-    CUtensorMap mapJ, mapXmh, mapXml, mapXph, mapXpl;
+    CUtensorMap mapJ, mapXm[3], mapXp[3];
 };
 
 namespace {
@@ -43,12 +43,14 @@ constexpr int kErrFull = 11, kErrDone = 12;
 constexpr uint32_t kATile = kRows * 128;   // 16 KB: 128 rows x 64 BF16
 constexpr uint32_t kBTile = kRep * 128;    // 8 KB: 64 rows x 64 BF16
 
-size_t gemm_smem() { return 1024 + 4 * size_t(kATile) + 8 * size_t(kBTile) + 64; }
+size_t gemm_smem() { return 1024 + 4 * size_t(kATile) + 12 * size_t(kBTile) + 64; }
 
-// partial[ks][r][y] = sum_{x in [256 ks, 256 ks + 256)} J[y][x] * (Xh[r][x] + Xl[r][x]); grid (npad / 128, npad / 256).
+// partial[ks][r][y] = sum_{x in [256 ks, 256 ks + 256)} J[y][x] * (X0 + X1 + X2)[r][x], X = the three BF16 terms of
+// an f32 operand (24 significant bits; J is exact in BF16, so every product is exact); grid (npad / 128, npad / 256).
 __global__ void __launch_bounds__(kGemmThreads, 1)
     mf_gemm_kernel(const __grid_constant__ CUtensorMap mapJ, const __grid_constant__ CUtensorMap mapXh,
-                   const __grid_constant__ CUtensorMap mapXl, float* __restrict__ partial, int npad, int* err) {
+                   const __grid_constant__ CUtensorMap mapXm, const __grid_constant__ CUtensorMap mapXl,
+                   float* __restrict__ partial, int npad, int* err) {
     // kind::f16 instruction descriptor: f32 accumulator, BF16 A and B, both K-major, N = 64, M = 128
     constexpr uint32_t IDESC =
         (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(kRep >> 3) << 17) | (uint32_t(kRows >> 4) << 24);
@@ -56,7 +58,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t* sa = smem;
     uint8_t* sbh = sa + 4 * kATile;
-    uint8_t* sbl = sbh + 4 * kBTile;
+    uint8_t* sbm = sbh + 4 * kBTile;
+    uint8_t* sbl = sbm + 4 * kBTile;
     uint64_t* bars = reinterpret_cast<uint64_t*>(sbl + 4 * kBTile);
     uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 2);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -68,7 +71,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)), "r"(64)
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                     "r"(512)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -77,27 +81,36 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     tc_fence_after();
     const uint32_t tmem = *tslot;
     if (tid == 0) {
-        mbar_arrive_expect_tx(bar_full, 4 * (kATile + 2 * kBTile));
+        mbar_arrive_expect_tx(bar_full, 4 * (kATile + 3 * kBTile));
         for (int a = 0; a < 4; ++a) {
             tma_load_2d(smem_u32(sa + a * kATile), &mapJ, k0 + 64 * a, y0, bar_full);
             tma_load_2d(smem_u32(sbh + a * kBTile), &mapXh, k0 + 64 * a, 0, bar_full);
+            tma_load_2d(smem_u32(sbm + a * kBTile), &mapXm, k0 + 64 * a, 0, bar_full);
             tma_load_2d(smem_u32(sbl + a * kBTile), &mapXl, k0 + 64 * a, 0, bar_full);
         }
         const bool ok = mbar_wait(bar_full, 0u, err, kErrFull);
         tc_fence_after();
         if (ok) {
+            // The tensor core's f32 accumulation truncates toward zero each time an MMA adds into an accumulator, a
+            // bias of up to half an ulp of the accumulator per add. Keeping the leading-term products of each 64-wide
+            // K atom in their own accumulator (columns 64a .. 64a + 63) and the small mid / lo products in a fifth
+            // (columns 256 ..) keeps the accumulators small and the adds per accumulator few; the epilogue sums them
+            // with round-to-nearest.
 #pragma unroll
             for (int a = 0; a < 4; ++a)
 #pragma unroll
                 for (int kk = 0; kk < 4; ++kk)
-                    mma_f16(tmem, sw128_desc(smem_u32(sa + a * kATile) + 32 * kk),
-                            sw128_desc(smem_u32(sbh + a * kBTile) + 32 * kk), IDESC, (a | kk) != 0 ? 1u : 0u);
+                    mma_f16(tmem + uint32_t(64 * a), sw128_desc(smem_u32(sa + a * kATile) + 32 * kk),
+                            sw128_desc(smem_u32(sbh + a * kBTile) + 32 * kk), IDESC, kk != 0 ? 1u : 0u);
 #pragma unroll
             for (int a = 0; a < 4; ++a)
 #pragma unroll
-                for (int kk = 0; kk < 4; ++kk)
-                    mma_f16(tmem, sw128_desc(smem_u32(sa + a * kATile) + 32 * kk),
+                for (int kk = 0; kk < 4; ++kk) {
+                    mma_f16(tmem + 256u, sw128_desc(smem_u32(sa + a * kATile) + 32 * kk),
+                            sw128_desc(smem_u32(sbm + a * kBTile) + 32 * kk), IDESC, (a | kk) != 0 ? 1u : 0u);
+                    mma_f16(tmem + 256u, sw128_desc(smem_u32(sa + a * kATile) + 32 * kk),
                             sw128_desc(smem_u32(sbl + a * kBTile) + 32 * kk), IDESC, 1u);
+                }
         }
         mma_commit(bar_done);
     }
@@ -107,25 +120,48 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     // warp w reads TMEM lanes 32w .. 32w + 31 = rows y0 + 32w + lane; columns = replicas
     const int y = y0 + warp * 32 + lane;
     float* dst = partial + size_t(blockIdx.y) * kRep * npad + y;
+    const uint32_t tl = tmem + (uint32_t(warp * 32) << 16);
     uint32_t v[32];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-        tmem_ld32(tmem + (uint32_t(warp * 32) << 16) + uint32_t(32 * h), v);
+        float s01[32], s23[32];
+        tmem_ld32(tl + uint32_t(32 * h), v);
         tmem_wait_ld();
 #pragma unroll
-        for (int e = 0; e < 32; ++e) dst[size_t(32 * h + e) * npad] = __uint_as_float(v[e]);
+        for (int e = 0; e < 32; ++e) s01[e] = __uint_as_float(v[e]);
+        tmem_ld32(tl + uint32_t(64 + 32 * h), v);
+        tmem_wait_ld();
+#pragma unroll
+        for (int e = 0; e < 32; ++e) s01[e] += __uint_as_float(v[e]);
+        tmem_ld32(tl + uint32_t(128 + 32 * h), v);
+        tmem_wait_ld();
+#pragma unroll
+        for (int e = 0; e < 32; ++e) s23[e] = __uint_as_float(v[e]);
+        tmem_ld32(tl + uint32_t(192 + 32 * h), v);
+        tmem_wait_ld();
+#pragma unroll
+        for (int e = 0; e < 32; ++e) s23[e] += __uint_as_float(v[e]);
+        tmem_ld32(tl + uint32_t(256 + 32 * h), v);
+        tmem_wait_ld();
+#pragma unroll
+        for (int e = 0; e < 32; ++e) dst[size_t(32 * h + e) * npad] = (s01[e] + s23[e]) + __uint_as_float(v[e]);
     }
     tc_fence_before();
     __syncthreads();
     if (warp == 0) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(64) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512) : "memory");
     }
 }
 
-__device__ __forceinline__ void split_bf16(float v, __nv_bfloat16& hi, __nv_bfloat16& lo) {
-    hi = __float2bfloat16_rn(v);
-    lo = __float2bfloat16_rn(v - __bfloat162float(hi));
+// v = x[0] + x[1] + x[2] + O(2^-24 |v|): three BF16 terms, each rounding the remainder of the previous ones.
+__device__ __forceinline__ void split_bf16(float v, __nv_bfloat16* x, size_t plane) {
+    const __nv_bfloat16 h = __float2bfloat16_rn(v);
+    const float r1 = v - __bfloat162float(h);
+    const __nv_bfloat16 m = __float2bfloat16_rn(r1);
+    x[0] = h;
+    x[plane] = m;
+    x[2 * plane] = __float2bfloat16_rn(r1 - __bfloat162float(m));
 }
 
 // Deterministic block sum (fixed shuffle tree, then warp 0 over the warp partials); the result is valid in warp 0.
@@ -152,17 +188,16 @@ __device__ __forceinline__ void block_sum(float (&v)[NV], float* red) {
     }
 }
 
-// Soft counts n[r] = sum_{i < n} (1 - m[r,i]^2) and the BF16 split of m; one block per replica.
+// Soft counts n[r] = sum_{i < n} (1 - m[r,i]^2) and the BF16 terms of m; one block per replica.
 __global__ void __launch_bounds__(kElemThreads) mf_prep_kernel(const float* __restrict__ m, int n, int npad,
-                                                               float* __restrict__ nout, __nv_bfloat16* __restrict__ xh,
-                                                               __nv_bfloat16* __restrict__ xl) {
+                                                               float* __restrict__ nout, __nv_bfloat16* __restrict__ x) {
     __shared__ float red[32];
     const int r = blockIdx.x;
     float acc[1] = {0.f};
     for (int i = threadIdx.x; i < npad; i += blockDim.x) {
         const size_t idx = size_t(r) * npad + i;
         const float v = m[idx];
-        split_bf16(v, xh[idx], xl[idx]);
+        split_bf16(v, x + idx, size_t(kRep) * npad);
         if (i < n) acc[0] += 1.f - v * v;
     }
     block_sum(acc, red);
@@ -178,7 +213,7 @@ struct FwdArgs {
     const float* m_prev;
     const float* n_cur;      // [64]
     float* m_next;
-    __nv_bfloat16 *xh, *xl;  // split of m_next
+    __nv_bfloat16* x;        // BF16 terms of m_next [3][64][npad]
     float* n_next;           // [64]
     float* P_out;            // [64][npad] or null
 };
@@ -196,7 +231,7 @@ __global__ void __launch_bounds__(kElemThreads) mf_fwd_kernel(const FwdArgs a) {
         const float P = H + a.bias[i] + q * a.m_cur[idx] - gamma * a.m_prev[idx];
         const float mn = i < a.n ? tanhf(beta * P) : 0.f;
         a.m_next[idx] = mn;
-        split_bf16(mn, a.xh[idx], a.xl[idx]);
+        split_bf16(mn, a.x + idx, size_t(kRep) * npad);
         if (a.P_out) a.P_out[idx] = P;
         if (i < a.n) acc[0] += 1.f - mn * mn;
     }
@@ -219,7 +254,7 @@ struct BwdArgs {
     const float* P;            // P_t
     const float* n_cur;        // n_t [64]
     float* pbar;               // out: pbar_t
-    __nv_bfloat16 *xh, *xl;    // out: split of pbar_t
+    __nv_bfloat16* x;          // out: BF16 terms of pbar_t [3][64][npad]
     float* s_out;              // out: s_t [64]
     float* gsched;             // out: [S][4][64]
 };
@@ -253,7 +288,7 @@ __global__ void __launch_bounds__(kElemThreads) mf_bwd_kernel(const BwdArgs a) {
         const float abar = i < a.n ? G * (1.f - mn * mn) : 0.f;
         const float pb = beta * abar;
         a.pbar[idx] = pb;
-        split_bf16(pb, a.xh[idx], a.xl[idx]);
+        split_bf16(pb, a.x + idx, size_t(kRep) * npad);
         acc[0] += abar * a.P[idx];
         acc[1] += pb * a.m_cur[idx];
         acc[2] += pb * a.m_prev[idx];
@@ -275,12 +310,12 @@ bool check(cudaError_t e, const char* what, std::string* why) {
     return false;
 }
 
-int gemm(MfContext* c, const CUtensorMap& mh, const CUtensorMap& ml, cudaStream_t st, std::string* why) {
+int gemm(MfContext* c, const CUtensorMap (&mx)[3], cudaStream_t st, std::string* why) {
     const size_t smem = gemm_smem();
     cudaError_t e = cudaFuncSetAttribute(mf_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e == cudaSuccess) {
-        mf_gemm_kernel<<<dim3(c->npad / kRows, c->npad / kKC), kGemmThreads, smem, st>>>(c->mapJ, mh, ml, c->partial,
-                                                                                        c->npad, c->err);
+        mf_gemm_kernel<<<dim3(c->npad / kRows, c->npad / kKC), kGemmThreads, smem, st>>>(c->mapJ, mx[0], mx[1], mx[2],
+                                                                                        c->partial, c->npad, c->err);
         e = cudaGetLastError();
     }
     return check(e, "mean-field GEMM launch", why) ? 0 : -2;
@@ -289,13 +324,13 @@ int gemm(MfContext* c, const CUtensorMap& mh, const CUtensorMap& ml, cudaStream_
 float* mslot(float* base, int k, int npad) { return base + size_t(k) * kRep * npad; }
 
 // Forward steps t = t0 .. t1 - 1: m_t = cur(t), m_{t-1} = prev(t); writes m_{t+1} to next(t) and P_t to pout(t)
-// when that is not null. The BF16 split of m_t must already be in c->xm.
+// when that is not null. The BF16 terms of m_t must already be in c->xm.
 template <class CurFn, class PrevFn, class NextFn, class PFn>
 int run_steps(MfContext* c, int t0, int t1, const float* beta, const float* q, const float* u, const float* w,
               CurFn cur, PrevFn prev, NextFn next, PFn pout, cudaStream_t st, std::string* why) {
     const int npad = c->npad;
     for (int t = t0; t < t1; ++t) {
-        int rc = gemm(c, c->mapXmh, c->mapXml, st, why);
+        int rc = gemm(c, c->mapXm, st, why);
         if (rc) return rc;
         FwdArgs a{};
         a.partial = c->partial;
@@ -312,8 +347,7 @@ int run_steps(MfContext* c, int t0, int t1, const float* beta, const float* q, c
         a.m_prev = prev(t);
         a.n_cur = c->nbuf + size_t(t) * kRep;
         a.m_next = next(t);
-        a.xh = c->xm;
-        a.xl = c->xm + size_t(kRep) * npad;
+        a.x = c->xm;
         a.n_next = c->nbuf + size_t(t + 1) * kRep;
         a.P_out = pout(t);
         mf_fwd_kernel<<<kRep, kElemThreads, 0, st>>>(a);
@@ -359,8 +393,8 @@ int mf_create(const int8_t* J, const int32_t* bias, int n, MfContext** out, std:
               check(cudaMemcpy(c->bias, bh.data(), npad * sizeof(float), cudaMemcpyHostToDevice), "upload bias", why) &&
               check(cudaMalloc(&c->partial, size_t(npad / kKC) * plane * sizeof(float)), "cudaMalloc", why) &&
               check(cudaMalloc(&c->mring, 3 * plane * sizeof(float)), "cudaMalloc", why) &&
-              check(cudaMalloc(&c->xm, 2 * plane * sizeof(__nv_bfloat16)), "cudaMalloc", why) &&
-              check(cudaMalloc(&c->xp, 2 * plane * sizeof(__nv_bfloat16)), "cudaMalloc", why) &&
+              check(cudaMalloc(&c->xm, 3 * plane * sizeof(__nv_bfloat16)), "cudaMalloc", why) &&
+              check(cudaMalloc(&c->xp, 3 * plane * sizeof(__nv_bfloat16)), "cudaMalloc", why) &&
               check(cudaMalloc(&c->seg_m, (kMfCheckpoint + 2) * plane * sizeof(float)), "cudaMalloc", why) &&
               check(cudaMalloc(&c->seg_P, kMfCheckpoint * plane * sizeof(float)), "cudaMalloc", why) &&
               check(cudaMalloc(&c->pbar, 3 * plane * sizeof(float)), "cudaMalloc", why) &&
@@ -368,11 +402,10 @@ int mf_create(const int8_t* J, const int32_t* bias, int n, MfContext** out, std:
               check(cudaMalloc(&c->err, sizeof(int)), "cudaMalloc", why) &&
               check(cudaMemset(c->err, 0, sizeof(int)), "cudaMemset", why);
     if (ok) {
-        ok = make_map_2d(&c->mapJ, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, c->J, npad, npad, 64, kRows) &&
-             make_map_2d(&c->mapXmh, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, c->xm, npad, kRep, 64, kRep) &&
-             make_map_2d(&c->mapXml, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, c->xm + plane, npad, kRep, 64, kRep) &&
-             make_map_2d(&c->mapXph, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, c->xp, npad, kRep, 64, kRep) &&
-             make_map_2d(&c->mapXpl, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, c->xp + plane, npad, kRep, 64, kRep);
+        ok = make_map_2d(&c->mapJ, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, c->J, npad, npad, 64, kRows);
+        for (int k = 0; k < 3 && ok; ++k)
+            ok = make_map_2d(&c->mapXm[k], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, c->xm + k * plane, npad, kRep, 64, kRep) &&
+                 make_map_2d(&c->mapXp[k], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, c->xp + k * plane, npad, kRep, 64, kRep);
         if (!ok && why) *why = "cuTensorMapEncodeTiled failed";
     }
     if (!ok) {
@@ -397,7 +430,7 @@ int mf_forward(MfContext* c, int S, const float* beta, const float* q, const flo
     if (!check(cudaMemcpyAsync(mslot(ring, 0, npad), mprev, plane * 4, cudaMemcpyDeviceToDevice, st), "copy", why) ||
         !check(cudaMemcpyAsync(mslot(ring, 1, npad), m0, plane * 4, cudaMemcpyDeviceToDevice, st), "copy", why))
         return -2;
-    mf_prep_kernel<<<kRep, kElemThreads, 0, st>>>(mslot(ring, 1, npad), c->n, npad, c->nbuf, c->xm, c->xm + plane);
+    mf_prep_kernel<<<kRep, kElemThreads, 0, st>>>(mslot(ring, 1, npad), c->n, npad, c->nbuf, c->xm);
     if (!check(cudaGetLastError(), "mean-field prep", why)) return -2;
     // m_t lives in ring slot (t + 1) % 3, m_{t-1} in slot t % 3
     for (int t0 = 0; t0 < S; t0 += kMfCheckpoint) {
@@ -439,7 +472,7 @@ int mf_backward(MfContext* c, int S, const float* beta, const float* q, const fl
                    why))
             return -2;
         mf_prep_kernel<<<kRep, kElemThreads, 0, st>>>(mslot(c->seg_m, 1, npad), c->n, npad,
-                                                     c->nbuf + size_t(t0) * kRep, c->xm, c->xm + plane);
+                                                     c->nbuf + size_t(t0) * kRep, c->xm);
         if (!check(cudaGetLastError(), "mean-field prep", why)) return -2;
         rc = run_steps(
             c, t0, t1, beta, q, u, w, [&](int t) { return mslot(c->seg_m, t - t0 + 1, npad); },
@@ -450,7 +483,7 @@ int mf_backward(MfContext* c, int S, const float* beta, const float* q, const fl
         for (int t = t1 - 1; t >= t0; --t) {
             const bool last = t == S - 1;
             if (!last) {
-                rc = gemm(c, c->mapXph, c->mapXpl, st, why);
+                rc = gemm(c, c->mapXp, st, why);
                 if (rc) return rc;
             }
             BwdArgs a{};
@@ -475,8 +508,7 @@ int mf_backward(MfContext* c, int S, const float* beta, const float* q, const fl
             a.P = mslot(c->seg_P, t - t0, npad);
             a.n_cur = c->nbuf + size_t(t) * kRep;
             a.pbar = mslot(c->pbar, t % 3, npad);
-            a.xh = c->xp;
-            a.xl = c->xp + plane;
+            a.x = c->xp;
             a.s_out = c->svec + (t % 3) * kRep;
             a.gsched = gsched;
             mf_bwd_kernel<<<kRep, kElemThreads, 0, st>>>(a);

@@ -112,8 +112,9 @@ class Tables:
         return bool(np.any(self.arrays()["kcorr"] != 0))
 
     def __del__(self):
-        if getattr(self, "_h", None) and _lib._lib is not None and self._h.value:
-            _lib._lib.anc_tables_destroy(self._h)
+        lib = getattr(_lib, "_lib", None) if _lib is not None else None
+        if getattr(self, "_h", None) and lib is not None and self._h.value:
+            lib.anc_tables_destroy(self._h)
             self._h = C.c_void_p()
 
 
@@ -172,8 +173,9 @@ class DeviceInstance:
         return dict(plain_ok=bool(ok.value), hclamp=hc.value)
 
     def __del__(self):
-        if getattr(self, "_h", None) and _lib._lib is not None and self._h.value:
-            _lib._lib.anc_instance_destroy(self._h)
+        lib = getattr(_lib, "_lib", None) if _lib is not None else None
+        if getattr(self, "_h", None) and lib is not None and self._h.value:
+            lib.anc_instance_destroy(self._h)
             self._h = C.c_void_p()
 
 

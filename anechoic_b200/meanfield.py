@@ -97,8 +97,9 @@ class MeanField:
         return out
 
     def __del__(self):
-        if getattr(self, "_h", None) and _lib._lib is not None and self._h.value:
-            _lib._lib.anc_mf_destroy(self._h)
+        lib = getattr(_lib, "_lib", None) if _lib is not None else None
+        if getattr(self, "_h", None) and lib is not None and self._h.value:
+            lib.anc_mf_destroy(self._h)
             self._h = C.c_void_p()
 
 
@@ -199,12 +200,16 @@ def _llround(x: float) -> int:
     return int(math.floor(x + 0.5)) if x >= 0 else -int(math.floor(-x + 0.5))
 
 
-def soft_cut(inst: Instance, m: torch.Tensor, J: Optional[torch.Tensor] = None) -> torch.Tensor:
+def soft_cut(inst: Instance, m: torch.Tensor, J: Optional[torch.Tensor] = None,
+             sumw: Optional[int] = None) -> torch.Tensor:
     """Cut of magnetisations m [R, n] by the golden model's formula (sumw + m^T J m / 2) / 2 (sca_ref.hpp:153
-    without the integer truncation); equals the exact cut for m in {-1, +1}^n."""
+    without the integer truncation); equals the exact cut for m in {-1, +1}^n. Pass J (on m's device) and sumw to
+    avoid recomputing them."""
     if J is None:
         J = torch.as_tensor(inst.to_dense(), dtype=m.dtype, device=m.device)
-    return (inst.stats()["sumw"] + 0.5 * ((m @ J) * m).sum(dim=1)) / 2.0
+    if sumw is None:
+        sumw = inst.stats()["sumw"]
+    return (sumw + 0.5 * ((m @ J.to(m.dtype)) * m).sum(dim=1)) / 2.0
 
 
 def initial_magnetisations(n: int, R: int, seed: int) -> torch.Tensor:
@@ -221,6 +226,7 @@ def tune(inst: Instance, S: int = 200, R: int = 64, theta0=(30.0, math.log(6.0),
     sch = SoftSchedule(S=S, mode=mode)
     m0 = mf.pad(initial_magnetisations(inst.n, R, seed))
     J = torch.as_tensor(inst.to_dense(), dtype=torch.float32, device="cuda")
+    sumw = inst.stats()["sumw"]
     raw = torch.tensor([math.log(theta0[0]), math.log(max(theta0[1], 1e-3)), theta0[2], theta0[3], theta0[4]],
                        dtype=torch.float64, device="cuda", requires_grad=True)
     opt = torch.optim.Adam([raw], lr=lr)
@@ -229,11 +235,11 @@ def tune(inst: Instance, S: int = 200, R: int = 64, theta0=(30.0, math.log(6.0),
         theta = torch.stack([raw[0].exp(), raw[1].exp(), raw[2], raw[3], raw[4]])
         beta, q, u, w = sch.vectors(theta)
         mS = relax(mf, beta, q, u, w, m0)
-        cut = soft_cut(inst, mS[:R, : inst.n], J).mean()
+        cut = soft_cut(inst, mS[:R, : inst.n], J, sumw).mean()
         opt.zero_grad()
         (-cut).backward()
         opt.step()
-        hist.append((it, float(cut), [float(x) for x in theta.detach().tolist()]))
+        hist.append((it, cut.item(), [float(x) for x in theta.detach().tolist()]))
         if log:
             log(hist[-1])
     theta = torch.stack([raw[0].exp(), raw[1].exp(), raw[2], raw[3], raw[4]]).detach()

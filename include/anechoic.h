@@ -216,7 +216,7 @@ ANC_API int anc_run_batch_noalloc(int njobs, const anc_device_job* jobs, void* s
  * (kappa T_{t-1} temperature-scaled, -jv constant): the tanh form of the reference's effective process
  * (research/dmft_sca_20261004/dmft_torch.py:38-57) and the soft version of sca_ref.hpp:118-131.
  * J in BF16 (exact for the integer couplings), f32 magnetisations and accumulation (tcgen05 kind::f16 GEMM with m
- * split into BF16 hi + lo), checkpoints every 16 steps in the adjoint. All pointers below are DEVICE pointers;
+ * split into three BF16 terms), checkpoints every 16 steps in the adjoint. All pointers below are DEVICE pointers;
  * calls are asynchronous on `stream` (NULL = default); anc_mf_check synchronises and reports a device wait timeout.
  *   sched:  [4][S] f32 rows beta, q, u, w
  *   m0, mprev, m_out: [64][npad] f32 (rows = replicas; unused rows and columns i >= n stay zero)

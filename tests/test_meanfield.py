@@ -2,10 +2,17 @@
 checkpoints every 16 steps) against the FP64 oracle (oracle/meanfield_ref.py, torch float64 autograd) and central
 finite differences; and exact-engine parity under a tuned (q-ramped) schedule.
 
-Stated error (floating point, so tolerances are written here): the kernels hold m in f32 and feed it to the tensor
-cores as a BF16 hi + lo pair (about 16 significant bits); J is exact in BF16.
-  forward  max |m_S - m_S(fp64)| <= 2e-3 (64 replicas x 200 steps on the N=2000 +-1 instance)
-  gradient relative error of each of the five schedule derivatives <= 2e-2 against FP64 autograd
+Stated error (floating point, so tolerances are written here). The kernels hold m in f32 and feed it to the tensor
+cores as three BF16 terms (24 significant bits); J is exact in BF16, so every product is exact, and the f32
+accumulation is split over five TMEM accumulators summed with round-to-nearest. Measured on B200: the J m product
+has rms error 2e-6 against fp64 (an f32 torch matmul: 2e-5).
+  one step (non-integer start)  max |m_1 - m_1(fp64)| <= 1e-6
+The synchronous recurrence amplifies rounding over many steps (a 1e-10 change of m_0 moves the fp64 gradient by
+3e-6 at 200 steps), so longer horizons are stated relative to an f32 torch implementation of the same recurrence and
+in the mean:
+  S steps   max |m_S - m_S(fp64)| <= 3 max |m_S(f32 torch) - m_S(fp64)| + 1e-5,  mean |m_S - m_S(fp64)| <= 1e-4
+  gradient  relative error of each of the five schedule derivatives <= 2e-2 against FP64 autograd (measured 8e-3
+            at 200 steps; f32 torch autograd: 0.32)
 """
 import math
 
@@ -24,10 +31,10 @@ pytestmark = pytest.mark.gpu
 THETA0 = (30.0, math.log(6.0), 4.0, 0.0, 1.05)     # reference default schedule, counted Onsager lambda 1.05
 
 
-def _case(inst, S, R, mode, theta, seed=1):
+def _case(inst, S, R, mode, theta, seed=1, m0=None):
     mf = MeanField(inst)
     sch = SoftSchedule(S=S, mode=mode)
-    m0r = initial_magnetisations(inst.n, R, seed)
+    m0r = initial_magnetisations(inst.n, R, seed) if m0 is None else m0.float()
     J64 = torch.as_tensor(inst.to_dense(), dtype=torch.float64, device="cuda")
     b64 = torch.zeros(inst.n, dtype=torch.float64, device="cuda") if inst.bias is None else \
         torch.as_tensor(inst.bias, dtype=torch.float64, device="cuda")
@@ -43,8 +50,21 @@ def _case(inst, S, R, mode, theta, seed=1):
     m64 = relax64(J64, b64, b_, q_, u_, w_, m0, torch.ones_like(m0))
     cut64 = soft_cut64(J64, sumw, m64).mean()
     cut64.backward()
-    return dict(mS=mS[:R, : inst.n].double(), m64=m64.detach(), g=th.grad.detach(), g64=th64.grad.detach(),
-                cut=float(cut), cut64=float(cut64))
+    tf32 = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    with torch.no_grad():
+        m32 = relax64(J64.float(), b64.float(), *(v.detach().float() for v in (b_, q_, u_, w_)), m0.float(),
+                      torch.ones_like(m0).float()).double()
+    torch.backends.cuda.matmul.allow_tf32 = tf32
+    return dict(mS=mS[:R, : inst.n].detach().double(), m64=m64.detach(), m32=m32, g=th.grad.detach(),
+                g64=th64.grad.detach(), cut=float(cut.detach()), cut64=float(cut64.detach()))
+
+
+def _check_forward(r):
+    err = (r["mS"] - r["m64"]).abs()
+    err32 = (r["m32"] - r["m64"]).abs().max().item()
+    assert err.max().item() <= 3 * err32 + 1e-5, (err.max().item(), err32)
+    assert err.mean().item() <= 1e-4, err.mean().item()
 
 
 def _rel(g, g64):
@@ -59,9 +79,11 @@ def pm1(cuda):
 
 def test_config4_forward_and_gradient_vs_fp64(pm1):
     """N=2000 +-1, 64 replicas, 200 unrolled steps, counted Onsager: forward and the five schedule gradients."""
+    mr = torch.rand(64, pm1.n, generator=torch.Generator().manual_seed(3)) * 2 - 1
+    one = _case(pm1, 1, 64, "counted", THETA0, m0=mr)
+    assert (one["mS"] - one["m64"]).abs().max().item() <= 1e-6
     r = _case(pm1, 200, 64, "counted", THETA0)
-    err = (r["mS"] - r["m64"]).abs().max().item()
-    assert err <= 2e-3, err
+    _check_forward(r)
     rel = _rel(r["g"], r["g64"])
     assert rel <= 2e-2, (rel, r["g"].tolist(), r["g64"].tolist())
     assert abs(r["cut"] - r["cut64"]) <= 1e-3 * abs(r["cut64"])
@@ -72,15 +94,16 @@ def test_other_corrections_and_ragged_checkpoints(cuda, mode):
     """K=2 couplings with bias, n = 700 (npad 768), S = 37 (two full checkpoint segments and a ragged one)."""
     inst = I.random_kbit(700, 2, 44, pzero=0.4, bmax=3)
     r = _case(inst, 37, 40, mode, (12.0, math.log(8.0), 1.0, 0.5, 1.5))
-    err = (r["mS"] - r["m64"]).abs().max().item()
-    assert err <= 2e-3, err
+    _check_forward(r)
     rel = _rel(r["g"], r["g64"])
     assert rel <= 2e-2, (rel, r["g"].tolist(), r["g64"].tolist())
 
 
 def test_kernel_gradient_vs_central_differences(pm1):
-    """dL/dtheta from the adjoint kernels against central differences of the kernels' own forward."""
-    S, R = 48, 64
+    """dL/dtheta from the adjoint kernels against central differences of the kernels' own forward, over one
+    checkpoint segment (16 steps), where the map is well conditioned; the 200-step gradient is checked against FP64
+    autograd above, and the FP64 oracle against central differences in tests/test_meanfield_oracle.py."""
+    S, R = 16, 64
     mf = MeanField(pm1)
     sch = SoftSchedule(S=S, mode="counted")
     m0 = mf.pad(initial_magnetisations(pm1.n, R, 5))
@@ -92,7 +115,7 @@ def test_kernel_gradient_vs_central_differences(pm1):
     th = torch.tensor(THETA0, dtype=torch.float64, device="cuda", requires_grad=True)
     loss(th).backward()
     for k in range(5):
-        h = 2e-3 * max(1.0, abs(THETA0[k]))
+        h = 1e-3 * max(1.0, abs(THETA0[k]))
         tp = torch.tensor(THETA0, dtype=torch.float64, device="cuda")
         tm = tp.clone()
         tp[k] += h
@@ -100,7 +123,7 @@ def test_kernel_gradient_vs_central_differences(pm1):
         with torch.no_grad():
             fd = (loss(tp) - loss(tm)).item() / (2 * h)
         g = th.grad[k].item()
-        assert abs(fd - g) <= 5e-2 * max(abs(fd), abs(g), 1.0), (k, fd, g)
+        assert abs(fd - g) <= 2e-2 * max(abs(fd), abs(g), 1.0), (k, fd, g)
 
 
 def test_tuned_schedule_runs_bit_exact_on_the_engine(pm1, oracle):
