@@ -247,10 +247,12 @@ int launch_plain_single(anc_instance* I, const anc::PlainJob& job, cudaStream_t 
     L.np_max = I->np;
     L.nwj_max = I->K == 0 ? I->nw : I->nwj;
     const int P = plain_P(I->np);
-    const size_t smem = anc::plain_smem_bytes(L.np_max, L.nwj_max, I->K, P);
+    bool stream = false;
+    const size_t smem = anc::plain_smem_plan(L.np_max, L.nwj_max, I->K, P, &stream);
     if (smem > 227 * 1024) return fail(ANC_EINVAL, "instance too large for the plain engine (%zu B shared memory)", smem);
+    L.stream = stream ? 1 : 0;
     int per_sm = 0;
-    int rc = anc::plain_max_blocks_per_sm(I->K, P, smem, &per_sm);
+    int rc = anc::plain_max_blocks_per_sm(I->K, P, smem, &per_sm, stream);
     if (rc) return cuda_fail(cudaError_t(rc), "occupancy");
     if (per_sm < 1) return fail(ANC_EINVAL, "plain engine cannot be resident (smem %zu)", smem);
     const int grid = std::max(1, std::min(job.ntrials, per_sm * I->sms));
@@ -795,10 +797,12 @@ int anc_run_batch(int njobs, const anc_job* jobs, const anc_run_opts* o) {
         L.np_max = np_max;
         L.nwj_max = nwj_max;
         const int P = plain_P(np_max);
-        const size_t smem = anc::plain_smem_bytes(np_max, nwj_max, K, P);
+        bool stream = false;
+        const size_t smem = anc::plain_smem_plan(np_max, nwj_max, K, P, &stream);
         if (smem > 227 * 1024) return fail(ANC_EINVAL, "batch instance too large for the plain engine");
+        L.stream = stream ? 1 : 0;
         int per_sm = 0;
-        int rc = anc::plain_max_blocks_per_sm(K, P, smem, &per_sm);
+        int rc = anc::plain_max_blocks_per_sm(K, P, smem, &per_sm, stream);
         if (rc) return cuda_fail(cudaError_t(rc), "occupancy");
         if (per_sm < 1) return fail(ANC_EINVAL, "plain engine cannot be resident");
         const int grid = std::max(1, std::min(L.nitems, per_sm * sms));
@@ -930,10 +934,12 @@ extern "C" int anc_run_batch_noalloc(int njobs, const anc_device_job* jobs, void
         L.np_max = np_max;
         L.nwj_max = nwj_max;
         const int P = plain_P(np_max);
-        const size_t smem = anc::plain_smem_bytes(np_max, nwj_max, K, P);
+        bool stream = false;
+        const size_t smem = anc::plain_smem_plan(np_max, nwj_max, K, P, &stream);
         if (smem > 227 * 1024) return fail(ANC_EINVAL, "instance too large for the plain engine");
+        L.stream = stream ? 1 : 0;
         int per_sm = 0;
-        int rc = anc::plain_max_blocks_per_sm(K, P, smem, &per_sm);
+        int rc = anc::plain_max_blocks_per_sm(K, P, smem, &per_sm, stream);
         if (rc) return cuda_fail(cudaError_t(rc), "occupancy");
         if (per_sm < 1) return fail(ANC_EINVAL, "plain engine cannot be resident");
         rc = anc::plain_launch(L, K, P, std::max(1, std::min(cnt, per_sm * sms)), smem, st);

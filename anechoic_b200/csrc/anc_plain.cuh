@@ -11,7 +11,9 @@
 //      its group (coalesced: a warp reads 128 contiguous bytes of one row) and adds it into bit-sliced counters with
 //      carry-save adders (a Harley-Seal tree over batches of 8 rows, LOP3 arithmetic, 32 couplings per op). The
 //      groups' counters are summed by a bit-sliced adder tree in shared memory; the deciding thread of slot y
-//      extracts y's count at the start of the next step, when it reads h_y.
+//      extracts y's count at the start of the next step, when it reads h_y. When the counters of all 2(K-1)
+//      sign/magnitude sets do not fit in shared memory (N = 16384, K = 4), each set is added into the fields as soon
+//      as it is complete (streaming layout, one result buffer).
 //      Sparse couplings (CSR rows) are scattered with shared-memory atomics, one warp per flipped row.
 //   The initial field h = b + J s0 reuses step 2 with F = all active slots and factor 1.
 // All arithmetic is integer and order-independent, so the result is bit-exact with the golden model.
@@ -53,11 +55,12 @@ struct PlainLaunch {
     int nitems;
     int* next_item;                    // queue head (zeroed before launch)
     int np_max, nwj_max;               // shared-memory layout
+    int stream;                        // 1: dense counts go into the fields set by set (one result buffer)
 };
 
 // Shared-memory bytes for a launch (P = counter planes).
-inline size_t plain_smem_bytes(int np_max, int nwj_max, int K, int P) {
-    const size_t C = K <= 1 ? 1 : size_t(2 * (K - 1));
+inline size_t plain_smem_bytes(int np_max, int nwj_max, int K, int P, bool stream = false) {
+    const size_t C = (K <= 1 || stream) ? 1 : size_t(2 * (K - 1));
     size_t b = size_t(np_max) * 4 * 2 + size_t(nwj_max) * 4 * 2;
     if (K != 0) {
         const size_t comb = size_t(nwj_max > kPlainThreads ? nwj_max : kPlainThreads);
@@ -66,8 +69,18 @@ inline size_t plain_smem_bytes(int np_max, int nwj_max, int K, int P) {
     return b;
 }
 
+// Shared-memory plan of a launch: the full layout when it fits in 227 KB; otherwise, for K = 2 / 4 with at most one
+// counter word per thread (N <= 16384), the streaming layout, where each of the 2(K-1) sign/magnitude counter sets
+// is added into the fields as soon as it is complete, so one result buffer serves them all (*stream = true).
+inline size_t plain_smem_plan(int np_max, int nwj_max, int K, int P, bool* stream) {
+    constexpr size_t kLimit = 227 * 1024;
+    const size_t full = plain_smem_bytes(np_max, nwj_max, K, P, false);
+    *stream = K >= 2 && full > kLimit && nwj_max <= kPlainThreads;
+    return *stream ? plain_smem_bytes(np_max, nwj_max, K, P, true) : full;
+}
+
 // Host launcher (plain_engine.cu). Returns a cudaError_t value.
 int plain_launch(const PlainLaunch& L, int K, int P, int grid, size_t smem, cudaStream_t stream);
-int plain_max_blocks_per_sm(int K, int P, size_t smem, int* out);
+int plain_max_blocks_per_sm(int K, int P, size_t smem, int* out, bool stream = false);
 
 }  // namespace anc

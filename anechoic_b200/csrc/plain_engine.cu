@@ -82,10 +82,23 @@ __device__ __forceinline__ int64_t warp_sum64(int64_t v) {
     return v;
 }
 
-// Dense field pass: bit-sliced counts of the flipped rows, combined across groups into res[cc][w][P].
-template <int K, int P>
+// Streaming layout: add counter set cc (sign/magnitude pair (b, +/-), weight +/- 2^(b-1)) of slots y < n, held in
+// res[w][P], into the fields: h_y += mult * (+/-) count_y << (b - 1). Ends with a CTA barrier.
+template <int P>
+__device__ __forceinline__ void stream_apply(const uint32_t* res, int cc, int32_t* h, int n, int mult) {
+    __syncthreads();
+    const int32_t m = (cc & 1) ? -mult : mult;
+    const int sh = cc >> 1;
+    for (int y = threadIdx.x; y < n; y += T) h[y] += m * (extract_count<P>(res + size_t(y >> 5) * P, y & 31) << sh);
+    __syncthreads();
+}
+
+// Dense field pass: bit-sliced counts of the flipped rows, combined across groups into res[cc][w][P]; with STREAM
+// (K >= 2, nwj <= T) each set cc is instead combined into res[w][P] and added into h (factor mult) right away.
+template <int K, int P, bool STREAM>
 __device__ __forceinline__ void dense_pass(const uint32_t* __restrict__ planes, size_t plane_stride, int nwj, int nf,
-                                           const uint32_t* flist, uint32_t* comb, uint32_t* res) {
+                                           const uint32_t* flist, uint32_t* comb, uint32_t* res, int32_t* h, int n,
+                                           int mult) {
     constexpr int NC = K <= 1 ? 1 : 2 * (K - 1);
     const int tid = threadIdx.x;
     if (nwj <= T) {
@@ -125,6 +138,14 @@ __device__ __forceinline__ void dense_pass(const uint32_t* __restrict__ planes, 
             }
         }
         if (G == 1) {
+            if (STREAM) {
+#pragma unroll
+                for (int cc = 0; cc < NC; ++cc) {
+                    if (active) cnt[cc].store(res + size_t(w) * P);
+                    stream_apply<P>(res, cc, h, n, mult);
+                }
+                return;
+            }
             if (active) {
 #pragma unroll
                 for (int cc = 0; cc < NC; ++cc) cnt[cc].store(res + (size_t(cc) * nwj + w) * P);
@@ -144,7 +165,12 @@ __device__ __forceinline__ void dense_pass(const uint32_t* __restrict__ planes, 
                 }
                 __syncthreads();
             }
-            if (active && g == 0) cnt[cc].store(res + (size_t(cc) * nwj + w) * P);
+            if (STREAM) {
+                if (active && g == 0) cnt[cc].store(res + size_t(w) * P);
+                stream_apply<P>(res, cc, h, n, mult);
+            } else if (active && g == 0) {
+                cnt[cc].store(res + (size_t(cc) * nwj + w) * P);
+            }
         }
     } else {
         for (int w0 = 0; w0 < nwj; w0 += T) {
@@ -209,7 +235,7 @@ __device__ __forceinline__ int32_t dense_delta(const uint32_t* res, int nwj, int
     }
 }
 
-template <int K, int P, bool SPARSE>
+template <int K, int P, bool SPARSE, bool STREAM>
 __global__ void __launch_bounds__(T, 1) plain_kernel(const __grid_constant__ PlainLaunch L) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
     __shared__ int s_item, s_nf[2], s_lin[8];
@@ -278,8 +304,8 @@ __global__ void __launch_bounds__(T, 1) plain_kernel(const __grid_constant__ Pla
                 }
             }
         } else {
-            dense_pass<K, P>(planes, plane_stride, nwj, pass_nf, flist, comb, res);
-            pass_pending = true;
+            dense_pass<K, P, STREAM>(planes, plane_stride, nwj, pass_nf, flist, comb, res, h, n, 1);
+            pass_pending = !STREAM;
         }
         __syncthreads();
 
@@ -344,8 +370,8 @@ __global__ void __launch_bounds__(T, 1) plain_kernel(const __grid_constant__ Pla
                         }
                     }
                 } else {
-                    dense_pass<K, P>(planes, plane_stride, nwj, nf, flist, comb, res);
-                    pass_pending = true;
+                    dense_pass<K, P, STREAM>(planes, plane_stride, nwj, nf, flist, comb, res, h, n, 2);
+                    pass_pending = !STREAM;
                 }
             }
             __syncthreads();
@@ -383,18 +409,18 @@ __global__ void __launch_bounds__(T, 1) plain_kernel(const __grid_constant__ Pla
     }
 }
 
-template <int K, int P, bool SPARSE>
+template <int K, int P, bool SPARSE, bool STREAM = false>
 int launch_t(const PlainLaunch& L, int grid, size_t smem, cudaStream_t st) {
-    auto fn = plain_kernel<K, P, SPARSE>;
+    auto fn = plain_kernel<K, P, SPARSE, STREAM>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return int(e);
     fn<<<grid, T, smem, st>>>(L);
     return int(cudaGetLastError());
 }
 
-template <int K, int P, bool SPARSE>
+template <int K, int P, bool SPARSE, bool STREAM = false>
 int occ_t(size_t smem, int* out) {
-    auto fn = plain_kernel<K, P, SPARSE>;
+    auto fn = plain_kernel<K, P, SPARSE, STREAM>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return int(e);
     return int(cudaOccupancyMaxActiveBlocksPerMultiprocessor(out, fn, T, smem));
@@ -402,9 +428,15 @@ int occ_t(size_t smem, int* out) {
 
 }  // namespace
 
-// K: 0 = sparse, 1/2/4 dense planes. P: 12 or 16 counter planes (dense only).
+// K: 0 = sparse, 1/2/4 dense planes. P: 12 or 16 counter planes (dense only). L.stream selects the streaming layout
+// (K = 2 / 4, P = 16 only: it is needed only for NP > 8192).
 int plain_launch(const PlainLaunch& L, int K, int P, int grid, size_t smem, cudaStream_t st) {
     if (K == 0) return launch_t<1, 12, true>(L, grid, smem, st);
+    if (L.stream) {
+        if (P == 16 && K == 2) return launch_t<2, 16, false, true>(L, grid, smem, st);
+        if (P == 16 && K == 4) return launch_t<4, 16, false, true>(L, grid, smem, st);
+        return int(cudaErrorInvalidValue);
+    }
     if (P == 12) {
         if (K == 1) return launch_t<1, 12, false>(L, grid, smem, st);
         if (K == 2) return launch_t<2, 12, false>(L, grid, smem, st);
@@ -417,8 +449,13 @@ int plain_launch(const PlainLaunch& L, int K, int P, int grid, size_t smem, cuda
     return int(cudaErrorInvalidValue);
 }
 
-int plain_max_blocks_per_sm(int K, int P, size_t smem, int* out) {
+int plain_max_blocks_per_sm(int K, int P, size_t smem, int* out, bool stream) {
     if (K == 0) return occ_t<1, 12, true>(smem, out);
+    if (stream) {
+        if (P == 16 && K == 2) return occ_t<2, 16, false, true>(smem, out);
+        if (P == 16 && K == 4) return occ_t<4, 16, false, true>(smem, out);
+        return int(cudaErrorInvalidValue);
+    }
     if (P == 12) {
         if (K == 1) return occ_t<1, 12, false>(smem, out);
         if (K == 2) return occ_t<2, 12, false>(smem, out);

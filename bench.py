@@ -378,6 +378,76 @@ def bench_ours(args, ws, rank, local):
     return 0
 
 
+# ------------------------------------------------------------------------------------------------ other workloads
+def bench_workload(args, ws, rank, local):
+    """Opt-in single-GPU workloads (one JSON line each; the default line above is the headline):
+    sparse51  51 synthetic sparse instances of uneven size (N = 800 .. 20000; G-set-shaped classes, weights +1 or
+              iid +-1, K = 2 range with integer bias in [-2, 2]), 64 anneals each, all in ONE persistent launch of
+              the plain engine (CSR path); temperature-scaled correction kappa 2 with ramp, S = 1000.
+    dense16k  N = 16384 complete graph, couplings iid uniform in [-7, 7] (K = 4) with bias uniform in [-7, 7],
+              256 anneals, S = 5000, counted Onsager lambda 1.05 with ramp (the range plan's exact clamp is active)."""
+    import numpy as np
+    import torch
+    import anechoic_b200 as A
+    from anechoic_b200 import instances as I
+    torch.cuda.set_device(local)
+    if args.workload == "sparse51":
+        insts = [b() for _, b in I.sparse_classes_manifest()]
+        sched = dict(S=1000, t0=6.0, t1=0.5, q=1.5, kappa=2.0, ramp=True)
+        per = 64
+        desc = "51 sparse instances N=800..20000 (K=2 range, bias), 64 anneals each, one persistent launch"
+    else:
+        insts = [I.random_kbit(16384, 4, 20261009, pzero=0.0, bmax=7)]
+        sched = dict(S=5000, t0=float(2 * np.sqrt(16384) * 4), t1=2.0, q=4.0, lam=1.05, ramp=True)
+        per = 256
+        desc = "N=16384 complete, J uniform [-7,7] (K=4), bias [-7,7], 256 anneals, S=5000"
+    devs = [A.DeviceInstance(i) for i in insts]
+    tb = A.Tables.from_schedule(A.Schedule(**sched))
+
+    def jobs(step):
+        return [dict(dev=d, tb=tb, seed=RUN_SEED, trial_offset=(step << 12) + 64 * k, nchains=per)
+                for k, d in enumerate(devs)]
+
+    def launch(step):
+        return A.run_batch(jobs(step), engine=args.engine) if len(devs) > 1 else \
+            [A.run(devs[0], tb, RUN_SEED, step << 12, per, engine=args.engine)]
+
+    for w in range(args.warmup):
+        launch(1000 + w)
+    ms, flips = [], 0
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            outs = launch(k)
+            ms.append(outs[0].device_ms)
+            flips += sum(int(o.flips.sum()) for o in outs)
+    t = sum(ms) / len(ms)
+    anneals = per * len(devs)
+    S = sched["S"]
+    # algorithmic bytes per launch: coupling rows of flipped spins (CSR entries of 4 B, or K bit planes of N/8 B)
+    # plus fields (8 B) and spin bits (1/4 B) per slot and step
+    mean_flips = flips / args.steps
+    if args.workload == "sparse51":
+        row_bytes = sum(4.0 * (len(i.col) / i.n) for i in insts) / len(insts)
+        slot_bytes = sum(i.n for i in insts) * per * S * 8.25
+    else:
+        row_bytes = 4 * 16384 / 8
+        slot_bytes = 16384 * per * S * 8.25
+    alg = mean_flips * row_bytes + slot_bytes
+    hbm, _, peak_kind = measured_peaks()
+    ach = alg / (t / 1000.0) / 1e9
+    line = {"metric": "anneals/s", "workload": args.workload, "value": anneals / (t / 1000.0), "unit": "anneals/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t, "higher_is_better": True,
+            "dtype": "int32", "data": "synthetic", "config": {"workload": desc, "S": S, "anneals": anneals,
+                                                              "engine": args.engine},
+            "mean_flips_per_anneal_step": mean_flips / (anneals * S),
+            "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                         "peak_kind": peak_kind, "algorithmic_per_launch": alg},
+            "gpu_launches": args.steps, "clocks": clk.summary()}
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -388,10 +458,14 @@ def main():
     ap.add_argument("--tensor-kind", default="auto", choices=["auto", "int8", "fp4"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-engine comparison run")
+    ap.add_argument("--workload", default="pm1", choices=["pm1", "sparse51", "dense16k"],
+                    help="pm1: the headline line (default); the others print their own opt-in line")
     args = ap.parse_args()
     ws, rank, local = dist_env()
     if args.impl == "reference":
         return bench_reference(args, ws, rank)
+    if args.workload != "pm1":
+        return bench_workload(args, ws, rank, local)
     return bench_ours(args, ws, rank, local)
 
 

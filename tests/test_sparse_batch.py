@@ -1,0 +1,44 @@
+"""GPU parity of the 51-instance sparse batch (uneven sizes N = 800 .. 20000: Erdos-Renyi p = 0.06 at N = 800,
+degree-~6 and degree-~12 random graphs, 2-D toroidal grids; weights +1 or iid +-1; K = 2 planes with integer bias;
+temperature-scaled correction) in ONE persistent launch of the plain engine (CSR path: adjacency rows in shared
+memory, integer weights), against the golden-model restatement:
+every spin, flip count, sum s*h, sum b*s and n_lin step of every anneal."""
+import pytest
+
+import anechoic_b200 as A
+from anechoic_b200 import instances as I
+from tests.test_parity_plain import assert_same
+
+pytestmark = pytest.mark.gpu
+
+SCHED = dict(S=60, t0=6.0, t1=0.5, q=1.5, kappa=2.0, ramp=True)
+
+
+@pytest.fixture(scope="module")
+def batch(cuda):
+    insts = [(name, build()) for name, build in I.sparse_classes_manifest()]
+    assert len(insts) == 51 and max(i.n for _, i in insts) == 20000
+    tb = A.Tables.from_schedule(A.Schedule(**SCHED))
+    devs = [A.DeviceInstance(i) for _, i in insts]
+    for (_, i), d in zip(insts, devs):
+        assert i.stats()["maxabs"] == 1 and d.info["sparse"] == 1   # K = 2 range, CSR storage
+    jobs = [dict(dev=d, tb=tb, seed=20261008, trial_offset=1000 * k, nchains=2, trace=True) for k, d in enumerate(devs)]
+    return insts, A.run_batch(jobs)
+
+
+def test_every_instance_vs_oracle(batch, oracle):
+    insts, outs = batch
+    otb = oracle.tables(**SCHED)
+    for k, ((name, inst), r) in enumerate(zip(insts, outs)):
+        ref = oracle.run_batch(inst.n, otb, 20261008, 1000 * k, 2, csr=inst.to_csr(), bias=inst.bias)
+        for c in range(2):
+            assert_same(r, {kk: v[c] for kk, v in ref.items()}, c, f"{name} chain {c}")
+
+
+def test_energies_rescored_on_the_host(batch):
+    """Device energy E = -(sum s*h + sum b*s)/2 equals an independent rescoring of the returned spins."""
+    insts, outs = batch
+    for (name, inst), r in zip(insts, outs):
+        e = r.energies()
+        for c in range(2):
+            assert int(e[c]) == inst.energy(r.spins[c]), name
