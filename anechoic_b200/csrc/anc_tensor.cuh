@@ -10,6 +10,8 @@ namespace anc {
 
 struct TensorInstance {
     int n = 0, np = 0;
+    int npp = 0;                 // permuted width of J_perm (np, or 16384 for the streaming kernel)
+    bool stream = false;         // 32 < NP/256 <= 64: J streamed from HBM (tensor_stream.cu)
     std::vector<int> perm;       // slot i -> permuted index (CTA-contiguous slot slices)
     int8_t* d_J = nullptr;       // J_perm [np][np] int8 (row = y, contiguous x)
     size_t bytes = 0;
@@ -60,6 +62,11 @@ int tensor_run(TensorInstance* ti, const TensorRun& r, cudaStream_t st, std::str
 // Whether the fp4 kernel can run this instance with this bias bound exactly (the fields stay far inside the range
 // where fp32 accumulation of integers is exact).
 bool tensor_fp4_eligible(const TensorInstance* ti, int64_t bias_absmax);
+// Streaming kernel for NP in (8192, 16384] (tensor_stream.cu): support test, slot permutation, permuted width, launch.
+bool stream_supported(int n);
+void stream_permutation(int np, std::vector<int>* p);
+int stream_width();
+int stream_run(TensorInstance* ti, const TensorRun& r, const int32_t* bias_perm, cudaStream_t st, std::string* why);
 // After the stream has reached the launch: -3 if a bounded device wait expired, 0 otherwise.
 int tensor_check_error(TensorInstance* ti, cudaStream_t st, std::string* why);
 void tensor_free_instance(TensorInstance* ti);

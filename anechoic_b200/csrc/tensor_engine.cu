@@ -1306,6 +1306,12 @@ int res_pair_slots(int npairs, int* out) {
 int tensor_geometry(int n, int nchains, TensorGeometry* g) {
     const int np = std::max(2048, ((n + 255) / 256) * 256);
     const int R = np / 256;
+    if (stream_supported(n)) {
+        g->cluster = 1;
+        g->ctas = 128;
+        g->max_active_clusters = 128;
+        return 0;
+    }
     if (R == 8) {
         const int npairs = ((nchains + kM - 1) / kM + 1) / 2;
         int slots = 0;
@@ -1317,7 +1323,6 @@ int tensor_geometry(int n, int nchains, TensorGeometry* g) {
     }
     g->cluster = kC;
     g->ctas = kC * ((nchains + kM - 1) / kM);
-    if (R == 8) return max_clusters_t<8>(&g->max_active_clusters);
     if (R == 12) return max_clusters_t<12>(&g->max_active_clusters);
     if (R == 16) return max_clusters_t<16>(&g->max_active_clusters);
     return int(cudaErrorInvalidValue);
@@ -1327,34 +1332,43 @@ bool tensor_supported(int n, int K, int nchains) {
     (void)K;
     const int np = std::max(2048, ((n + 255) / 256) * 256);
     const int R = np / 256;
-    return nchains >= 1 && (R == 8 || R == 12 || R == 16);
+    return nchains >= 1 && (R == 8 || R == 12 || R == 16 || stream_supported(n));
 }
 
 bool tensor_prefer(int n, int K, int nchains, int S) {
     (void)S;
+    // the streaming kernel reads J once per step for two replica groups; the plain engine reads the flipped rows of
+    // every anneal, which no longer fit in L2 at these sizes
+    if (stream_supported(n)) return tensor_supported(n, K, nchains) && nchains >= 64;
     return tensor_supported(n, K, nchains) && nchains >= 256;
 }
 
 int tensor_build_instance(const int8_t* J, int n, TensorInstance* out, std::string* why) {
     const int np = std::max(2048, ((n + 255) / 256) * 256);
     const int R = np / 256, nc = 16 * R;
-    if (!(R == 8 || R == 12 || R == 16)) {
-        if (why) *why = "tensor engine supports NP in {2048, 3072, 4096}";
+    if (!(R == 8 || R == 12 || R == 16 || stream_supported(n))) {
+        if (why) *why = "tensor engine supports NP in {2048, 3072, 4096} and (8192, 16384]";
         return -1;
     }
+    const bool big = stream_supported(n);
     std::vector<int> p(np);
-    for (int i = 0; i < np; ++i) {
-        const int l = i % 256, k = i / 256, cc = l / 16, jl = l % 16;
-        p[i] = cc * nc + jl * R + k;
+    if (big) {
+        stream_permutation(np, &p);
+    } else {
+        for (int i = 0; i < np; ++i) {
+            const int l = i % 256, k = i / 256, cc = l / 16, jl = l % 16;
+            p[i] = cc * nc + jl * R + k;
+        }
     }
-    std::vector<int8_t> Jp(size_t(np) * np, 0);
+    const int npp = big ? stream_width() : np;
+    std::vector<int8_t> Jp(size_t(npp) * npp, 0);
     bool unit = true;
     int64_t rowmax = 0;
     for (int x = 0; x < n; ++x) {
         int64_t rs = 0;
         for (int y = 0; y < n; ++y) {
             const int8_t v = J[size_t(x) * n + y];
-            Jp[size_t(p[y]) * np + p[x]] = v;   // row = y (N), col = x (K)
+            Jp[size_t(p[y]) * npp + p[x]] = v;   // row = y (N), col = x (K)
             rs += v < 0 ? -v : v;
             unit = unit && v >= -1 && v <= 1;
         }
@@ -1362,11 +1376,13 @@ int tensor_build_instance(const int8_t* J, int n, TensorInstance* out, std::stri
     }
     out->n = n;
     out->np = np;
+    out->npp = npp;
+    out->stream = big;
     out->perm.assign(p.begin(), p.end());
     out->rowsum_max = rowmax;
     cudaError_t e = cudaMalloc(&out->d_J, Jp.size());
     if (e == cudaSuccess) e = cudaMemcpy(out->d_J, Jp.data(), Jp.size(), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess && unit && R == 8) {
+    if (e == cudaSuccess && unit && R == 8 && !big) {
         // packed e2m1, two per byte (even K index in the low nibble): +1 -> 0x2, -1 -> 0xA, 0 -> 0x0
         std::vector<uint8_t> J4(size_t(np) * np / 2, 0);
         for (size_t y = 0; y < size_t(np); ++y)
@@ -1397,15 +1413,15 @@ namespace {
 // Permuted bias on the device (built once per instance from the caller's device bias) and its max |b|.
 int ensure_bias_perm(TensorInstance* ti, const int32_t* bias, std::string* why) {
     if (!bias || ti->d_bias_perm) return 0;
-    std::vector<int32_t> b(ti->n), bp(ti->np, 0);
+    std::vector<int32_t> b(ti->n), bp(ti->npp, 0);
     cudaError_t e = cudaMemcpy(b.data(), bias, size_t(ti->n) * 4, cudaMemcpyDeviceToHost);
     int64_t mx = 0;
     for (int i = 0; i < ti->n && e == cudaSuccess; ++i) {
         bp[ti->perm[i]] = b[i];
         mx = std::max<int64_t>(mx, b[i] < 0 ? -int64_t(b[i]) : int64_t(b[i]));
     }
-    if (e == cudaSuccess) e = cudaMalloc(&ti->d_bias_perm, size_t(ti->np) * 4);
-    if (e == cudaSuccess) e = cudaMemcpy(ti->d_bias_perm, bp.data(), size_t(ti->np) * 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMalloc(&ti->d_bias_perm, size_t(ti->npp) * 4);
+    if (e == cudaSuccess) e = cudaMemcpy(ti->d_bias_perm, bp.data(), size_t(ti->npp) * 4, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
         if (why) *why = std::string("bias: ") + cudaGetErrorString(e);
         return -2;
@@ -1632,6 +1648,7 @@ int tensor_run(TensorInstance* ti, const TensorRun& r, cudaStream_t st, std::str
         return -1;
     }
     if (fp4 && r.kind != TENSOR_KIND_INT8) return f4_run(ti, r, st, why);
+    if (ti->stream) return stream_run(ti, r, r.bias ? ti->d_bias_perm : nullptr, st, why);
     if (R == 8) return res_run(ti, r, st, why);
     const int groups = (r.nchains + kM - 1) / kM;
     // workspace: exchange buffers, permuted bias, error word
