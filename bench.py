@@ -257,7 +257,8 @@ def bench_ours(args, ws, rank, local):
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.int32, device="cuda")   # > L2 (126 MB)
     L = _lib.load()
     stream = torch.cuda.current_stream()
-    trial_base = rank << 20
+    from anechoic_b200 import replicas
+    trial_base = replicas.trial_base(rank)
 
     def timed(eng, knd, steps, warmup, clocks=False):
         """Device-timed launches (inputs resident, outputs on the device); returns per-launch ms and the kernel."""
@@ -301,26 +302,21 @@ def bench_ours(args, ws, rank, local):
             succ += s_; succ_batches += int(s_ > 0); flips_total += int(r.flips.sum())
         return succ, succ_batches, flips_total
 
-    def max_over_ranks(x):
-        if not dist:
-            return x
-        t = torch.tensor([x], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    max_over_ranks = replicas.reduce_max
 
     ms, kernel, clk = timed(engine, kind, args.steps, args.warmup, clocks=True)
     t_batch_ms = max_over_ranks(sum(ms) / len(ms))
-    succ, succ_batches, flips_total = scored(engine, kind, args.steps)
+    succ, succ_batches, flips_total = replicas.reduce_sum(scored(engine, kind, args.steps))
 
     # the plain (bit-column) engine on the same batches, for the batched-vs-plain comparison of the metric
     plain = None
     if kernel != "plain" and not args.no_plain:
         pms, _, _ = timed("plain", "auto", args.steps, args.warmup)
         p_ms = max_over_ranks(sum(pms) / len(pms))
-        p_succ, p_sb, _ = scored("plain", "auto", args.steps)
+        p_succ, p_sb, _ = replicas.reduce_sum(scored("plain", "auto", args.steps))
         plain = {"anneals_per_s": CHAINS * ws / (p_ms / 1000.0), "ms_per_step": p_ms,
-                 "tts99_us_primary": 1000.0 * tts99(p_sb / args.steps, p_ms),
-                 "tts99_us_secondary": 1000.0 * tts99_secondary(p_succ / (CHAINS * args.steps), CHAINS, p_ms)}
+                 "tts99_us_primary": 1000.0 * tts99(p_sb / (args.steps * ws), p_ms),
+                 "tts99_us_secondary": 1000.0 * tts99_secondary(p_succ / (CHAINS * args.steps * ws), CHAINS, p_ms)}
 
     # e2e: the same batch through the public C ABI with host buffers -- schedule tables uploaded from host memory
     # and results (spins, sum s*h, sum b*s, flips) read back to host memory inside every timed step
@@ -345,7 +341,7 @@ def bench_ours(args, ws, rank, local):
     S = SCHED["S"]
     anneals = CHAINS * ws
     value = anneals / (t_batch_ms / 1000.0)
-    B, nb = CHAINS, args.steps
+    B, nb = CHAINS, args.steps * ws          # success counts are summed over ranks: ws batches per timed step
     P_batch = succ_batches / nb
     p = succ / (B * nb)
     mean_flips = flips_total / (B * nb)
