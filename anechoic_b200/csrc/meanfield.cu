@@ -28,6 +28,18 @@ struct MfContext {
     int nbuf_steps = 0;
     int* err = nullptr;               // device error word
     CUtensorMap mapJ, mapXm[3], mapXp[3];
+    // CUDA graphs of the forward and adjoint launch sequences (one step count each), captured on internal buffers:
+    // the caller's inputs are copied in and the outputs copied out around each graph launch
+    cudaStream_t cap = nullptr;
+    cudaGraphExec_t fwd_exec = nullptr, bwd_exec = nullptr;
+    int fwd_S = 0, bwd_S = 0, io_steps = 0;
+    float* sched_i = nullptr;         // [4][S]
+    float* m0_i = nullptr;            // [64][npad]
+    float* mprev_i = nullptr;
+    float* mout_i = nullptr;
+    float* gm_i = nullptr;
+    float* ckpt_i = nullptr;          // [ceil(S/16)][2][64][npad]
+    float* gs_i = nullptr;            // [S][4][64]
 };
 
 namespace {
@@ -311,14 +323,9 @@ bool check(cudaError_t e, const char* what, std::string* why) {
 }
 
 int gemm(MfContext* c, const CUtensorMap (&mx)[3], cudaStream_t st, std::string* why) {
-    const size_t smem = gemm_smem();
-    cudaError_t e = cudaFuncSetAttribute(mf_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    if (e == cudaSuccess) {
-        mf_gemm_kernel<<<dim3(c->npad / kRows, c->npad / kKC), kGemmThreads, smem, st>>>(c->mapJ, mx[0], mx[1], mx[2],
-                                                                                        c->partial, c->npad, c->err);
-        e = cudaGetLastError();
-    }
-    return check(e, "mean-field GEMM launch", why) ? 0 : -2;
+    mf_gemm_kernel<<<dim3(c->npad / kRows, c->npad / kKC), kGemmThreads, gemm_smem(), st>>>(c->mapJ, mx[0], mx[1], mx[2],
+                                                                                           c->partial, c->npad, c->err);
+    return check(cudaGetLastError(), "mean-field GEMM launch", why) ? 0 : -2;
 }
 
 float* mslot(float* base, int k, int npad) { return base + size_t(k) * kRep * npad; }
@@ -408,6 +415,10 @@ int mf_create(const int8_t* J, const int32_t* bias, int n, MfContext** out, std:
                  make_map_2d(&c->mapXp[k], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, c->xp + k * plane, npad, kRep, 64, kRep);
         if (!ok && why) *why = "cuTensorMapEncodeTiled failed";
     }
+    if (ok)
+        ok = check(cudaFuncSetAttribute(mf_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(gemm_smem())),
+                   "GEMM attributes", why) &&
+             check(cudaStreamCreateWithFlags(&c->cap, cudaStreamNonBlocking), "capture stream", why);
     if (!ok) {
         mf_destroy(c);
         return -2;
@@ -416,14 +427,12 @@ int mf_create(const int8_t* J, const int32_t* bias, int n, MfContext** out, std:
     return 0;
 }
 
-int mf_forward(MfContext* c, int S, const float* beta, const float* q, const float* u, const float* w, const float* m0,
-               const float* mprev, float* ckpt, float* m_out, cudaStream_t st, std::string* why) {
-    if (!c || S < 1 || !beta || !q || !u || !w || !m0 || !mprev || !ckpt || !m_out) {
-        if (why) *why = "invalid mean-field forward arguments";
-        return -1;
-    }
-    int rc = ensure_steps(c, S, why);
-    if (rc) return rc;
+namespace {
+
+// The forward launch sequence on explicit buffers (recorded into the forward graph).
+int forward_body(MfContext* c, int S, const float* beta, const float* q, const float* u, const float* w,
+                 const float* m0, const float* mprev, float* ckpt, float* m_out, cudaStream_t st, std::string* why) {
+    int rc = 0;
     const int npad = c->npad;
     const size_t plane = size_t(kRep) * npad;
     float* ring = c->mring;
@@ -453,14 +462,10 @@ int mf_forward(MfContext* c, int S, const float* beta, const float* q, const flo
     return 0;
 }
 
-int mf_backward(MfContext* c, int S, const float* beta, const float* q, const float* u, const float* w,
-                const float* ckpt, const float* g_m, float* gsched, cudaStream_t st, std::string* why) {
-    if (!c || S < 1 || !beta || !q || !u || !w || !ckpt || !g_m || !gsched) {
-        if (why) *why = "invalid mean-field backward arguments";
-        return -1;
-    }
-    int rc = ensure_steps(c, S, why);
-    if (rc) return rc;
+// The adjoint launch sequence on explicit buffers (recorded into the adjoint graph).
+int backward_body(MfContext* c, int S, const float* beta, const float* q, const float* u, const float* w,
+                  const float* ckpt, const float* g_m, float* gsched, cudaStream_t st, std::string* why) {
+    int rc = 0;
     const int npad = c->npad;
     const size_t plane = size_t(kRep) * npad;
     const int nseg = (S + kMfCheckpoint - 1) / kMfCheckpoint;
@@ -518,6 +523,119 @@ int mf_backward(MfContext* c, int S, const float* beta, const float* q, const fl
     return 0;
 }
 
+// Internal buffers for S steps (allocated outside any capture; graphs recorded on older buffers are dropped).
+int ensure_io(MfContext* c, int S, std::string* why) {
+    int rc = ensure_steps(c, S, why);
+    if (rc) return rc;
+    if (S <= c->io_steps) return 0;
+    for (float** p : {&c->sched_i, &c->m0_i, &c->mprev_i, &c->mout_i, &c->gm_i, &c->ckpt_i, &c->gs_i}) {
+        if (*p) cudaFree(*p);
+        *p = nullptr;
+    }
+    for (cudaGraphExec_t* g : {&c->fwd_exec, &c->bwd_exec}) {
+        if (*g) cudaGraphExecDestroy(*g);
+        *g = nullptr;
+    }
+    c->fwd_S = c->bwd_S = c->io_steps = 0;
+    const size_t plane = size_t(kRep) * c->npad;
+    const size_t nseg = (S + kMfCheckpoint - 1) / kMfCheckpoint;
+    const bool ok = check(cudaMalloc(&c->sched_i, 4 * size_t(S) * 4), "cudaMalloc", why) &&
+                    check(cudaMalloc(&c->m0_i, plane * 4), "cudaMalloc", why) &&
+                    check(cudaMalloc(&c->mprev_i, plane * 4), "cudaMalloc", why) &&
+                    check(cudaMalloc(&c->mout_i, plane * 4), "cudaMalloc", why) &&
+                    check(cudaMalloc(&c->gm_i, plane * 4), "cudaMalloc", why) &&
+                    check(cudaMalloc(&c->ckpt_i, nseg * 2 * plane * 4), "cudaMalloc", why) &&
+                    check(cudaMalloc(&c->gs_i, size_t(S) * 4 * kRep * 4), "cudaMalloc", why);
+    if (!ok) return -2;
+    c->io_steps = S;
+    return 0;
+}
+
+// Copy the four schedule vectors into sched_i rows [4][S].
+bool copy_sched(MfContext* c, int S, const float* beta, const float* q, const float* u, const float* w, cudaStream_t st,
+                std::string* why) {
+    const float* v[4] = {beta, q, u, w};
+    for (int k = 0; k < 4; ++k)
+        if (!check(cudaMemcpyAsync(c->sched_i + size_t(k) * S, v[k], size_t(S) * 4, cudaMemcpyDeviceToDevice, st),
+                   "copy schedule", why))
+            return false;
+    return true;
+}
+
+// Record body(cap stream) into *exec once per step count.
+template <class Body>
+int ensure_graph(MfContext* c, cudaGraphExec_t* exec, int* exec_S, int S, Body body, std::string* why) {
+    if (*exec && *exec_S == S) return 0;
+    if (*exec) cudaGraphExecDestroy(*exec);
+    *exec = nullptr;
+    cudaGraph_t g = nullptr;
+    if (!check(cudaStreamBeginCapture(c->cap, cudaStreamCaptureModeThreadLocal), "begin capture", why)) return -2;
+    const int rc = body(c->cap);
+    const cudaError_t e = cudaStreamEndCapture(c->cap, &g);
+    if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (!check(e, "end capture", why)) return -2;
+    const cudaError_t ei = cudaGraphInstantiate(exec, g, 0);
+    cudaGraphDestroy(g);
+    if (!check(ei, "instantiate graph", why)) return -2;
+    *exec_S = S;
+    return 0;
+}
+
+}  // namespace
+
+int mf_forward(MfContext* c, int S, const float* beta, const float* q, const float* u, const float* w, const float* m0,
+               const float* mprev, float* ckpt, float* m_out, cudaStream_t st, std::string* why) {
+    if (!c || S < 1 || !beta || !q || !u || !w || !m0 || !mprev || !ckpt || !m_out) {
+        if (why) *why = "invalid mean-field forward arguments";
+        return -1;
+    }
+    int rc = ensure_io(c, S, why);
+    if (rc) return rc;
+    const size_t plane = size_t(kRep) * c->npad, nseg = (S + kMfCheckpoint - 1) / kMfCheckpoint;
+    rc = ensure_graph(c, &c->fwd_exec, &c->fwd_S, S, [&](cudaStream_t cs) {
+        const float* sb = c->sched_i;
+        return forward_body(c, S, sb, sb + S, sb + 2 * size_t(S), sb + 3 * size_t(S), c->m0_i, c->mprev_i, c->ckpt_i,
+                            c->mout_i, cs, why);
+    }, why);
+    if (rc) return rc;
+    if (!copy_sched(c, S, beta, q, u, w, st, why) ||
+        !check(cudaMemcpyAsync(c->m0_i, m0, plane * 4, cudaMemcpyDeviceToDevice, st), "copy m0", why) ||
+        !check(cudaMemcpyAsync(c->mprev_i, mprev, plane * 4, cudaMemcpyDeviceToDevice, st), "copy mprev", why) ||
+        !check(cudaGraphLaunch(c->fwd_exec, st), "forward graph launch", why) ||
+        !check(cudaMemcpyAsync(ckpt, c->ckpt_i, nseg * 2 * plane * 4, cudaMemcpyDeviceToDevice, st), "copy ckpt", why) ||
+        !check(cudaMemcpyAsync(m_out, c->mout_i, plane * 4, cudaMemcpyDeviceToDevice, st), "copy m_S", why))
+        return -2;
+    return 0;
+}
+
+int mf_backward(MfContext* c, int S, const float* beta, const float* q, const float* u, const float* w,
+                const float* ckpt, const float* g_m, float* gsched, cudaStream_t st, std::string* why) {
+    if (!c || S < 1 || !beta || !q || !u || !w || !ckpt || !g_m || !gsched) {
+        if (why) *why = "invalid mean-field backward arguments";
+        return -1;
+    }
+    int rc = ensure_io(c, S, why);
+    if (rc) return rc;
+    const size_t plane = size_t(kRep) * c->npad, nseg = (S + kMfCheckpoint - 1) / kMfCheckpoint;
+    rc = ensure_graph(c, &c->bwd_exec, &c->bwd_S, S, [&](cudaStream_t cs) {
+        const float* sb = c->sched_i;
+        return backward_body(c, S, sb, sb + S, sb + 2 * size_t(S), sb + 3 * size_t(S), c->ckpt_i, c->gm_i, c->gs_i, cs,
+                             why);
+    }, why);
+    if (rc) return rc;
+    if (!copy_sched(c, S, beta, q, u, w, st, why) ||
+        !check(cudaMemcpyAsync(c->ckpt_i, ckpt, nseg * 2 * plane * 4, cudaMemcpyDeviceToDevice, st), "copy ckpt", why) ||
+        !check(cudaMemcpyAsync(c->gm_i, g_m, plane * 4, cudaMemcpyDeviceToDevice, st), "copy dL/dm", why) ||
+        !check(cudaGraphLaunch(c->bwd_exec, st), "adjoint graph launch", why) ||
+        !check(cudaMemcpyAsync(gsched, c->gs_i, size_t(S) * 4 * kRep * 4, cudaMemcpyDeviceToDevice, st), "copy grads",
+               why))
+        return -2;
+    return 0;
+}
+
 int mf_check_error(MfContext* c, cudaStream_t st, std::string* why) {
     int h = 0;
     cudaError_t e = cudaMemcpyAsync(&h, c->err, 4, cudaMemcpyDeviceToHost, st);
@@ -533,6 +651,13 @@ int mf_check_error(MfContext* c, cudaStream_t st, std::string* why) {
 
 void mf_destroy(MfContext* c) {
     if (!c) return;
+    if (c->fwd_exec) cudaGraphExecDestroy(c->fwd_exec);
+    if (c->bwd_exec) cudaGraphExecDestroy(c->bwd_exec);
+    if (c->cap) cudaStreamDestroy(c->cap);
+    for (void* p : {static_cast<void*>(c->sched_i), static_cast<void*>(c->m0_i), static_cast<void*>(c->mprev_i),
+                    static_cast<void*>(c->mout_i), static_cast<void*>(c->gm_i), static_cast<void*>(c->ckpt_i),
+                    static_cast<void*>(c->gs_i)})
+        if (p) cudaFree(p);
     for (void* p : {static_cast<void*>(c->J), static_cast<void*>(c->bias), static_cast<void*>(c->partial),
                     static_cast<void*>(c->mring), static_cast<void*>(c->xm), static_cast<void*>(c->xp),
                     static_cast<void*>(c->seg_m), static_cast<void*>(c->seg_P), static_cast<void*>(c->pbar),
