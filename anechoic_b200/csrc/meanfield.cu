@@ -23,8 +23,9 @@ struct MfContext {
     float* seg_m = nullptr;           // [kMfCheckpoint + 2][64][npad]: m_{t0-1} .. m_{t0+16} of a segment
     float* seg_P = nullptr;           // [kMfCheckpoint][64][npad]
     float* pbar = nullptr;            // [3][64][npad] ring of pbar_t
-    float* svec = nullptr;            // [3][64] ring of s_t
-    float* nbuf = nullptr;            // [S + 1][64] soft counts n_t
+    float* svec = nullptr;            // [3][nch][64] ring of s_t, per 256-column chunk
+    float* nbuf = nullptr;            // [S + 1][nch][64] soft counts n_t, per 256-column chunk
+    float* gparts = nullptr;          // [S][4][nch][64] per-chunk schedule-gradient sums
     int nbuf_steps = 0;
     int* err = nullptr;               // device error word
     CUtensorMap mapJ, mapXm[3], mapXp[3];
@@ -200,20 +201,27 @@ __device__ __forceinline__ void block_sum(float (&v)[NV], float* red) {
     }
 }
 
-// Soft counts n[r] = sum_{i < n} (1 - m[r,i]^2) and the BF16 terms of m; one block per replica.
+// Sum of replica r's per-chunk partials parts[ch][r], in chunk order (deterministic).
+__device__ __forceinline__ float sum_parts(const float* __restrict__ parts, int nch, int r) {
+    float v = 0.f;
+    for (int ch = 0; ch < nch; ++ch) v += parts[ch * kRep + r];
+    return v;
+}
+
+// Elementwise kernels run on a (replica, 256-column chunk) grid, one element per thread; per-replica sums are
+// written per chunk (parts[chunk][replica]) and summed in chunk order by their readers.
+
+// Soft count partials n[ch][r] = sum_{i in chunk, i < n} (1 - m[r,i]^2) and the BF16 terms of m.
 __global__ void __launch_bounds__(kElemThreads) mf_prep_kernel(const float* __restrict__ m, int n, int npad,
                                                                float* __restrict__ nout, __nv_bfloat16* __restrict__ x) {
     __shared__ float red[32];
-    const int r = blockIdx.x;
-    float acc[1] = {0.f};
-    for (int i = threadIdx.x; i < npad; i += blockDim.x) {
-        const size_t idx = size_t(r) * npad + i;
-        const float v = m[idx];
-        split_bf16(v, x + idx, size_t(kRep) * npad);
-        if (i < n) acc[0] += 1.f - v * v;
-    }
+    const int r = blockIdx.x, i = blockIdx.y * kElemThreads + threadIdx.x;
+    const size_t idx = size_t(r) * npad + i;
+    const float v = m[idx];
+    split_bf16(v, x + idx, size_t(kRep) * npad);
+    float acc[1] = {i < n ? 1.f - v * v : 0.f};
     block_sum(acc, red);
-    if (threadIdx.x == 0) nout[r] = acc[0];
+    if (threadIdx.x == 0) nout[blockIdx.y * kRep + r] = acc[0];
 }
 
 struct FwdArgs {
@@ -223,32 +231,29 @@ struct FwdArgs {
     const float *beta, *q, *u, *w;
     const float* m_cur;
     const float* m_prev;
-    const float* n_cur;      // [64]
+    const float* n_cur;      // [nch][64] partials of n_t
     float* m_next;
     __nv_bfloat16* x;        // BF16 terms of m_next [3][64][npad]
-    float* n_next;           // [64]
+    float* n_next;           // [nch][64] partials of n_{t+1}
     float* P_out;            // [64][npad] or null
 };
 
 __global__ void __launch_bounds__(kElemThreads) mf_fwd_kernel(const FwdArgs a) {
     __shared__ float red[32];
-    const int r = blockIdx.x, npad = a.npad;
+    const int r = blockIdx.x, npad = a.npad, nch = gridDim.y, i = blockIdx.y * kElemThreads + threadIdx.x;
     const float beta = a.beta[a.t], q = a.q[a.t];
-    const float gamma = a.u[a.t] * a.n_cur[r] + a.w[a.t];
-    float acc[1] = {0.f};
-    for (int i = threadIdx.x; i < npad; i += blockDim.x) {
-        const size_t idx = size_t(r) * npad + i;
-        float H = 0.f;
-        for (int ks = 0; ks < a.ksplit; ++ks) H += a.partial[(size_t(ks) * kRep + r) * npad + i];
-        const float P = H + a.bias[i] + q * a.m_cur[idx] - gamma * a.m_prev[idx];
-        const float mn = i < a.n ? tanhf(beta * P) : 0.f;
-        a.m_next[idx] = mn;
-        split_bf16(mn, a.x + idx, size_t(kRep) * npad);
-        if (a.P_out) a.P_out[idx] = P;
-        if (i < a.n) acc[0] += 1.f - mn * mn;
-    }
+    const float gamma = a.u[a.t] * sum_parts(a.n_cur, nch, r) + a.w[a.t];
+    const size_t idx = size_t(r) * npad + i;
+    float H = 0.f;
+    for (int ks = 0; ks < a.ksplit; ++ks) H += a.partial[(size_t(ks) * kRep + r) * npad + i];
+    const float P = H + a.bias[i] + q * a.m_cur[idx] - gamma * a.m_prev[idx];
+    const float mn = i < a.n ? tanhf(beta * P) : 0.f;
+    a.m_next[idx] = mn;
+    split_bf16(mn, a.x + idx, size_t(kRep) * npad);
+    if (a.P_out) a.P_out[idx] = P;
+    float acc[1] = {i < a.n ? 1.f - mn * mn : 0.f};
     block_sum(acc, red);
-    if (threadIdx.x == 0) a.n_next[r] = acc[0];
+    if (threadIdx.x == 0) a.n_next[blockIdx.y * kRep + r] = acc[0];
 }
 
 struct BwdArgs {
@@ -257,18 +262,18 @@ struct BwdArgs {
     const float* g_final;      // dL/dm_S (used when t = S - 1)
     const float* pbar_next;    // pbar_{t+1} or null
     const float* pbar_next2;   // pbar_{t+2} or null
-    const float* s_next;       // s_{t+1} [64] or null
-    const float* n_next2;      // n_{t+2} [64] or null
+    const float* s_next;       // partials of s_{t+1} [nch][64], or null
+    const float* n_next2;      // partials of n_{t+2} [nch][64], or null
     const float *beta, *q, *u, *w;
     const float* m_next;       // m_{t+1}
     const float* m_cur;        // m_t
     const float* m_prev;       // m_{t-1}
     const float* P;            // P_t
-    const float* n_cur;        // n_t [64]
+    const float* n_cur;        // partials of n_t [nch][64]
     float* pbar;               // out: pbar_t
     __nv_bfloat16* x;          // out: BF16 terms of pbar_t [3][64][npad]
-    float* s_out;              // out: s_t [64]
-    float* gsched;             // out: [S][4][64]
+    float* s_out;              // out: partials of s_t [nch][64]
+    float* gparts;             // out: [S][4][nch][64] partials
 };
 
 // One adjoint step t:
@@ -278,42 +283,48 @@ struct BwdArgs {
 //   dL/dbeta_t += sum abar_t P_t, dL/dq_t += sum pbar_t m_t, dL/du_t += -s_t n_t, dL/dw_t += -s_t
 __global__ void __launch_bounds__(kElemThreads) mf_bwd_kernel(const BwdArgs a) {
     __shared__ float red[3 * 32];
-    const int r = blockIdx.x, npad = a.npad, t = a.t;
+    const int r = blockIdx.x, npad = a.npad, t = a.t, nch = gridDim.y, ch = blockIdx.y;
+    const int i = ch * kElemThreads + threadIdx.x;
     const float beta = a.beta[t];
     const bool last = t == a.S - 1;
     const float q1 = last ? 0.f : a.q[t + 1];
-    const float us = last ? 0.f : 2.f * a.u[t + 1] * a.s_next[r];
-    const float g2 = a.pbar_next2 ? a.u[t + 2] * a.n_next2[r] + a.w[t + 2] : 0.f;
-    float acc[3] = {0.f, 0.f, 0.f};   // sum abar * P, sum pbar * m_t, sum pbar * m_{t-1}
-    for (int i = threadIdx.x; i < npad; i += blockDim.x) {
-        const size_t idx = size_t(r) * npad + i;
-        float G;
-        if (last) {
-            G = a.g_final[idx];
-        } else {
-            float H = 0.f;
-            for (int ks = 0; ks < a.ksplit; ++ks) H += a.partial[(size_t(ks) * kRep + r) * npad + i];
-            G = H + q1 * a.pbar_next[idx] + us * a.m_next[idx];
-            if (a.pbar_next2) G -= g2 * a.pbar_next2[idx];
-        }
-        const float mn = a.m_next[idx];
-        const float abar = i < a.n ? G * (1.f - mn * mn) : 0.f;
-        const float pb = beta * abar;
-        a.pbar[idx] = pb;
-        split_bf16(pb, a.x + idx, size_t(kRep) * npad);
-        acc[0] += abar * a.P[idx];
-        acc[1] += pb * a.m_cur[idx];
-        acc[2] += pb * a.m_prev[idx];
+    const float us = last ? 0.f : 2.f * a.u[t + 1] * sum_parts(a.s_next, nch, r);
+    const float g2 = a.pbar_next2 ? a.u[t + 2] * sum_parts(a.n_next2, nch, r) + a.w[t + 2] : 0.f;
+    const size_t idx = size_t(r) * npad + i;
+    float G;
+    if (last) {
+        G = a.g_final[idx];
+    } else {
+        float H = 0.f;
+        for (int ks = 0; ks < a.ksplit; ++ks) H += a.partial[(size_t(ks) * kRep + r) * npad + i];
+        G = H + q1 * a.pbar_next[idx] + us * a.m_next[idx];
+        if (a.pbar_next2) G -= g2 * a.pbar_next2[idx];
     }
+    const float mn = a.m_next[idx];
+    const float abar = i < a.n ? G * (1.f - mn * mn) : 0.f;
+    const float pb = beta * abar;
+    a.pbar[idx] = pb;
+    split_bf16(pb, a.x + idx, size_t(kRep) * npad);
+    float acc[3] = {abar * a.P[idx], pb * a.m_cur[idx], pb * a.m_prev[idx]};   // abar P, pbar m_t, pbar m_{t-1}
     block_sum(acc, red);
     if (threadIdx.x == 0) {
-        a.s_out[r] = acc[2];
-        float* g = a.gsched + size_t(t) * 4 * kRep;
-        g[0 * kRep + r] = acc[0];
-        g[1 * kRep + r] = acc[1];
-        g[2 * kRep + r] = -acc[2] * a.n_cur[r];
-        g[3 * kRep + r] = -acc[2];
+        a.s_out[ch * kRep + r] = acc[2];
+        float* g = a.gparts + size_t(t) * 4 * nch * kRep;
+        g[(0 * nch + ch) * kRep + r] = acc[0];
+        g[(1 * nch + ch) * kRep + r] = acc[1];
+        g[(2 * nch + ch) * kRep + r] = -acc[2] * sum_parts(a.n_cur, nch, r);
+        g[(3 * nch + ch) * kRep + r] = -acc[2];
     }
+}
+
+// gsched[t][k][r] = sum over chunks of gparts[t][k][ch][r] (chunk order); one thread per (t, k, r).
+__global__ void mf_gsum_kernel(const float* __restrict__ gparts, int S, int nch, float* __restrict__ gsched) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= S * 4 * kRep) return;
+    const int r = e % kRep, tk = e / kRep;
+    float v = 0.f;
+    for (int ch = 0; ch < nch; ++ch) v += gparts[(size_t(tk) * nch + ch) * kRep + r];
+    gsched[e] = v;
 }
 
 bool check(cudaError_t e, const char* what, std::string* why) {
@@ -329,6 +340,9 @@ int gemm(MfContext* c, const CUtensorMap (&mx)[3], cudaStream_t st, std::string*
 }
 
 float* mslot(float* base, int k, int npad) { return base + size_t(k) * kRep * npad; }
+
+// 256-column chunks of the elementwise grid.
+int nch(const MfContext* c) { return c->npad / kElemThreads; }
 
 // Forward steps t = t0 .. t1 - 1: m_t = cur(t), m_{t-1} = prev(t); writes m_{t+1} to next(t) and P_t to pout(t)
 // when that is not null. The BF16 terms of m_t must already be in c->xm.
@@ -352,12 +366,12 @@ int run_steps(MfContext* c, int t0, int t1, const float* beta, const float* q, c
         a.w = w;
         a.m_cur = cur(t);
         a.m_prev = prev(t);
-        a.n_cur = c->nbuf + size_t(t) * kRep;
+        a.n_cur = c->nbuf + size_t(t) * nch(c) * kRep;
         a.m_next = next(t);
         a.x = c->xm;
-        a.n_next = c->nbuf + size_t(t + 1) * kRep;
+        a.n_next = c->nbuf + size_t(t + 1) * nch(c) * kRep;
         a.P_out = pout(t);
-        mf_fwd_kernel<<<kRep, kElemThreads, 0, st>>>(a);
+        mf_fwd_kernel<<<dim3(kRep, nch(c)), kElemThreads, 0, st>>>(a);
         if (!check(cudaGetLastError(), "mean-field forward step", why)) return -2;
     }
     return 0;
@@ -365,10 +379,14 @@ int run_steps(MfContext* c, int t0, int t1, const float* beta, const float* q, c
 
 int ensure_steps(MfContext* c, int S, std::string* why) {
     if (S <= c->nbuf_steps) return 0;
-    if (c->nbuf) cudaFree(c->nbuf);
-    c->nbuf = nullptr;
+    for (float** p : {&c->nbuf, &c->gparts}) {
+        if (*p) cudaFree(*p);
+        *p = nullptr;
+    }
     c->nbuf_steps = 0;
-    if (!check(cudaMalloc(&c->nbuf, size_t(S + 1) * kRep * sizeof(float)), "cudaMalloc", why)) return -2;
+    if (!check(cudaMalloc(&c->nbuf, size_t(S + 1) * nch(c) * kRep * sizeof(float)), "cudaMalloc", why) ||
+        !check(cudaMalloc(&c->gparts, size_t(S) * 4 * nch(c) * kRep * sizeof(float)), "cudaMalloc", why))
+        return -2;
     c->nbuf_steps = S;
     return 0;
 }
@@ -405,7 +423,7 @@ int mf_create(const int8_t* J, const int32_t* bias, int n, MfContext** out, std:
               check(cudaMalloc(&c->seg_m, (kMfCheckpoint + 2) * plane * sizeof(float)), "cudaMalloc", why) &&
               check(cudaMalloc(&c->seg_P, kMfCheckpoint * plane * sizeof(float)), "cudaMalloc", why) &&
               check(cudaMalloc(&c->pbar, 3 * plane * sizeof(float)), "cudaMalloc", why) &&
-              check(cudaMalloc(&c->svec, 3 * kRep * sizeof(float)), "cudaMalloc", why) &&
+              check(cudaMalloc(&c->svec, 3 * size_t(npad / kElemThreads) * kRep * sizeof(float)), "cudaMalloc", why) &&
               check(cudaMalloc(&c->err, sizeof(int)), "cudaMalloc", why) &&
               check(cudaMemset(c->err, 0, sizeof(int)), "cudaMemset", why);
     if (ok) {
@@ -439,7 +457,7 @@ int forward_body(MfContext* c, int S, const float* beta, const float* q, const f
     if (!check(cudaMemcpyAsync(mslot(ring, 0, npad), mprev, plane * 4, cudaMemcpyDeviceToDevice, st), "copy", why) ||
         !check(cudaMemcpyAsync(mslot(ring, 1, npad), m0, plane * 4, cudaMemcpyDeviceToDevice, st), "copy", why))
         return -2;
-    mf_prep_kernel<<<kRep, kElemThreads, 0, st>>>(mslot(ring, 1, npad), c->n, npad, c->nbuf, c->xm);
+    mf_prep_kernel<<<dim3(kRep, nch(c)), kElemThreads, 0, st>>>(mslot(ring, 1, npad), c->n, npad, c->nbuf, c->xm);
     if (!check(cudaGetLastError(), "mean-field prep", why)) return -2;
     // m_t lives in ring slot (t + 1) % 3, m_{t-1} in slot t % 3
     for (int t0 = 0; t0 < S; t0 += kMfCheckpoint) {
@@ -476,8 +494,8 @@ int backward_body(MfContext* c, int S, const float* beta, const float* q, const 
         if (!check(cudaMemcpyAsync(mslot(c->seg_m, 0, npad), ck, 2 * plane * 4, cudaMemcpyDeviceToDevice, st), "copy",
                    why))
             return -2;
-        mf_prep_kernel<<<kRep, kElemThreads, 0, st>>>(mslot(c->seg_m, 1, npad), c->n, npad,
-                                                     c->nbuf + size_t(t0) * kRep, c->xm);
+        mf_prep_kernel<<<dim3(kRep, nch(c)), kElemThreads, 0, st>>>(mslot(c->seg_m, 1, npad), c->n, npad,
+                                                                   c->nbuf + size_t(t0) * nch(c) * kRep, c->xm);
         if (!check(cudaGetLastError(), "mean-field prep", why)) return -2;
         rc = run_steps(
             c, t0, t1, beta, q, u, w, [&](int t) { return mslot(c->seg_m, t - t0 + 1, npad); },
@@ -501,8 +519,8 @@ int backward_body(MfContext* c, int S, const float* beta, const float* q, const 
             a.g_final = g_m;
             a.pbar_next = last ? nullptr : mslot(c->pbar, (t + 1) % 3, npad);
             a.pbar_next2 = t + 2 < S ? mslot(c->pbar, (t + 2) % 3, npad) : nullptr;
-            a.s_next = last ? nullptr : c->svec + ((t + 1) % 3) * kRep;
-            a.n_next2 = t + 2 < S ? c->nbuf + size_t(t + 2) * kRep : nullptr;
+            a.s_next = last ? nullptr : c->svec + size_t((t + 1) % 3) * nch(c) * kRep;
+            a.n_next2 = t + 2 < S ? c->nbuf + size_t(t + 2) * nch(c) * kRep : nullptr;
             a.beta = beta;
             a.q = q;
             a.u = u;
@@ -511,15 +529,18 @@ int backward_body(MfContext* c, int S, const float* beta, const float* q, const 
             a.m_cur = mslot(c->seg_m, t - t0 + 1, npad);
             a.m_prev = mslot(c->seg_m, t - t0, npad);
             a.P = mslot(c->seg_P, t - t0, npad);
-            a.n_cur = c->nbuf + size_t(t) * kRep;
+            a.n_cur = c->nbuf + size_t(t) * nch(c) * kRep;
             a.pbar = mslot(c->pbar, t % 3, npad);
             a.x = c->xp;
-            a.s_out = c->svec + (t % 3) * kRep;
-            a.gsched = gsched;
-            mf_bwd_kernel<<<kRep, kElemThreads, 0, st>>>(a);
+            a.s_out = c->svec + size_t(t % 3) * nch(c) * kRep;
+            a.gparts = c->gparts;
+            mf_bwd_kernel<<<dim3(kRep, nch(c)), kElemThreads, 0, st>>>(a);
             if (!check(cudaGetLastError(), "mean-field adjoint step", why)) return -2;
         }
     }
+    const int ne = S * 4 * kRep;
+    mf_gsum_kernel<<<(ne + 255) / 256, 256, 0, st>>>(c->gparts, S, nch(c), gsched);
+    if (!check(cudaGetLastError(), "mean-field gradient sum", why)) return -2;
     return 0;
 }
 
@@ -661,7 +682,8 @@ void mf_destroy(MfContext* c) {
     for (void* p : {static_cast<void*>(c->J), static_cast<void*>(c->bias), static_cast<void*>(c->partial),
                     static_cast<void*>(c->mring), static_cast<void*>(c->xm), static_cast<void*>(c->xp),
                     static_cast<void*>(c->seg_m), static_cast<void*>(c->seg_P), static_cast<void*>(c->pbar),
-                    static_cast<void*>(c->svec), static_cast<void*>(c->nbuf), static_cast<void*>(c->err)})
+                    static_cast<void*>(c->svec), static_cast<void*>(c->nbuf), static_cast<void*>(c->gparts),
+                    static_cast<void*>(c->err)})
         if (p) cudaFree(p);
     delete c;
 }
