@@ -445,6 +445,12 @@ int anc_mf_check(anc_meanfield* mf, void* stream) {
     return ANC_OK;
 }
 
+int anc_mf_set_wait_ns(anc_meanfield* mf, uint64_t ns) {
+    if (!mf || !mf->ctx) return fail(ANC_EINVAL, "anc_mf_set_wait_ns: null handle");
+    anc::mf_set_wait_ns(mf->ctx, ns);
+    return ANC_OK;
+}
+
 void anc_mf_destroy(anc_meanfield* mf) {
     if (!mf) return;
     anc::mf_destroy(mf->ctx);

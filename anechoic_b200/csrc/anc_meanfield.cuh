@@ -39,6 +39,9 @@ int mf_forward(MfContext* c, int S, const float* beta, const float* q, const flo
 // g_m: dL/dm_S [64][npad]; gsched: [S][4][64] per-replica partial sums (beta, q, u, w).
 int mf_backward(MfContext* c, int S, const float* beta, const float* q, const float* u, const float* w,
                 const float* ckpt, const float* g_m, float* gsched, cudaStream_t st, std::string* why);
+// Limit of each device wait (default 2 s); a wait that reaches it makes the kernel record an error, let its own
+// copies and MMAs finish, skip the rest of its work and return.
+int mf_set_wait_ns(MfContext* c, uint64_t ns);
 // -3 if a bounded device wait expired during the last call on this context, 0 otherwise (synchronises st).
 int mf_check_error(MfContext* c, cudaStream_t st, std::string* why);
 void mf_destroy(MfContext* c);

@@ -40,16 +40,25 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
 
 // Bounded wait on phase `parity`; false (and the error word set) after kWaitNs. The timer is read only every 256
 // polls: a %globaltimer read costs hundreds of cycles and would otherwise delay the wake-up.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int* err, int code) {
+// Bounded wait with an explicit limit; limit_ns = 0 gives up at the first unsatisfied poll. err may be null (no record).
+__device__ __forceinline__ bool mbar_wait_for(uint32_t bar, uint32_t parity, int* err, int code, uint64_t limit_ns) {
     if (mbar_try_wait(bar, parity)) return true;
+    if (limit_ns == 0) {
+        if (err) atomicCAS(err, 0, code);
+        return false;
+    }
     const uint64_t t0 = globaltimer();
     for (uint32_t k = 1;; ++k) {
         if (mbar_try_wait(bar, parity)) return true;
-        if ((k & 255u) == 0 && globaltimer() - t0 > kWaitNs) {
-            atomicCAS(err, 0, code);
+        if ((k & 255u) == 0 && globaltimer() - t0 > limit_ns) {
+            if (err) atomicCAS(err, 0, code);
             return false;
         }
     }
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int* err, int code) {
+    return mbar_wait_for(bar, parity, err, code, kWaitNs);
 }
 
 __device__ __forceinline__ bool err_set(const int* err) { return *reinterpret_cast<const volatile int*>(err) != 0; }

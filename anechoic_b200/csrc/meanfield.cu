@@ -28,6 +28,7 @@ struct MfContext {
     float* gparts = nullptr;          // [S][4][nch][64] per-chunk schedule-gradient sums
     int nbuf_steps = 0;
     int* err = nullptr;               // device error word
+    uint64_t wait_ns = ptx::kWaitNs;  // limit of each device wait before the kernel gives up (recorded in the graphs)
     CUtensorMap mapJ, mapXm[3], mapXp[3];
     // CUDA graphs of the forward and adjoint launch sequences (one step count each), captured on internal buffers:
     // the caller's inputs are copied in and the outputs copied out around each graph launch
@@ -63,7 +64,7 @@ size_t gemm_smem() { return 1024 + 4 * size_t(kATile) + 12 * size_t(kBTile) + 64
 __global__ void __launch_bounds__(kGemmThreads, 1)
     mf_gemm_kernel(const __grid_constant__ CUtensorMap mapJ, const __grid_constant__ CUtensorMap mapXh,
                    const __grid_constant__ CUtensorMap mapXm, const __grid_constant__ CUtensorMap mapXl,
-                   float* __restrict__ partial, int npad, int* err) {
+                   float* __restrict__ partial, int npad, int* err, uint64_t wait_ns) {
     // kind::f16 instruction descriptor: f32 accumulator, BF16 A and B, both K-major, N = 64, M = 128
     constexpr uint32_t IDESC =
         (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(kRep >> 3) << 17) | (uint32_t(kRows >> 4) << 24);
@@ -101,7 +102,10 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
             tma_load_2d(smem_u32(sbm + a * kBTile), &mapXm, k0 + 64 * a, 0, bar_full);
             tma_load_2d(smem_u32(sbl + a * kBTile), &mapXl, k0 + 64 * a, 0, bar_full);
         }
-        const bool ok = mbar_wait(bar_full, 0u, err, kErrFull);
+        // a wait that gives up (after wait_ns) records the error, then waits once more, bounded by kWaitNs, for the
+        // copies it issued, so that none is in flight when the CTA skips its MMAs and exits
+        const bool ok = mbar_wait_for(bar_full, 0u, err, kErrFull, wait_ns);
+        if (!ok) mbar_wait_for(bar_full, 0u, nullptr, 0, kWaitNs);
         tc_fence_after();
         if (ok) {
             // The tensor core's f32 accumulation truncates toward zero each time an MMA adds into an accumulator, a
@@ -128,7 +132,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         mma_commit(bar_done);
     }
     __syncwarp();
-    mbar_wait(bar_done, 0u, err, kErrDone);
+    if (!mbar_wait_for(bar_done, 0u, err, kErrDone, wait_ns)) mbar_wait_for(bar_done, 0u, nullptr, 0, kWaitNs);
     tc_fence_after();
     // warp w reads TMEM lanes 32w .. 32w + 31 = rows y0 + 32w + lane; columns = replicas
     const int y = y0 + warp * 32 + lane;
@@ -335,7 +339,8 @@ bool check(cudaError_t e, const char* what, std::string* why) {
 
 int gemm(MfContext* c, const CUtensorMap (&mx)[3], cudaStream_t st, std::string* why) {
     mf_gemm_kernel<<<dim3(c->npad / kRows, c->npad / kKC), kGemmThreads, gemm_smem(), st>>>(c->mapJ, mx[0], mx[1], mx[2],
-                                                                                           c->partial, c->npad, c->err);
+                                                                                           c->partial, c->npad, c->err,
+                                                                                           c->wait_ns);
     return check(cudaGetLastError(), "mean-field GEMM launch", why) ? 0 : -2;
 }
 
@@ -654,6 +659,18 @@ int mf_backward(MfContext* c, int S, const float* beta, const float* q, const fl
         !check(cudaMemcpyAsync(gsched, c->gs_i, size_t(S) * 4 * kRep * 4, cudaMemcpyDeviceToDevice, st), "copy grads",
                why))
         return -2;
+    return 0;
+}
+
+int mf_set_wait_ns(MfContext* c, uint64_t ns) {
+    if (!c) return -1;
+    if (ns == c->wait_ns) return 0;
+    c->wait_ns = ns;
+    for (cudaGraphExec_t* g : {&c->fwd_exec, &c->bwd_exec}) {   // the limit is a kernel argument: record again
+        if (*g) cudaGraphExecDestroy(*g);
+        *g = nullptr;
+    }
+    c->fwd_S = c->bwd_S = 0;
     return 0;
 }
 

@@ -42,6 +42,7 @@ def _bind(L):
     L.anc_mf_forward.argtypes = [vp, i, vp, vp, vp, vp, vp, vp]
     L.anc_mf_backward.argtypes = [vp, i, vp, vp, vp, vp, vp]
     L.anc_mf_check.argtypes = [vp, vp]
+    L.anc_mf_set_wait_ns.argtypes = [vp, C.c_uint64]
     L.anc_mf_destroy.argtypes = [vp]
     L.anc_mf_destroy.restype = None
     L._mf_bound = True
@@ -86,6 +87,10 @@ class MeanField:
                                 self._stream()))
         check(L.anc_mf_check(self._h, self._stream()))
         return gs
+
+    def set_wait_ns(self, ns: int):
+        """Limit of each device wait (default 2 s) before the kernels give up and report ANC_ETIMEOUT."""
+        check(load().anc_mf_set_wait_ns(self._h, int(ns)))
 
     def pad(self, m: torch.Tensor) -> torch.Tensor:
         """[R, n] (R <= 64) -> [64, npad] f32 on the device, zero padded."""

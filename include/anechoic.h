@@ -231,6 +231,10 @@ ANC_API int anc_mf_forward(anc_meanfield* mf, int S, const float* sched, const f
 ANC_API int anc_mf_backward(anc_meanfield* mf, int S, const float* sched, const float* ckpt, const float* g_m,
                             float* gsched, void* stream);
 ANC_API int anc_mf_check(anc_meanfield* mf, void* stream);
+/* Limit (ns, default 2e9) of each device wait of this context's kernels. A wait that reaches it makes the kernel
+ * record an error, let its own copies and MMAs finish, skip the rest of its work and return; anc_mf_check then
+ * returns ANC_ETIMEOUT and clears the error, and the context stays usable. */
+ANC_API int anc_mf_set_wait_ns(anc_meanfield* mf, uint64_t ns);
 ANC_API void anc_mf_destroy(anc_meanfield* mf);
 
 /* Last device time of a synchronous run on this thread (ms, CUDA events around the launch). */

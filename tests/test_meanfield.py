@@ -157,3 +157,24 @@ def test_tuned_schedule_runs_bit_exact_on_the_engine(pm1, oracle):
     ref = oracle.run_batch(2000, arrays, 9, 0, 130, dense=pm1.dense)
     for c in range(130):
         assert_same(r, {k: v[c] for k, v in ref.items()}, c, f"chain {c}")
+
+
+def test_wait_limit_expiry_is_reported_and_the_context_recovers(pm1):
+    """Failure detection without a fault: with a zero wait limit the GEMM kernel's wait for its TMA tiles gives up
+    at once, records the error, lets its own copy land and returns; the host reads ANC_ETIMEOUT, and after the
+    limit is restored the same context computes the same result as a fresh one."""
+    import anechoic_b200 as A
+    S, R = 20, 64
+    sch = SoftSchedule(S=S, mode="counted")
+    th = torch.tensor(THETA0, dtype=torch.float64, device="cuda")
+    beta, q, u, w = sch.vectors(th)
+    mf = MeanField(pm1)
+    m0 = mf.pad(initial_magnetisations(pm1.n, R, 2))
+    mf.set_wait_ns(0)
+    with pytest.raises(A.AncError) as e:
+        relax(mf, beta, q, u, w, m0)
+    assert e.value.code == -3 and "wait expired" in str(e.value)
+    mf.set_wait_ns(2_000_000_000)
+    out = relax(mf, beta, q, u, w, m0)
+    ref = relax(MeanField(pm1), beta, q, u, w, m0)
+    assert torch.equal(out, ref)
