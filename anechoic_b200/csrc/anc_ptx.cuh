@@ -28,6 +28,10 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t byt
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
 }
 
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
 __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
@@ -59,6 +63,13 @@ __device__ __forceinline__ bool mbar_wait_for(uint32_t bar, uint32_t parity, int
 
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int* err, int code) {
     return mbar_wait_for(bar, parity, err, code, kWaitNs);
+}
+
+// Writer side of a cross-CTA publication: this thread's global stores are made visible to the async proxy (the
+// consumers read them with TMA) and at gpu scope, before the CTA barrier after which one thread releases the flag.
+// Every writer fences its own stores; the release of the publishing thread is not relied on to cover other warps'.
+__device__ __forceinline__ void writer_fence() {
+    asm volatile("fence.proxy.async.global;\n\tfence.acq_rel.gpu;" ::: "memory");
 }
 
 __device__ __forceinline__ bool err_set(const int* err) { return *reinterpret_cast<const volatile int*>(err) != 0; }

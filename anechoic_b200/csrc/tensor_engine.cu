@@ -436,7 +436,7 @@ constexpr int kResStages = 5;
 constexpr int kResMmaWarp = kDW + kResPW;
 constexpr int kResThreads = (kDW + kResPW + 1) * 32;
 constexpr int kResChunks = 17;            // 16 D chunks + 1 n_lin chunk per (step, group)
-constexpr int kErrFlag = 4, kErrJ = 5;
+constexpr int kErrFlag = 4, kErrJ = 5, kErrInit = 6;
 
 struct ResParams {
     int n, S, npairs;
@@ -478,7 +478,7 @@ __global__ void __launch_bounds__(kResThreads, 1)
     uint8_t* stages = ones + 2048;                          // kResStages x 16 KB (1024-aligned)
     uint64_t* bars = reinterpret_cast<uint64_t*>(stages + kResStages * TILE);
     // bars: full[5], empty[5], hready[2], jbar
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kResStages + 3);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kResStages + 4);   // bars: ... jbar, init
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int cs = int(blockIdx.x % kResSlices);
@@ -487,6 +487,7 @@ __global__ void __launch_bounds__(kResThreads, 1)
     int* err = P.err;
     const uint32_t bar_full = smem_u32(bars), bar_empty = smem_u32(bars + kResStages);
     const uint32_t bar_h0 = smem_u32(bars + 2 * kResStages), bar_j = smem_u32(bars + 2 * kResStages + 2);
+    const uint32_t bar_init = smem_u32(bars + 2 * kResStages + 3);   // decision warps: fields of a new pair set
 
     if (tid == 0) {
         for (int s = 0; s < kResStages; ++s) {
@@ -496,6 +497,7 @@ __global__ void __launch_bounds__(kResThreads, 1)
         mbar_init(bar_h0, 1);
         mbar_init(bar_h0 + 8, 1);
         mbar_init(bar_j, 1);
+        mbar_init(bar_init, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     for (int i = tid; i < 2048; i += blockDim.x) ones[i] = i < 128 ? 1 : 0;
@@ -522,6 +524,7 @@ __global__ void __launch_bounds__(kResThreads, 1)
     uint32_t hph[2] = {0u, 0u};            // decision side: completed "h ready" phases per group
     uint32_t q = 0;                        // running chunk index (producers, MMA)
     bool jready = false;
+    uint32_t iph = 0u;                     // MMA thread: completed "fields set" phases
     const bool prof = P.prof != nullptr;
     long long pr[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     const long long t_loop0 = clock64();
@@ -570,10 +573,13 @@ __global__ void __launch_bounds__(kResThreads, 1)
                 }
             }
             tmem_wait_st();
-            asm volatile("fence.proxy.async.global;" ::: "memory");
+            writer_fence();
             tc_fence_before();
             asm volatile("bar.sync 1, %0;" ::"r"(kDW * 32) : "memory");
             if (tid == 0) {
+                // the MMA thread may accumulate into these fields only after they are set: tiles of other slices
+                // can land before this CTA leaves its previous pair
+                mbar_arrive(bar_init);
                 flag_publish(P.flags + G[0] * kResSlices + cs, 1u);
                 flag_publish(P.flags + G[1] * kResSlices + cs, 1u);
             }
@@ -657,7 +663,7 @@ __global__ void __launch_bounds__(kResThreads, 1)
                     int8_t* drow = P.dbuf + ((size_t(G[g]) * 2 + par) * kM + r) * NPAD + cs * kResYS + qq * 16;
                     *reinterpret_cast<uint4*>(drow) = make_uint4(db[0], db[1], db[2], db[3]);
                     P.nlx[((size_t(G[g]) * 2 + par) * kM + r) * 128 + cs * 4 + qq] = int8_t(nl);
-                    asm volatile("fence.proxy.async.global;" ::: "memory");
+                    writer_fence();
                     tc_fence_before();
                     if (prof) { const long long t1 = clock64(); pr[1] += t1 - t0; t0 = t1; }
                     asm volatile("bar.sync 1, %0;" ::"r"(kDW * 32) : "memory");
@@ -723,6 +729,9 @@ __global__ void __launch_bounds__(kResThreads, 1)
                     if (!err_set(err)) mbar_wait(bar_j, 0u, err, kErrJ);
                     jready = true;
                 }
+                if (!err_set(err)) mbar_wait(bar_init, iph & 1u, err, kErrInit);
+                ++iph;
+                tc_fence_after();
                 for (int m = -1; m < S; ++m) {
                     for (int g = 0; g < 2; ++g) {
                         const long long t0 = prof ? clock64() : 0;
@@ -801,6 +810,7 @@ constexpr int kF4Stages = 5;
 constexpr int kF4MmaWarp = kDW + kF4PW;
 constexpr int kF4Threads = (kDW + kF4PW + 1) * 32;
 constexpr int kF4Chunks = 9;              // 8 D tiles (2048 fp4 = 1024 bytes per row) + 1 n_lin tile per step
+constexpr int kF4Cluster = 4;            // CTAs per cluster: a quarter of a replica group on one GPC
 constexpr int kF4SfCol = 160;             // TMEM columns 144..255 hold scale factors 0x7F (1.0)
 
 struct F4Params {
@@ -870,7 +880,7 @@ __global__ void __launch_bounds__(kF4Threads, 1)
     uint8_t* ones = smem + 8 * TILE;                        // 2 KB: row 0 = 128 x int8(1)
     uint8_t* stages = ones + 2048;
     uint64_t* bars = reinterpret_cast<uint64_t*>(stages + kF4Stages * TILE);   // full[5], empty[5], hready, jbar
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kF4Stages + 2);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kF4Stages + 3);   // bars: ... hready, jbar, init
     __shared__ volatile long long s_pub[2];      // profiling: clock64 of this CTA's flag publish, by step parity
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -880,6 +890,7 @@ __global__ void __launch_bounds__(kF4Threads, 1)
     int* err = P.err;
     const uint32_t bar_full = smem_u32(bars), bar_empty = smem_u32(bars + kF4Stages);
     const uint32_t bar_h = smem_u32(bars + 2 * kF4Stages), bar_j = smem_u32(bars + 2 * kF4Stages + 1);
+    const uint32_t bar_init = smem_u32(bars + 2 * kF4Stages + 2);   // decision warps: fields of a new group set
 
     if (tid == 0) {
         for (int s = 0; s < kF4Stages; ++s) {
@@ -888,6 +899,7 @@ __global__ void __launch_bounds__(kF4Threads, 1)
         }
         mbar_init(bar_h, 1);
         mbar_init(bar_j, 1);
+        mbar_init(bar_init, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     for (int i = tid; i < 2048; i += blockDim.x) ones[i] = i < 128 ? 1 : 0;
@@ -922,6 +934,7 @@ __global__ void __launch_bounds__(kF4Threads, 1)
     const int r = (warp & 3) * 32 + lane, qq = warp >> 2;
     uint32_t hph = 0u, q = 0;
     bool jready = false;
+    uint32_t iph = 0u;                     // MMA thread: completed "fields set" phases
     const bool prof = P.prof != nullptr;
     long long pa = 0, pb = 0, pc = 0, pd = 0;   // phase cycle totals; meaning depends on the warp's role
     const long long t_loop0 = clock64();
@@ -970,10 +983,15 @@ __global__ void __launch_bounds__(kF4Threads, 1)
                 }
                 tmem_wait_st();
             }
-            asm volatile("fence.proxy.async.global;" ::: "memory");
+            writer_fence();
             tc_fence_before();
             asm volatile("bar.sync 1, %0;" ::"r"(kDW * 32) : "memory");
-            if (tid == 0) flag_release(P.flags + g * kF4Slices + cs, 1u);
+            if (tid == 0) {
+                // the MMA thread may accumulate into these fields only after they are set: tiles of other slices
+                // can land before this CTA leaves its previous group
+                mbar_arrive(bar_init);
+                flag_release(P.flags + g * kF4Slices + cs, 1u);
+            }
             const float hclf = float(P.hclamp);
             long long last_pub = 0, p_pub = 0, p_wake = 0;   // profiling (thread 0): publish cost, wake - publish
             for (int m = 0; m <= S; ++m) {
@@ -1052,7 +1070,7 @@ __global__ void __launch_bounds__(kF4Threads, 1)
                 uint8_t* drow = P.dbuf + ((size_t(g) * 2 + par) * kM + r) * ROWB + cs * 64 + qq * 16;
                 *reinterpret_cast<uint4*>(drow) = make_uint4(db[0], db[1], db[2], db[3]);
                 P.nlx[((size_t(g) * 2 + par) * kM + r) * 128 + cs * 4 + qq] = int8_t(nl);
-                asm volatile("fence.proxy.async.global;" ::: "memory");
+                writer_fence();
                 tc_fence_before();
                 if (prof) { const long long t1 = clock64(); pb += t1 - t0; t0 = t1; }
                 asm volatile("bar.sync 1, %0;" ::"r"(kDW * 32) : "memory");
@@ -1140,6 +1158,9 @@ __global__ void __launch_bounds__(kF4Threads, 1)
                     if (!err_set(err)) mbar_wait(bar_j, 0u, err, kErrJ);
                     jready = true;
                 }
+                if (!err_set(err)) mbar_wait(bar_init, iph & 1u, err, kErrInit);
+                ++iph;
+                tc_fence_after();
                 long long p_first = 0, p_last = 0, p_nl = 0, p_h = 0, tf0 = 0, tf7 = 0, tf8 = 0;
                 for (int m = -1; m < S; ++m) {
                     const long long t0 = prof ? clock64() : 0;
@@ -1284,7 +1305,7 @@ int max_clusters_t(int* out) {
 }
 
 size_t res_smem_bytes() {
-    return 1024 + 16 * size_t(kResYS) * kKChunk + 2048 + size_t(kResStages) * kM * kKChunk + (2 * kResStages + 3) * 8 + 16;
+    return 1024 + 16 * size_t(kResYS) * kKChunk + 2048 + size_t(kResStages) * kM * kKChunk + (2 * kResStages + 4) * 8 + 16;
 }
 
 // Concurrent pair slots of the resident kernel (32 co-resident CTAs each).
@@ -1431,7 +1452,7 @@ int ensure_bias_perm(TensorInstance* ti, const int32_t* bias, std::string* why) 
 }
 
 size_t f4_smem_bytes() {
-    return 1024 + 8 * size_t(kM) * kKChunk + 2048 + size_t(kF4Stages) * kM * kKChunk + (2 * kF4Stages + 2) * 8 + 16;
+    return 1024 + 8 * size_t(kM) * kKChunk + 2048 + size_t(kF4Stages) * kM * kKChunk + (2 * kF4Stages + 3) * 8 + 16;
 }
 
 // Concurrent group slots of the fp4 kernel (16 co-resident CTAs each).
@@ -1444,7 +1465,23 @@ int f4_group_slots(int ngroups, int* out) {
     if (e == cudaSuccess) e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return int(e);
-    *out = std::max(0, std::min(ngroups, (per_sm * sms) / kF4Slices));
+    int clusters = 0;
+    {
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = kF4Cluster;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        cfg.gridDim = dim3(kF4Slices);
+        cfg.blockDim = dim3(kF4Threads);
+        cfg.dynamicSmemBytes = smem;
+        e = cudaOccupancyMaxActiveClusters(&clusters, fn, &cfg);
+        if (e != cudaSuccess) return int(e);
+    }
+    *out = std::max(0, std::min(ngroups, std::min((per_sm * sms) / kF4Slices, clusters / (kF4Slices / kF4Cluster))));
     return 0;
 }
 
@@ -1521,11 +1558,15 @@ int f4_run(TensorInstance* ti, const TensorRun& r, cudaStream_t st, std::string*
     const size_t smem = f4_smem_bytes();
     e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     cudaLaunchConfig_t cfg = {};
-    cudaLaunchAttribute at[1];
+    cudaLaunchAttribute at[2];
     at[0].id = cudaLaunchAttributeCooperative;
     at[0].val.cooperative = 1;
+    at[1].id = cudaLaunchAttributeClusterDimension;
+    at[1].val.clusterDim.x = kF4Cluster;
+    at[1].val.clusterDim.y = 1;
+    at[1].val.clusterDim.z = 1;
     cfg.attrs = at;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = 2;
     cfg.gridDim = dim3(kF4Slices * slots);
     cfg.blockDim = dim3(kF4Threads);
     cfg.dynamicSmemBytes = smem;

@@ -39,7 +39,7 @@ constexpr int kSStages = 4;
 constexpr uint32_t kSTile = 128 * 128;     // 16 KB
 constexpr uint32_t kSStage = 3 * kSTile;   // J tile + two dS tiles
 constexpr int kSChunks = kSSlices + 2;     // dS chunks + 2 n_lin chunks per step
-constexpr int kErrFull = 1, kErrEmpty = 2, kErrHready = 3, kErrFlag = 4;
+constexpr int kErrFull = 1, kErrEmpty = 2, kErrHready = 3, kErrFlag = 4, kErrInit = 6;
 
 struct StreamParams {
     int n, R, S;
@@ -75,8 +75,8 @@ __global__ void __launch_bounds__(kSThreads, 1)
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t* stages = smem;                                 // kSStages x (J, dS0, dS1)
     uint8_t* ones = stages + kSStages * kSStage;            // 2 KB: row 0 = 128 x int8(1)
-    uint64_t* bars = reinterpret_cast<uint64_t*>(ones + 2048);   // full[4], empty[4], hready
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kSStages + 1);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(ones + 2048);   // full[4], empty[4], hready, init
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kSStages + 2);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int cs = int(blockIdx.x);
@@ -84,6 +84,7 @@ __global__ void __launch_bounds__(kSThreads, 1)
     int* err = P.err;
     const uint32_t bar_full = smem_u32(bars), bar_empty = smem_u32(bars + kSStages);
     const uint32_t bar_h = smem_u32(bars + 2 * kSStages);
+    const uint32_t bar_init = smem_u32(bars + 2 * kSStages + 1);   // decision warps: fields of a new pair set
 
     if (tid == 0) {
         for (int s = 0; s < kSStages; ++s) {
@@ -91,6 +92,7 @@ __global__ void __launch_bounds__(kSThreads, 1)
             mbar_init(bar_empty + 8 * s, 1);
         }
         mbar_init(bar_h, 1);
+        mbar_init(bar_init, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     for (int i = tid; i < 2048; i += blockDim.x) ones[i] = i < 128 ? 1 : 0;
@@ -165,13 +167,17 @@ __global__ void __launch_bounds__(kSThreads, 1)
                 }
                 tmem_wait_st();
             }
-            asm volatile("fence.proxy.async.global;" ::: "memory");
+            writer_fence();
             tc_fence_before();
             asm volatile("bar.sync 1, %0;" ::"r"(kSDW * 32) : "memory");
-            if (tid == 0)
+            if (tid == 0) {
+                // the MMA thread may accumulate into these fields only after they are set: tiles of other slices
+                // can land before this CTA leaves its previous pair
+                mbar_arrive(bar_init);
                 asm volatile("fence.acq_rel.gpu;\n\tst.release.gpu.global.u32 [%0], %1;" ::"l"(P.flags + pr * kSSlices + cs),
                              "r"(1u)
                              : "memory");
+            }
             const int32_t hcl = P.hclamp;
             for (int m = 0; m <= S; ++m) {
                 long long t0 = prof ? clock64() : 0;
@@ -272,7 +278,7 @@ __global__ void __launch_bounds__(kSThreads, 1)
                 P.nlx[(drow0 + size_t(par) * kSM) * 256 + 2 * cs + jl] = int8_t(__popcll(lm));
                 sw ^= fm;
                 dw = fm;
-                asm volatile("fence.proxy.async.global;" ::: "memory");
+                writer_fence();
                 tc_fence_before();
                 if (prof) { const long long t1 = clock64(); pb += t1 - t0; t0 = t1; }
                 asm volatile("bar.sync 1, %0;" ::"r"(kSDW * 32) : "memory");
@@ -348,6 +354,8 @@ __global__ void __launch_bounds__(kSThreads, 1)
         } else if (warp == kSMmaWarp) {
             // ---------------- MMA thread ----------------
             if (lane == 0) {
+                if (!err_set(err)) mbar_wait(bar_init, uint32_t(pr) & 1u, err, kErrInit);
+                tc_fence_after();
                 for (int m = -1; m < S; ++m) {
                     const long long t0 = prof ? clock64() : 0;
                     for (int c = 0; c < kSChunks; ++c, ++q) {
@@ -402,7 +410,7 @@ __global__ void __launch_bounds__(kSThreads, 1)
     }
 }
 
-size_t stream_smem_bytes() { return 1024 + size_t(kSStages) * kSStage + 2048 + (2 * kSStages + 1) * 8 + 16; }
+size_t stream_smem_bytes() { return 1024 + size_t(kSStages) * kSStage + 2048 + (2 * kSStages + 2) * 8 + 16; }
 
 }  // namespace
 

@@ -49,11 +49,13 @@ def test_stream_kernel_vs_oracle(k4_16384, oracle):
 
 
 def test_stream_kernel_equals_plain(k4_16384):
+    """300 anneals: two rounds of replica-group pairs on the same CTAs (the second pair's fields must be set before
+    the first tiles of other slices are accumulated)."""
     inst, dev = k4_16384
     sc = dict(K4_SCHED, S=25)
     tb = A.Tables.from_schedule(A.Schedule(**sc))
-    a = A.run(dev, tb, 8, 0, 256, trace=True, engine="tensor")
-    b = A.run(dev, tb, 8, 0, 256, trace=True, engine="plain")
+    a = A.run(dev, tb, 8, 0, 300, trace=True, engine="tensor")
+    b = A.run(dev, tb, 8, 0, 300, trace=True, engine="plain")
     assert np.array_equal(a.spins, b.spins) and np.array_equal(a.trace, b.trace)
     assert np.array_equal(a.sum_sh, b.sum_sh) and np.array_equal(a.sum_bs, b.sum_bs)
     assert np.array_equal(a.flips, b.flips)

@@ -74,8 +74,8 @@ def test_ragged_chain_count_and_offset(pm1, oracle, kind):
 
 @pytest.mark.parametrize("kind", KINDS)
 def test_tensor_equals_plain(pm1, kind):
-    """Both engines on the same 1100 trials (more replica groups than the fp4 kernel's co-resident slots):
-    identical results."""
+    """Both engines on the same 1100 trials: more replica groups than co-resident slots, so CTAs run a second round
+    (its fields must be set before tiles from faster slices are accumulated). Identical results."""
     inst, dev = pm1
     tb = A.Tables.from_schedule(A.Schedule(S=300, kappa=2.0, ramp=True))
     a = A.run(dev, tb, 11, 500, 1100, trace=True, engine="tensor", tensor_kind=kind)
