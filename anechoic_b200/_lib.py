@@ -116,11 +116,19 @@ def opts(engine: str = "auto", wide="auto", profile: bool = False, tensor_kind: 
     return o
 
 
-PROFILE_FIELDS = ("wait_fields", "decide", "nlin_publish", "cluster_barrier", "nlin_read", "mma_wait_tma",
-                  "mma_phase", "tma_wait_stage", "step", "ctas", "cluster", "max_active_clusters", "mma_issue",
-                  "mma_commit", "first_tile_after_publish", "last_tile_after_publish", "nlin_tile_after_publish",
+# Tensor-engine phase counters (SM cycles per step, averaged over CTAs). Names follow the fp4 kernel; the int8 and
+# streaming kernels fill slots 2-7 with: named barrier + n_lin publish, cluster barrier, n_lin read, MMA waiting for
+# TMA stages, MMA phase, TMA waiting for free stages.
+PROFILE_FIELDS = ("wait_fields", "decide", "publish", "draw", "exchange", "mma_wait", "mma_phase", "tma_wait_stage",
+                  "step", "ctas", "cluster", "max_active_clusters", "mma_issue", "mma_commit",
+                  "first_tile_after_publish", "last_tile_after_publish", "nlin_tile_after_publish",
                   "fields_commit_after_publish", "tile0_flags_after_publish", "tile7_flags_after_publish",
-                  "tile0_tma_after_publish", "tile7_tma_after_publish")
+                  "tile0_stored_after_publish", "tile7_stored_after_publish",
+                  *(f"tile{t}_full_after_publish" for t in range(2, 7)),
+                  *(f"warp{w}_tile7_stored_after_publish" for w in range(8)),
+                  *(f"warp{w}_tile7_flags_after_publish" for w in range(8)),
+                  *(f"tile{t}_issued_after_publish" for t in range(8)),
+                  *(f"tile{t}_mma_wait" for t in range(8)))
 
 
 def last_kernel():

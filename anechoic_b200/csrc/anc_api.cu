@@ -373,9 +373,10 @@ int run_host_impl(anc_instance* I, anc_tables* tb, uint64_t seed, uint32_t off, 
         const size_t ns = anc::kTensorProfSlots;
         std::vector<long long> h(size_t(I->prof_ctas) * ns);
         CK(cudaMemcpy(h.data(), I->w_prof.p, h.size() * sizeof(long long), cudaMemcpyDeviceToHost));
-        g_prof.assign(22, 0.0);
-        const int slot_of[19] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 12, 13, 14, 15, 16, 17, 18, 19, 20, 21};   // slot -> output
-        for (int s = 0; s < 19; ++s) {
+        g_prof.assign(22 + (ns - 19), 0.0);
+        int slot_of[anc::kTensorProfSlots] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 12, 13, 14, 15, 16, 17, 18, 19, 20, 21};
+        for (size_t s = 19; s < ns; ++s) slot_of[s] = int(22 + s - 19);                  // slot -> output
+        for (size_t s = 0; s < ns; ++s) {
             double acc = 0;
             for (int b = 0; b < I->prof_ctas; ++b) acc += double(h[size_t(b) * ns + s]);
             g_prof[slot_of[s]] = acc / I->prof_ctas / std::max(1, I->prof_S);

@@ -27,7 +27,7 @@ struct TensorInstance {
 };
 
 // Slots per CTA of the opt-in phase profile (clock64 totals, see tensor_engine.cu).
-constexpr int kTensorProfSlots = 24;
+constexpr int kTensorProfSlots = 56;
 
 // Operand format of the field update: int8 (any |J| <= 127) or packed fp4 e2m1 (|J| <= 1, NP = 2048).
 constexpr int TENSOR_KIND_AUTO = 0, TENSOR_KIND_INT8 = 1, TENSOR_KIND_FP4 = 2;

@@ -71,13 +71,14 @@ struct TensorParams {
 };
 
 // opt-in phase profile (clock64 cycles summed over the steps, per CTA):
-//   0 decision warps waiting for h   1 TMEM load + decide + D store   2 named barrier + n_lin publish
-//   3 cluster barrier (decision warps; fp4 kernel: flag publish alone)   4 n_lin read (fp4 kernel: fields ready
-//     minus own publish)   5 MMA thread waiting for TMA stages   6 MMA thread: barrier end -> last commit issued
-//   7 TMA thread waiting for free stages   8 whole step loop   9 MMA issue   10 MMA commits
-//   fp4 kernel, measured from this CTA's own publish: 11 first D tile in shared memory, 12 last D tile, 13 n_lin
-//     tile, 14 fields-ready commit issued, 15 / 16 flags of D tile 0 / 7 seen by the producer, 17 / 18 TMA of D tile
-//     0 / 7 issued
+//   0 decision warps waiting for h   1 TMEM load + decide + D store   2 named barrier + n_lin publish (fp4 kernel:
+//     named barrier + flag release)   3 cluster barrier (fp4 kernel: the next step's draws)   4 n_lin read (fp4
+//     kernel: the exchange, flags to last tile stored and n_lin summed)   5 MMA thread waiting for stages
+//   6 MMA thread: barrier end -> last commit issued   7 TMA thread waiting for free stages   8 whole step loop
+//   9 MMA issue   10 MMA commits
+//   fp4 kernel, measured from this CTA's own publish: 11 first D tile full, 12 last D tile full, 14 fields-ready
+//     commit issued, 15 / 16 flags of D tile 0 / 7 seen by decision thread 0, 17 / 18 its copies of D tile 0 / 7
+//     landed and arrived
 constexpr int kProfSlots = kTensorProfSlots;
 
 // ------------------------------------------------------------------------------------------------ helpers
@@ -795,23 +796,38 @@ __global__ void __launch_bounds__(kResThreads, 1)
 // runs as tcgen05.mma.kind::mxf4.block_scale (M 128, N 128, K 64) with every block scale 1.0 (ue8m0 0x7F) and fp32
 // accumulation, exact for these integer fields. A cooperative persistent grid of 16 y-slices x G replica groups:
 // CTA (group slot, slice cs) owns RNG lanes 16cs .. 16cs+15 (128 columns at p = 8l + k), keeps its J slice
-// (128 rows x 2048 fp4 = 128 KB) resident, and runs one group of 128 replicas at a time:
-//   16 decision warps: thread (replica r, quarter qq) owns lanes 16cs + 4qq + j (j < 4) x 8 rounds = 32 slots =
-//     TMEM columns qq*32 + j*8 + k; it decides (lanes interleaved for ILP), writes its 32 D nibbles (16 bytes) and
-//     its n_lin partial byte, and one thread publishes flag[g][cs] = m + 2.
-//   4 producer warps poll the 16 slice flags warp-wide and TMA each 128 x 128-byte D tile (256 K values = two
-//     source slices) as both slices publish; a 9th tile carries the n_lin partials.
-//   the MMA thread: 4 x mxf4 MMAs per D tile into the fp32 field accumulator, 2 x i8 MMAs (N 16) of the partials
-//     against a ones row into an int32 n_lin accumulator.
+// (128 rows x 2048 fp4 = 128 KB) resident, and runs one group of 128 replicas at a time. Per step:
+//   8 decision warps: thread (replica r, half hf) owns quarters qq = 2hf, 2hf+1; quarter qq is lanes
+//     16cs + 4qq + j (j < 4) x 8 rounds = 32 slots = TMEM columns qq*32 + j*8 + k. The step's draws were made while
+//     the previous step's MMAs ran (the lane states live in TMEM); the thread reads its 64 fields, decides,
+//     writes its 64 D nibbles (32 bytes) and two n_lin partial bytes to the group's exchange buffers, and after a
+//     named barrier one thread publishes flag[g][cs] = m + 2 with a release store (the barrier orders every
+//     writer's stores before it, and release is cumulative over them).
+//   The same warps then fetch the step's D: tile t (128 replicas x 256 K, the slices of CTAs 2t and 2t+1) is
+//     loaded once both slice flags are seen, with 16-byte asynchronous L2 copies (four per thread, up to 6 tiles in flight),
+//     into a stage of a 6-deep shared-memory ring in the 128-byte-swizzled K-major layout the MMA reads; each
+//     thread fences the async proxy and one lane per warp arrives on the stage's barrier. Each thread also sums
+//     its replica's 64 n_lin partial bytes for the next step's correction.
+//   The MMA thread: 4 mxf4 MMAs per tile into the fp32 fields in TMEM, a commit per stage to free it, and a commit
+//     of "fields ready" after the 8th tile.
+//   The poller warp: watches the 16 slice flags of the group in L2 and mirrors what it sees into shared memory
+//     (acquire at gpu scope, release at cta scope), so the decision warps wait on shared memory.
+// The exchange crosses L2 through the generic proxy only; the async proxy reads shared memory alone, after the
+// loaders' proxy fence. 10 warps leave 168 registers per thread (a fifth warp on an SM sub-partition would cap
+// them at 96).
 constexpr int kF4Slices = 16;
 constexpr int kF4YS = 128;
-constexpr int kF4PW = 3;               // producer warps (20 warps in all: 96 registers per thread)
-constexpr int kF4Stages = 5;
-constexpr int kF4MmaWarp = kDW + kF4PW;
-constexpr int kF4Threads = (kDW + kF4PW + 1) * 32;
-constexpr int kF4Chunks = 9;              // 8 D tiles (2048 fp4 = 1024 bytes per row) + 1 n_lin tile per step
+constexpr int kF4DW = 8;                  // decision warps (two quarters of 32 columns per thread)
+constexpr int kF4Stages = 6;
+constexpr int kF4Tiles = 8;               // D tiles per step (2048 fp4 = 1024 bytes per row, 128 bytes per tile)
+constexpr int kF4MmaWarp = kF4DW;
+constexpr int kF4PollWarp = kF4DW + 1;   // watches the group's 16 slice flags for the whole CTA
+constexpr int kF4Threads = (kF4DW + 2) * 32;
 constexpr int kF4Cluster = 4;            // CTAs per cluster: a quarter of a replica group on one GPC
 constexpr int kF4SfCol = 160;             // TMEM columns 144..255 hold scale factors 0x7F (1.0)
+constexpr int kF4RngCol = 256;            // TMEM columns 256..319: RNG lane states, 32 per half hf
+constexpr int kF4TmemCols = 512;
+constexpr int kF4Bars = 2 * kF4Stages + 3;   // full[6], empty[6], fields ready, J loaded, drain
 
 struct F4Params {
     int n, S, ngroups;
@@ -826,7 +842,7 @@ struct F4Params {
     int nchains;
     uint32_t* flags;                    // [ngroups][16] (zeroed)
     uint8_t* dbuf;                      // [ngroups][2][128][1024] packed e2m1
-    int8_t* nlx;                        // [ngroups][2][128][128]
+    int8_t* nlx;                        // [ngroups][2][128][128]: byte 4 cs + qq = partial n_lin
     uint32_t* out_spins;                // [nchains][64] (zeroed)
     unsigned long long* out_sum_sh;
     unsigned long long* out_sum_bs;
@@ -837,51 +853,219 @@ struct F4Params {
     long long* prof;
 };
 
-// One decision pass of a thread's 32 columns (column = 8 j + k: RNG lane j of the thread, round k), interleaving the
-// four lanes' streams. Outputs the flip mask and the mask of slots inside the linear band -2T < z < 2T.
-//   s*h: the field in f32 with its sign flipped for s = -1 (bit 31 of ~sw), clamped when the range plan asks;
-//   z = s*h*65536 + q -/+ corr through the exact conversion 1.5*2^23 + x (|x| < 2^22): the low 16 bits of that
-//   encoding are x, so encoding << 16 = x * 65536 modulo 2^32;
-//   r = floor((u16 - 32768) * 4T / 65536) = mulhi((u16 - 32768) << 16, 4T).
-template <bool CLAMP>
-__device__ __forceinline__ void f4_decide(Xoshiro (&rng)[4], const uint32_t (&hv)[32], uint32_t downs, uint32_t dw,
-                                          int32_t xs, int32_t twocorr, int32_t fourT, int32_t c1, uint32_t lw,
-                                          float hclf, uint32_t& fm, uint32_t& lm) {
-    fm = 0u;
-    lm = 0u;
+// The step's draws for the thread's eight RNG lanes (quarter e = jj / 4, lane j = jj % 4; 8 rounds each, every
+// lane's stream in round order), kept as their top 16 bits: pk[16e + 4j + k/2] holds column j*8 + k of quarter e in
+// its high half for even k and in its low half for odd k. The lane states live in TMEM (32 columns at taddr:
+// a, b, c, d of lanes jj = 0..7), loaded, advanced and stored back here.
+__device__ __forceinline__ void f4_draw(uint32_t taddr, uint32_t (&pk)[32]) {
+    uint32_t st[32];
+    tmem_ld32(taddr, st);
+    tmem_wait_ld();
+    Xoshiro rng[8];
+#pragma unroll
+    for (int jj = 0; jj < 8; ++jj) rng[jj] = Xoshiro{st[4 * jj], st[4 * jj + 1], st[4 * jj + 2], st[4 * jj + 3]};
 #pragma unroll
     for (int k = 0; k < 8; ++k)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int col = j * 8 + k;
-            const uint32_t u = rng_next(rng[j]);
-            float hsf = __uint_as_float(hv[col] ^ ((downs << (31 - col)) & 0x80000000u));
-            if (CLAMP) hsf = fminf(fmaxf(hsf, -hclf), hclf);
-            const int32_t zb = __float_as_int(hsf + 12582912.0f);
-            int32_t zt = (zb << 16) + xs;
-            if ((dw >> col) & 1u) zt += twocorr;
-            const int32_t thr = __mulhi(int32_t((u & 0xffff0000u) ^ 0x80000000u), fourT);
-            if (zt < thr) fm |= 1u << col;
-            if (uint32_t(zt + c1) < lw) lm |= 1u << col;
+        for (int jj = 0; jj < 8; ++jj) {
+            const uint32_t u = rng_next(rng[jj]);
+            uint32_t& w = pk[16 * (jj >> 2) + 4 * (jj & 3) + k / 2];
+            if (k & 1) w |= u >> 16;
+            else w = u & 0xffff0000u;
         }
+#pragma unroll
+    for (int jj = 0; jj < 8; ++jj) {
+        st[4 * jj] = rng[jj].a;
+        st[4 * jj + 1] = rng[jj].b;
+        st[4 * jj + 2] = rng[jj].c;
+        st[4 * jj + 3] = rng[jj].d;
+    }
+    tmem_st32(taddr, st);
+    tmem_wait_st();
+}
+
+// One decision pass over quarter E's 32 columns (fields hv, packed draws pk[16E ..]). Outputs the flip mask and
+// the mask of slots inside the linear band -2T < z < 2T.
+//   r = floor((u16 - 32768) * 4T / 65536) = mulhi((u16 - 32768) << 16, 4T);
+//   s*h: the field in f32 with its sign flipped for s = -1 (bit 31 of ~sw), clamped when the range plan asks;
+//   z = s*h*65536 + q -/+ corr through the exact conversion 1.5*2^23 + x (|x| < 2^22): the low 16 bits of that
+//   encoding are x, so encoding << 16 = x * 65536 modulo 2^32.
+template <bool CLAMP, int E>
+__device__ __forceinline__ void f4_decide(const uint32_t (&pk)[32], const uint32_t (&hv)[32], uint32_t downs,
+                                          uint32_t dw, int32_t xs, int32_t twocorr, int32_t fourT, int32_t c1,
+                                          uint32_t lw, float hclf, uint32_t& fm, uint32_t& lm) {
+    fm = 0u;
+    lm = 0u;
+#pragma unroll
+    for (int col = 0; col < 32; ++col) {
+        const int j = col >> 3, k = col & 7;
+        const uint32_t w = pk[16 * E + 4 * j + k / 2];
+        const uint32_t u16 = (k & 1) ? (w << 16) : (w & 0xffff0000u);
+        const int32_t thr = __mulhi(int32_t(u16 ^ 0x80000000u), fourT);
+        float hsf = __uint_as_float(hv[col] ^ ((downs << (31 - col)) & 0x80000000u));
+        if (CLAMP) hsf = fminf(fmaxf(hsf, -hclf), hclf);
+        const int32_t zb = __float_as_int(hsf + 12582912.0f);
+        int32_t zt = (zb << 16) + xs;
+        if ((dw >> col) & 1u) zt += twocorr;
+        if (zt < thr) fm |= 1u << col;
+        if (uint32_t(zt + c1) < lw) lm |= 1u << col;
+    }
+}
+
+// dS nibbles of 8 columns: flipped down->up = +2 (0x4), up->down = -2 (0xC); word w holds columns 8w .. 8w+7.
+__device__ __forceinline__ uint4 f4_dnibbles(uint32_t fm, uint32_t fdn) {
+    uint32_t db[4];
+#pragma unroll
+    for (int w = 0; w < 4; ++w) {
+        uint32_t a8 = (fm >> (8 * w)) & 0xFFu, b8 = (fdn >> (8 * w)) & 0xFFu;
+        a8 = (a8 | (a8 << 12)) & 0x000F000Fu; a8 = (a8 | (a8 << 6)) & 0x03030303u; a8 = (a8 | (a8 << 3)) & 0x11111111u;
+        b8 = (b8 | (b8 << 12)) & 0x000F000Fu; b8 = (b8 | (b8 << 6)) & 0x03030303u; b8 = (b8 | (b8 << 3)) & 0x11111111u;
+        db[w] = (a8 << 2) | (b8 << 3);
+    }
+    return make_uint4(db[0], db[1], db[2], db[3]);
+}
+
+// Profiling marks of decision thread 0 in one exchange (clock64), or unused.
+struct F4ExMarks {
+    long long flags0, flags7, stored0, stored7;
+};
+
+// 16-byte global -> shared copy through L2 only (cp.async.cg), and its commit-group bookkeeping.
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// Wait until at most n of this thread's commit groups are pending (n folds to a constant once the caller's loop is
+// unrolled; larger n waits for all).
+__device__ __forceinline__ void cp_async_wait(int n) {
+    switch (n) {
+        case 1: asm volatile("cp.async.wait_group 1;" ::: "memory"); break;
+        case 2: asm volatile("cp.async.wait_group 2;" ::: "memory"); break;
+        case 3: asm volatile("cp.async.wait_group 3;" ::: "memory"); break;
+        case 4: asm volatile("cp.async.wait_group 4;" ::: "memory"); break;
+        case 5: asm volatile("cp.async.wait_group 5;" ::: "memory"); break;
+        case 6: asm volatile("cp.async.wait_group 6;" ::: "memory"); break;
+        default: asm volatile("cp.async.wait_group 0;" ::: "memory"); break;
+    }
+}
+
+// Fetch one step's D (step m, parity m & 1; m = -1 is the initial state) into the ring: 8 tiles at ring positions
+// q .. q+7, by the 256 decision threads: warp w copies tile rows 16w .. 16w+15, its copy instruction c covering the
+// four whole 128-byte rows 16w + 4c .. 16w + 4c + 3 (lane: row + lane / 8, 16-byte chunk lane % 8), so each
+// instruction touches four cache lines. Copies are asynchronous,
+// one commit group per tile. Tiles 0-5 go out at once (the previous step's MMAs freed every stage before its fields
+// were ready); tiles 0-3 are marked full as they land, so that the MMAs which free the stages of tiles 6 and 7 run
+// meanwhile; then 6 and 7 go out and 4-7 are marked full in order. A tile is marked full once its group has
+// landed: the thread fences the async proxy and its warp arrives on the stage's barrier. Returns the replica's n_lin
+// (the sum of its 64 partial bytes) when want_nlin, else 0. ok (warp-uniform) is false once this warp saw an error;
+// every wait is bounded, and after an error the warp stops copying and arriving but still waits for the copies it
+// has in flight.
+__device__ __forceinline__ int32_t f4_exchange(const F4Params& P, int g, int m, uint32_t stages_u32, uint32_t bar_full,
+                                               uint32_t bar_empty, uint32_t q, int tid, int r, bool want_nlin,
+                                               const uint32_t* s_flag, uint32_t tbase, bool& ok, bool prof,
+                                               F4ExMarks& mk) {
+    constexpr uint32_t TILE = kM * kKChunk;
+    static_assert(kF4Stages == 6 && kF4Tiles == 8, "the issue order below is written for 8 tiles on 6 stages");
+    const int lane = tid & 31;
+    int* err = P.err;
+    const int par = m & 1;
+    const uint32_t target = tbase + uint32_t(m + 2);    // the slice flags' value for step m, in the mirror's count
+    const int row0 = (tid >> 5) * 16 + (lane >> 3), ch = lane & 7;    // first tile row, 16-byte chunk of this thread
+    const uint8_t* src = P.dbuf + (size_t(g * 2 + par) * kM + row0) * 1024 + ch * 16;
+    // 128-byte swizzle: chunk ch of row x at ch ^ (x mod 8); rows row0 + 4c have x mod 8 = (row0 mod 8) ^ 4 (c & 1)
+    const uint32_t dst0 = uint32_t(row0 * 128 + ((ch ^ (row0 & 7)) << 4));
+    const uint32_t dst1 = uint32_t(row0 * 128 + ((ch ^ ((row0 + 4) & 7)) << 4));
+    // copy tile t into its stage once its slices are published (and, for t >= 6, its stage is free)
+    auto issue = [&](int t) {
+        const uint32_t qt = q + uint32_t(t), s = qt % kF4Stages, u = qt / kF4Stages;
+        if (ok && u >= 1) ok = __all_sync(0xffffffffu, mbar_wait(bar_empty + 8 * s, (u - 1) & 1u, err, kErrEmpty));
+        if (ok) {
+            // both slices published: every lane acquires the poller's mirror of their flags (cta scope; the poller
+            // acquired them at gpu scope)
+            const uint32_t fa = smem_u32(s_flag + 2 * t), fb = smem_u32(s_flag + 2 * t + 1);
+            const uint64_t t0 = globaltimer();
+            bool seen = false;
+            for (uint32_t k = 1;; ++k) {
+                uint32_t va, vb;
+                asm volatile("ld.acquire.cta.shared::cta.u32 %0, [%1];" : "=r"(va) : "r"(fa) : "memory");
+                asm volatile("ld.acquire.cta.shared::cta.u32 %0, [%1];" : "=r"(vb) : "r"(fb) : "memory");
+                if (va >= target && vb >= target) { seen = true; break; }
+                if ((k & 255u) == 0 && globaltimer() - t0 > kWaitNs) {
+                    atomicCAS(err, 0, kErrFlag);
+                    break;
+                }
+            }
+            ok = __all_sync(0xffffffffu, seen);
+        }
+        if (prof && lane == 0) {
+            if (t == 0) mk.flags0 = clock64();
+            if (t == kF4Tiles - 1) mk.flags7 = clock64();
+        }
+        if (ok) {
+            const uint32_t st = stages_u32 + s * TILE;
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+                cp_async16(st + uint32_t(c * 512) + ((c & 1) ? dst1 : dst0), src + size_t(c) * 4096 + t * 128);
+        }
+        cp_async_commit();          // one group per tile, empty when the copies were skipped
+    };
+    // mark tile t full once its group has landed; `later` groups were committed after it
+    auto arrive = [&](int t, int later) {
+        cp_async_wait(later);
+        if (ok) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(bar_full + 8 * ((q + uint32_t(t)) % kF4Stages));
+        }
+        if (prof && lane == 0) {
+            if (t == 0) mk.stored0 = clock64();
+            if (t == kF4Tiles - 1) mk.stored7 = clock64();
+        }
+    };
+#pragma unroll
+    for (int t = 0; t < 6; ++t) issue(t);
+    arrive(0, 5);
+    arrive(1, 4);
+    arrive(2, 3);
+    arrive(3, 2);
+    issue(6);
+    issue(7);
+    arrive(4, 3);
+    arrive(5, 2);
+    arrive(6, 1);
+    arrive(7, 0);
+    int32_t nl = 0;
+    if (ok && want_nlin) {
+        // every warp saw all 16 flags before its last tile
+        const uint4* np = reinterpret_cast<const uint4*>(P.nlx + (size_t(g * 2 + par) * kM + r) * 128);
+        uint4 nv[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) nv[i] = __ldcg(np + i);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            nl = __dp4a(int(nv[i].x), 0x01010101, nl);
+            nl = __dp4a(int(nv[i].y), 0x01010101, nl);
+            nl = __dp4a(int(nv[i].z), 0x01010101, nl);
+            nl = __dp4a(int(nv[i].w), 0x01010101, nl);
+        }
+    }
+    return nl;
 }
 
 __global__ void __launch_bounds__(kF4Threads, 1)
-    tensor_fp4_kernel(const __grid_constant__ CUtensorMap mapD, const __grid_constant__ CUtensorMap mapNL,
-                      const __grid_constant__ CUtensorMap mapJ, const __grid_constant__ F4Params P) {
-    constexpr int R = 8, ROWB = 1024;                       // rounds; bytes per packed D / J row
+    tensor_fp4_kernel(const __grid_constant__ CUtensorMap mapJ, const __grid_constant__ F4Params P) {
+    constexpr int R = 8;                                    // rounds
     constexpr uint32_t TILE = kM * kKChunk;                 // 16 KB tile (128 rows x 128 bytes)
     constexpr uint32_t IDESC_F4 = (1u << 7) | (1u << 10) | (uint32_t(kF4YS >> 3) << 17) | (1u << 23) | (uint32_t(kM >> 4) << 24);
-    constexpr uint32_t IDESC_NL = (2u << 4) | (1u << 7) | (1u << 10) | (uint32_t(16 >> 3) << 17) | (uint32_t(kM >> 4) << 24);
 
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t* jres = smem;                                   // 8 x 16 KB
-    uint8_t* ones = smem + 8 * TILE;                        // 2 KB: row 0 = 128 x int8(1)
-    uint8_t* stages = ones + 2048;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(stages + kF4Stages * TILE);   // full[5], empty[5], hready, jbar
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kF4Stages + 3);   // bars: ... hready, jbar, init
+    uint8_t* stages = smem + 8 * TILE;                      // kF4Stages x 16 KB
+    uint64_t* bars = reinterpret_cast<uint64_t*>(stages + kF4Stages * TILE);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + kF4Bars);
     __shared__ volatile long long s_pub[2];      // profiling: clock64 of this CTA's flag publish, by step parity
+    __shared__ uint32_t s_flag[kF4Slices];       // the poller's mirror of the slice flags: gi * (S + 2) + flag
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int cs = int(blockIdx.x % kF4Slices);
@@ -890,23 +1074,22 @@ __global__ void __launch_bounds__(kF4Threads, 1)
     int* err = P.err;
     const uint32_t bar_full = smem_u32(bars), bar_empty = smem_u32(bars + kF4Stages);
     const uint32_t bar_h = smem_u32(bars + 2 * kF4Stages), bar_j = smem_u32(bars + 2 * kF4Stages + 1);
-    const uint32_t bar_init = smem_u32(bars + 2 * kF4Stages + 2);   // decision warps: fields of a new group set
+    const uint32_t bar_fin = smem_u32(bars + 2 * kF4Stages + 2);    // MMA thread: drain before TMEM is freed
 
+    if (tid < kF4Slices) s_flag[tid] = 0u;
     if (tid == 0) {
         for (int s = 0; s < kF4Stages; ++s) {
-            mbar_init(bar_full + 8 * s, 1);
+            mbar_init(bar_full + 8 * s, kF4DW);
             mbar_init(bar_empty + 8 * s, 1);
         }
         mbar_init(bar_h, 1);
         mbar_init(bar_j, 1);
-        mbar_init(bar_init, 1);
+        mbar_init(bar_fin, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    for (int i = tid; i < 2048; i += blockDim.x) ones[i] = i < 128 ? 1 : 0;
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     if (warp == kF4MmaWarp) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                     "r"(256)
+                     "r"(kF4TmemCols)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -914,7 +1097,7 @@ __global__ void __launch_bounds__(kF4Threads, 1)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
-    if (warp == kDW && lane == 0) {
+    if (warp == kF4MmaWarp && lane == 0) {
         mbar_arrive_expect_tx(bar_j, 8 * TILE);
         for (int kc = 0; kc < 8; ++kc) tma_load_2d(smem_u32(jres + kc * TILE), &mapJ, kc * kKChunk, cs * kF4YS, bar_j);
     }
@@ -931,25 +1114,31 @@ __global__ void __launch_bounds__(kF4Threads, 1)
     __syncthreads();
     tc_fence_after();
 
-    const int r = (warp & 3) * 32 + lane, qq = warp >> 2;
+    const int r = (warp & 3) * 32 + lane, hf = warp >> 2;
     uint32_t hph = 0u, q = 0;
     bool jready = false;
-    uint32_t iph = 0u;                     // MMA thread: completed "fields set" phases
     const bool prof = P.prof != nullptr;
-    long long pa = 0, pb = 0, pc = 0, pd = 0;   // phase cycle totals; meaning depends on the warp's role
+    long long pa = 0, pb = 0, pc = 0, pd = 0, pe = 0;   // phase cycle totals; meaning depends on the warp's role
+    long long p_f0 = 0, p_f7 = 0, p_s0 = 0, p_s7 = 0;   // decision thread 0: marks after its own publish
     const long long t_loop0 = clock64();
 
-    for (int g = gs0; g < P.ngroups; g += gstride) {
-        if (warp < kDW) {
+    for (int g = gs0, gi = 0; g < P.ngroups; g += gstride, ++gi) {
+        const uint32_t tbase = uint32_t(gi) * uint32_t(S + 2);   // this group's offset in the flag mirror
+        if (warp < kF4DW) {
             // ---------------- decision warps ----------------
             const int chain = g * kM + r;
             const bool writer = chain < P.nchains;
-            Xoshiro rng[4];
-            uint32_t sw = 0u, dw = 0u, vmask = 0u, nlacc_prev = 0u;
-            int32_t nlin_prev = 0;
+            uint32_t sw[2] = {0u, 0u}, dw[2] = {0u, 0u}, vmask[2] = {0u, 0u};
             long long flips = 0;
-            {
-                uint32_t db[4] = {0u, 0u, 0u, 0u};
+            F4ExMarks mk{};
+            const uint32_t trng = tmem + tl + uint32_t(kF4RngCol + 32 * hf);
+            // initial spins from each lane's first draw per round, the state D = s0 (parity 1), the lane states and
+            // the fields h = b; once per group, so not unrolled over the two quarters
+#pragma unroll 1
+            for (int e = 0; e < 2; ++e) {
+                const int qq = 2 * hf + e;
+                Xoshiro rng[4];
+                uint32_t db[4] = {0u, 0u, 0u, 0u}, swq = 0u, dwq = 0u, vmq = 0u;
 #pragma unroll
                 for (int j = 0; j < 4; ++j) rng_seed(rng[j], P.seed, P.trial_offset + uint32_t(chain), uint32_t(16 * cs + 4 * qq + j));
 #pragma unroll
@@ -960,79 +1149,89 @@ __global__ void __launch_bounds__(kF4Threads, 1)
                         const uint32_t rv = rng_next(rng[j]);
                         const bool valid = i < n;
                         const uint32_t up = valid ? (rv >> 31) : 1u;
-                        sw |= up << col;
-                        if (valid) vmask |= 1u << col;
-                        if (valid && !up) dw |= 1u << col;
+                        swq |= up << col;
+                        if (valid) vmq |= 1u << col;
+                        if (valid && !up) dwq |= 1u << col;
                         db[col >> 3] |= (valid ? (up ? 0x2u : 0xAu) : 0u) << (4 * (col & 7));   // e2m1 +1 / -1
                     }
-                uint8_t* drow = P.dbuf + ((size_t(g) * 2 + 1) * kM + r) * ROWB + cs * 64 + qq * 16;
+                if (e == 0) { sw[0] = swq; dw[0] = dwq; vmask[0] = vmq; }
+                else { sw[1] = swq; dw[1] = dwq; vmask[1] = vmq; }
+                uint8_t* drow = P.dbuf + ((size_t(g) * 2 + 1) * kM + r) * 1024 + cs * 64 + qq * 16;
                 *reinterpret_cast<uint4*>(drow) = make_uint4(db[0], db[1], db[2], db[3]);
-                P.nlx[((size_t(g) * 2 + 1) * kM + r) * 128 + cs * 4 + qq] = 0;
-                uint32_t v[16];
+                uint32_t st[16];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    st[4 * j] = rng[j].a;
+                    st[4 * j + 1] = rng[j].b;
+                    st[4 * j + 2] = rng[j].c;
+                    st[4 * j + 3] = rng[j].d;
+                }
+                tmem_st16(trng + uint32_t(16 * e), st);
 #pragma unroll
                 for (int h2 = 0; h2 < 2; ++h2) {
 #pragma unroll
-                    for (int e = 0; e < 16; ++e)
-                        v[e] = __float_as_uint(P.bias_perm ? float(P.bias_perm[cs * kF4YS + qq * 32 + h2 * 16 + e]) : 0.f);
-                    tmem_st16(tmem + tl + uint32_t(qq * 32 + h2 * 16), v);
-                }
-                if (qq == 0) {
-#pragma unroll
-                    for (int e = 0; e < 16; ++e) v[e] = 0u;
-                    tmem_st16(tmem + tl + 128u, v);
+                    for (int x = 0; x < 16; ++x)
+                        st[x] = __float_as_uint(P.bias_perm ? float(P.bias_perm[cs * kF4YS + qq * 32 + h2 * 16 + x]) : 0.f);
+                    tmem_st16(tmem + tl + uint32_t(qq * 32 + h2 * 16), st);
                 }
                 tmem_wait_st();
             }
-            writer_fence();
+            // the fields are set before any tile of this group is marked full, so before the MMA thread accumulates
             tc_fence_before();
-            asm volatile("bar.sync 1, %0;" ::"r"(kDW * 32) : "memory");
-            if (tid == 0) {
-                // the MMA thread may accumulate into these fields only after they are set: tiles of other slices
-                // can land before this CTA leaves its previous group
-                mbar_arrive(bar_init);
-                flag_release(P.flags + g * kF4Slices + cs, 1u);
-            }
+            asm volatile("bar.sync 1, %0;" ::"r"(kF4DW * 32) : "memory");
+            if (tid == 0) flag_release(P.flags + g * kF4Slices + cs, 1u);
+            uint32_t pk[32];
+            // the run's error word is read once per step, off the critical path (its load overlaps the draws);
+            // a wait of this warp that gives up clears ok at once
+            const bool eok = !err_set(err);
+            f4_draw(trng, pk);
+            bool ok = __all_sync(0xffffffffu, eok);
+            int32_t nlin_next = f4_exchange(P, g, -1, smem_u32(stages), bar_full, bar_empty, q, tid, r, false, s_flag, tbase,
+                                            ok, false, mk);
+            q += kF4Tiles;
             const float hclf = float(P.hclamp);
-            long long last_pub = 0, p_pub = 0, p_wake = 0;   // profiling (thread 0): publish cost, wake - publish
             for (int m = 0; m <= S; ++m) {
                 long long t0 = prof ? clock64() : 0;
                 // this step's table entries, loaded before the wait for the fields
                 const int t = m < S ? m : S - 1;
                 const int32_t fourT = __ldg(P.fourT + t), qv = __ldg(P.q + t), kconst = __ldg(P.kconst + t);
                 const int64_t kcorr = __ldg(P.kcorr + t);
-                if (!err_set(err)) mbar_wait(bar_h, hph & 1u, err, kErrHready);
+                if (ok) ok = __all_sync(0xffffffffu, mbar_wait(bar_h, hph & 1u, err, kErrHready));
                 ++hph;
                 tc_fence_after();
                 if (prof) {
                     const long long t1 = clock64();
                     pa += t1 - t0;
                     t0 = t1;
-                    if (m >= 1) p_wake += t1 - last_pub;
                 }
-                uint32_t hv[32], nv;
-                tmem_ld32(tmem + tl + uint32_t(qq * 32), hv);
-                asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];" : "=r"(nv) : "r"(tmem + tl + 128u));
-                tmem_wait_ld();
-                const int32_t nlin = int32_t(nv - nlacc_prev);
-                nlacc_prev = nv;
-                if (m >= 1 && writer && cs == 0 && qq == 0 && P.out_trace) P.out_trace[size_t(chain) * S + (m - 1)] = nlin;
-                nlin_prev = nlin;
+                const int32_t nlin_prev = nlin_next;       // n_lin of step m - 1 (0 before the first step)
+                if (m >= 1 && writer && cs == 0 && hf == 0 && P.out_trace) P.out_trace[size_t(chain) * S + (m - 1)] = nlin_prev;
                 if (m == S) {
+                    // read-out, once per group: 16-column chunks from TMEM, not unrolled
                     long long sh = 0, bs = 0;
+#pragma unroll 1
+                    for (int c4 = 0; c4 < 4; ++c4) {
+                        const int qq = 2 * hf + (c4 >> 1);
+                        const uint32_t swq = (c4 >> 1) ? sw[1] : sw[0];
+                        uint32_t hc[16];
+                        tmem_ld16(tmem + tl + uint32_t(hf * 64 + 16 * c4), hc);
+                        tmem_wait_ld();
 #pragma unroll
-                    for (int col = 0; col < 32; ++col) {
-                        const int j = col / R, k = col % R, i = k * 256 + 16 * cs + 4 * qq + j;
-                        if (i >= n) continue;
-                        const bool up = (sw >> col) & 1u;
-                        const int32_t h = __float2int_rn(__uint_as_float(hv[col]));
-                        sh += up ? h : -h;
-                        if (P.bias_perm) {
-                            const int32_t b = P.bias_perm[cs * kF4YS + qq * 32 + col];
-                            bs += up ? b : -b;
-                        }
-                        if (writer) {
-                            if (up) atomicOr(P.out_spins + size_t(chain) * 64 + (i >> 5), 1u << (i & 31));
-                            if (P.out_h) P.out_h[size_t(chain) * n + i] = h;
+                        for (int x = 0; x < 16; ++x) {
+                            const int col = (c4 & 1) * 16 + x;      // column within quarter qq
+                            const int j = col / R, k = col % R, i = k * 256 + 16 * cs + 4 * qq + j;
+                            if (i >= n) continue;
+                            const bool up = (swq >> col) & 1u;
+                            const int32_t h = __float2int_rn(__uint_as_float(hc[x]));
+                            sh += up ? h : -h;
+                            if (P.bias_perm) {
+                                const int32_t b = P.bias_perm[cs * kF4YS + qq * 32 + col];
+                                bs += up ? b : -b;
+                            }
+                            if (writer) {
+                                if (up) atomicOr(P.out_spins + size_t(chain) * 64 + (i >> 5), 1u << (i & 31));
+                                if (P.out_h) P.out_h[size_t(chain) * n + i] = h;
+                            }
                         }
                     }
                     if (writer) {
@@ -1046,111 +1245,64 @@ __global__ void __launch_bounds__(kF4Threads, 1)
                 const int32_t corr = step_corr(nlin_prev, kcorr, kconst);
                 const uint32_t lw = uint32_t(2 * twoT - 1);
                 const int32_t xs = qv - corr, c1 = twoT - 1, twocorr = 2 * corr;
-                const uint32_t downs = ~sw;           // bit set: s = -1, the field's sign flips
-                uint32_t fm, lm;                      // flip mask, linear-band mask
-                if (P.hclamp > 0) f4_decide<true>(rng, hv, downs, dw, xs, twocorr, fourT, c1, lw, hclf, fm, lm);
-                else f4_decide<false>(rng, hv, downs, dw, xs, twocorr, fourT, c1, lw, hclf, fm, lm);
-                fm &= vmask;
-                lm &= vmask;
-                const int nl = __popc(lm);
-                flips += __popc(fm);
-                // dS nibbles: flipped down->up = +2 (0x4), up->down = -2 (0xC); word w holds columns 8w .. 8w+7
-                const uint32_t fdn = fm & sw;
-                uint32_t db[4];
-#pragma unroll
-                for (int w = 0; w < 4; ++w) {
-                    uint32_t a8 = (fm >> (8 * w)) & 0xFFu, b8 = (fdn >> (8 * w)) & 0xFFu;
-                    a8 = (a8 | (a8 << 12)) & 0x000F000Fu; a8 = (a8 | (a8 << 6)) & 0x03030303u; a8 = (a8 | (a8 << 3)) & 0x11111111u;
-                    b8 = (b8 | (b8 << 12)) & 0x000F000Fu; b8 = (b8 | (b8 << 6)) & 0x03030303u; b8 = (b8 | (b8 << 3)) & 0x11111111u;
-                    db[w] = (a8 << 2) | (b8 << 3);
-                }
-                sw ^= fm;
-                dw = fm;
                 const int par = m & 1;
-                uint8_t* drow = P.dbuf + ((size_t(g) * 2 + par) * kM + r) * ROWB + cs * 64 + qq * 16;
-                *reinterpret_cast<uint4*>(drow) = make_uint4(db[0], db[1], db[2], db[3]);
-                P.nlx[((size_t(g) * 2 + par) * kM + r) * 128 + cs * 4 + qq] = int8_t(nl);
-                writer_fence();
+                uint4 dq[2];
+                uint32_t nlb = 0u;
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    uint32_t hv[32];                  // the quarter's fields
+                    tmem_ld32(tmem + tl + uint32_t(hf * 64 + 32 * e), hv);
+                    tmem_wait_ld();
+                    const uint32_t downs = ~sw[e];    // bit set: s = -1, the field's sign flips
+                    uint32_t fm, lm;                  // flip mask, linear-band mask
+                    if (e == 0) {
+                        if (P.hclamp > 0) f4_decide<true, 0>(pk, hv, downs, dw[0], xs, twocorr, fourT, c1, lw, hclf, fm, lm);
+                        else f4_decide<false, 0>(pk, hv, downs, dw[0], xs, twocorr, fourT, c1, lw, hclf, fm, lm);
+                    } else {
+                        if (P.hclamp > 0) f4_decide<true, 1>(pk, hv, downs, dw[1], xs, twocorr, fourT, c1, lw, hclf, fm, lm);
+                        else f4_decide<false, 1>(pk, hv, downs, dw[1], xs, twocorr, fourT, c1, lw, hclf, fm, lm);
+                    }
+                    fm &= vmask[e];
+                    lm &= vmask[e];
+                    nlb |= uint32_t(__popc(lm)) << (8 * e);
+                    flips += __popc(fm);
+                    dq[e] = f4_dnibbles(fm, fm & sw[e]);
+                    sw[e] ^= fm;
+                    dw[e] = fm;
+                }
+                uint8_t* drow = P.dbuf + ((size_t(g) * 2 + par) * kM + r) * 1024 + cs * 64 + hf * 32;
+                reinterpret_cast<uint4*>(drow)[0] = dq[0];
+                reinterpret_cast<uint4*>(drow)[1] = dq[1];
+                *reinterpret_cast<uint16_t*>(P.nlx + ((size_t(g) * 2 + par) * kM + r) * 128 + cs * 4 + hf * 2) = uint16_t(nlb);
                 tc_fence_before();
                 if (prof) { const long long t1 = clock64(); pb += t1 - t0; t0 = t1; }
-                asm volatile("bar.sync 1, %0;" ::"r"(kDW * 32) : "memory");
-                const long long tb = prof ? clock64() : 0;
+                asm volatile("bar.sync 1, %0;" ::"r"(kF4DW * 32) : "memory");
                 if (tid == 0) flag_release(P.flags + g * kF4Slices + cs, uint32_t(m + 2));
+                long long tpub = 0;
                 if (prof) {
-                    last_pub = clock64();
-                    pc += last_pub - t0;
-                    p_pub += last_pub - tb;
-                    if (tid == 0) s_pub[m & 1] = last_pub;
+                    tpub = clock64();
+                    pc += tpub - t0;
+                    t0 = tpub;
+                    if (tid == 0) s_pub[m & 1] = tpub;
+                }
+                // the next step's draws while the other slices publish; the run's error word is read here too
+                const bool eok2 = !err_set(err);
+                if (m + 1 < S) f4_draw(trng, pk);
+                ok = ok && __all_sync(0xffffffffu, eok2);
+                if (prof) { const long long t1 = clock64(); pd += t1 - t0; t0 = t1; }
+                nlin_next = f4_exchange(P, g, m, smem_u32(stages), bar_full, bar_empty, q, tid, r, true, s_flag, tbase,
+                                        ok, prof, mk);
+                q += kF4Tiles;
+                if (prof) {
+                    pe += clock64() - t0;
+                    tpub = s_pub[m & 1];            // thread 0's publish: the same barrier episode for every warp
+                    p_f0 += mk.flags0 - tpub;
+                    p_f7 += mk.flags7 - tpub;
+                    p_s0 += mk.stored0 - tpub;
+                    p_s7 += mk.stored7 - tpub;
                 }
             }
             tc_fence_before();
-            if (prof && tid == 0) {
-                long long* dst = P.prof + size_t(blockIdx.x) * kProfSlots;
-                dst[3] += p_pub;
-                dst[4] += p_wake;
-            }
-        } else if (warp < kDW + kF4PW) {
-            // ---------------- producer warps ----------------
-            const int pwid = warp - kDW;
-            const uint32_t* fl = P.flags + g * kF4Slices;
-            long long p_rdy = 0, p_iss = 0;      // profiling: flags seen / TMA issued after the own publish (tiles 0, 7)
-            for (int m = -1; m < S; ++m) {
-                const int ay = (g * 2 + (m & 1)) * kM;
-                const uint32_t target = uint32_t(m + 2);
-                uint32_t ready = 0u;
-                for (int c = 0; c < kF4Chunks; ++c, ++q) {
-                    if (int(q % kF4PW) != pwid) continue;
-                    if (__shfl_sync(0xffffffffu, err_set(err) ? 1 : 0, 0)) continue;
-                    const int s = int(q % kF4Stages);
-                    const uint32_t u = q / kF4Stages;
-                    const long long w0 = prof ? clock64() : 0;
-                    if (u >= 1) {
-                        const int w = lane == 0 ? (mbar_wait(bar_empty + 8 * s, (u - 1) & 1u, err, kErrEmpty) ? 1 : 0) : 1;
-                        if (!__shfl_sync(0xffffffffu, w, 0)) continue;
-                    }
-                    const uint32_t need = c < 8 ? (3u << (2 * c)) : 0xffffu;
-                    bool ok = (ready & need) == need;
-                    if (!ok) {
-                        const uint64_t t0 = globaltimer();
-                        for (uint32_t k = 1;; ++k) {
-                            uint32_t v = 0xffffffffu;
-                            if (lane < kF4Slices)
-                                asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(fl + lane) : "memory");
-                            ready = __ballot_sync(0xffffffffu, v >= target);
-                            if ((ready & need) == need) { ok = true; break; }
-                            if ((k & 63u) == 0 && __shfl_sync(0xffffffffu, globaltimer() - t0 > kWaitNs, 0)) {
-                                if (lane == 0) atomicCAS(err, 0, kErrFlag);
-                                break;
-                            }
-                        }
-                        // acquire: relaxed reads that saw the release stores, then a fence; __syncwarp orders every
-                        // lane's acquire before lane 0's copy
-                        asm volatile("fence.acq_rel.gpu;" ::: "memory");
-                        __syncwarp();
-                    }
-                    const long long w1 = prof ? clock64() : 0;
-                    if (prof) pa += w1 - w0;
-                    if (!ok) continue;
-                    if (lane == 0) {
-                        asm volatile("fence.proxy.async.global;" ::: "memory");
-                        const uint32_t dst = smem_u32(stages + size_t(s) * TILE);
-                        mbar_arrive_expect_tx(bar_full + 8 * s, TILE);
-                        if (c < 8) tma_load_2d(dst, &mapD, c * kKChunk, ay, bar_full + 8 * s);
-                        else tma_load_2d(dst, &mapNL, 0, ay, bar_full + 8 * s);
-                        if (prof && m >= 0 && (c == 0 || c == 7)) {
-                            const long long pub = s_pub[m & 1];
-                            p_rdy += w1 - pub;
-                            p_iss += clock64() - pub;
-                        }
-                    }
-                    __syncwarp();
-                }
-            }
-            if (prof && lane == 0 && (pwid == 0 || pwid == 7 % kF4PW)) {
-                long long* dst = P.prof + size_t(blockIdx.x) * kProfSlots;
-                dst[pwid == 0 ? 15 : 16] += p_rdy;
-                dst[pwid == 0 ? 17 : 18] += p_iss;
-            }
         } else if (warp == kF4MmaWarp) {
             // ---------------- MMA thread ----------------
             if (lane == 0) {
@@ -1158,44 +1310,45 @@ __global__ void __launch_bounds__(kF4Threads, 1)
                     if (!err_set(err)) mbar_wait(bar_j, 0u, err, kErrJ);
                     jready = true;
                 }
-                if (!err_set(err)) mbar_wait(bar_init, iph & 1u, err, kErrInit);
-                ++iph;
-                tc_fence_after();
-                long long p_first = 0, p_last = 0, p_nl = 0, p_h = 0, tf0 = 0, tf7 = 0, tf8 = 0;
+                long long p_first = 0, p_last = 0, p_h = 0, tf0 = 0, tf7 = 0, pmid[5] = {0, 0, 0, 0, 0}, pti[8] = {}, ptw[8] = {};
+                bool mok = true;           // false once a wait gave up or the error word was seen set
                 for (int m = -1; m < S; ++m) {
                     const long long t0 = prof ? clock64() : 0;
-                    for (int c = 0; c < kF4Chunks; ++c, ++q) {
+                    mok = mok && !err_set(err);    // once per step, while the thread waits for the first tile
+                    for (int t = 0; t < kF4Tiles; ++t, ++q) {
                         const int s = int(q % kF4Stages);
                         const uint32_t u = q / kF4Stages;
                         const long long w0 = prof ? clock64() : 0;
-                        const bool ok = !err_set(err) && mbar_wait(bar_full + 8 * s, u & 1u, err, kErrFull);
+                        mok = mok && mbar_wait(bar_full + 8 * s, u & 1u, err, kErrFull);
+                        const bool ok = mok;
                         if (prof) {
                             const long long w1 = clock64();
                             pa += w1 - w0;
-                            if (c == 0) tf0 = w1;
-                            if (c == 7) tf7 = w1;
-                            if (c == 8) tf8 = w1;
+                            if (t == 0) tf0 = w1;
+                            if (t == kF4Tiles - 1) tf7 = w1;
+                            if (t >= 2 && t <= 6 && m >= 0) pmid[t - 2] += w1 - s_pub[m & 1];
                         }
                         tc_fence_after();
                         const long long i0 = prof ? clock64() : 0;
                         if (ok) {
                             const uint32_t a0 = smem_u32(stages + size_t(s) * TILE);
-                            if (c < 8) {
-                                const uint32_t b0 = smem_u32(jres + c * TILE);
+                            const uint32_t b0 = smem_u32(jres + t * TILE);
 #pragma unroll
-                                for (int kk = 0; kk < kKChunk / 32; ++kk)
-                                    mma_mxf4(tmem, sw128_desc(a0 + 32 * kk), sw128_desc(b0 + 32 * kk), IDESC_F4,
-                                             tmem + uint32_t(kF4SfCol), tmem + uint32_t(kF4SfCol + 32));
-                            } else {
-                                const uint32_t b0 = smem_u32(ones);
-#pragma unroll
-                                for (int kk = 0; kk < 2; ++kk)
-                                    mma_i8(tmem + 128u, sw128_desc(a0 + 32 * kk), sw128_desc(b0 + 32 * kk), IDESC_NL, 1u);
-                            }
+                            for (int kk = 0; kk < kKChunk / 32; ++kk)
+                                mma_mxf4(tmem, sw128_desc(a0 + 32 * kk), sw128_desc(b0 + 32 * kk), IDESC_F4,
+                                         tmem + uint32_t(kF4SfCol), tmem + uint32_t(kF4SfCol + 32));
                         }
                         const long long i1 = prof ? clock64() : 0;
                         mma_commit(bar_empty + 8 * s);
-                        if (prof) { const long long i2 = clock64(); pc += i1 - i0; pd += i2 - i1; }
+                        if (prof) {
+                            const long long i2 = clock64();
+                            pc += i1 - i0;
+                            pd += i2 - i1;
+                            if (m >= 0) {
+                                pti[t] += i1 - s_pub[m & 1];
+                                ptw[t] += i0 - w0;
+                            }
+                        }
                     }
                     mma_commit(bar_h);
                     if (prof) {
@@ -1205,7 +1358,6 @@ __global__ void __launch_bounds__(kF4Threads, 1)
                             const long long pub = s_pub[m & 1];
                             p_first += tf0 - pub;
                             p_last += tf7 - pub;
-                            p_nl += tf8 - pub;
                             p_h += th - pub;
                         }
                     }
@@ -1214,29 +1366,78 @@ __global__ void __launch_bounds__(kF4Threads, 1)
                     long long* dst = P.prof + size_t(blockIdx.x) * kProfSlots;
                     dst[11] += p_first;
                     dst[12] += p_last;
-                    dst[13] += p_nl;
                     dst[14] += p_h;
+                    for (int i = 0; i < 5; ++i) dst[19 + i] += pmid[i];
+                    for (int i = 0; i < 8; ++i) {
+                        dst[40 + i] += pti[i];
+                        dst[48 + i] += ptw[i];
+                    }
                 }
             } else {
-                q += uint32_t(S + 1) * kF4Chunks;
+                q += uint32_t(S + 1) * kF4Tiles;
             }
             __syncwarp();
+        } else if (warp == kF4PollWarp) {
+            // ---------------- flag poller ----------------
+            // lane j < 16 watches slice j's flag (values 1 .. S + 1 for steps -1 .. S - 1) with relaxed gpu-scope
+            // loads; whatever the warp newly sees it acquires (fence) and releases to the CTA through s_flag, so
+            // the decision warps wait on shared memory, not L2
+            const uint32_t* fl = P.flags + g * kF4Slices;
+            uint32_t seen = 0u;
+            bool pok = !err_set(err);
+            for (uint32_t target = 1; pok && target <= uint32_t(S + 1); ++target) {
+                const uint64_t t0 = globaltimer();
+                for (uint32_t k = 1;; ++k) {
+                    uint32_t v = 0u;
+                    if (lane < kF4Slices)
+                        asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(fl + lane) : "memory");
+                    const bool fresh = lane < kF4Slices && v > seen;
+                    if (__any_sync(0xffffffffu, fresh)) {
+                        asm volatile("fence.acq_rel.gpu;" ::: "memory");
+                        if (fresh) {
+                            asm volatile("st.release.cta.shared::cta.u32 [%0], %1;" ::"r"(smem_u32(s_flag + lane)),
+                                         "r"(tbase + v)
+                                         : "memory");
+                            seen = v;
+                        }
+                    }
+                    if (__all_sync(0xffffffffu, lane >= kF4Slices || seen >= target)) break;
+                    if ((k & 63u) == 0) {
+                        const bool late = lane == 0 && globaltimer() - t0 > kWaitNs;
+                        if (late) atomicCAS(err, 0, kErrFlag);
+                        if (__shfl_sync(0xffffffffu, (late || (lane == 0 && err_set(err))) ? 1 : 0, 0)) {
+                            pok = false;
+                            break;
+                        }
+                    }
+                }
+            }
         }
+    }
+    if (warp == kF4MmaWarp && lane == 0) {
+        // drain: every MMA issued has completed (and the J copy has landed) before TMEM and shared memory go away
+        if (!jready) mbar_wait_for(bar_j, 0u, nullptr, 0, kWaitNs);
+        mma_commit(bar_fin);
+        mbar_wait_for(bar_fin, 0u, nullptr, 0, kWaitNs);
     }
     if (prof) {
         long long* dst = P.prof + size_t(blockIdx.x) * kProfSlots;
-        if (warp == 0 && lane == 0) {
-            dst[0] = pa; dst[1] = pb; dst[2] = pc;
+        if (tid == 0) {
+            dst[0] = pa; dst[1] = pb; dst[2] = pc; dst[3] = pd; dst[4] = pe;
+            dst[15] = p_f0; dst[16] = p_f7; dst[17] = p_s0; dst[18] = p_s7;
+        }
+        if (warp < kF4DW && lane == 0) {
+            dst[24 + warp] = p_s7;
+            dst[32 + warp] = p_f7;
         }
         if (warp == kF4MmaWarp && lane == 0) {
             dst[5] = pa; dst[6] = pb; dst[8] = clock64() - t_loop0; dst[9] = pc; dst[10] = pd;
         }
-        if (warp == kDW && lane == 0) dst[7] = pa;
     }
     __syncthreads();
     if (warp == kF4MmaWarp) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kF4TmemCols) : "memory");
     }
 }
 
@@ -1452,7 +1653,7 @@ int ensure_bias_perm(TensorInstance* ti, const int32_t* bias, std::string* why) 
 }
 
 size_t f4_smem_bytes() {
-    return 1024 + 8 * size_t(kM) * kKChunk + 2048 + size_t(kF4Stages) * kM * kKChunk + (2 * kF4Stages + 3) * 8 + 16;
+    return 1024 + 8 * size_t(kM) * kKChunk + size_t(kF4Stages) * kM * kKChunk + kF4Bars * 8 + 16;
 }
 
 // Concurrent group slots of the fp4 kernel (16 co-resident CTAs each).
@@ -1514,9 +1715,8 @@ int f4_run(TensorInstance* ti, const TensorRun& r, cudaStream_t st, std::string*
     uint32_t* flags = reinterpret_cast<uint32_t*>(base + 256);
     uint8_t* dbuf = base + 256 + fbytes;
     int8_t* nlx = reinterpret_cast<int8_t*>(dbuf + dbytes);
-    CUtensorMap mapD, mapNL, mapJ;
-    if (!make_map(&mapD, dbuf, 1024, uint64_t(ngroups) * 2 * kM, kM) ||
-        !make_map(&mapNL, nlx, 128, uint64_t(ngroups) * 2 * kM, kM) || !make_map(&mapJ, ti->d_J4, 1024, 2048, kF4YS)) {
+    CUtensorMap mapJ;
+    if (!make_map(&mapJ, ti->d_J4, 1024, 2048, kF4YS)) {
         if (why) *why = "cuTensorMapEncodeTiled failed";
         return -2;
     }
@@ -1525,7 +1725,6 @@ int f4_run(TensorInstance* ti, const TensorRun& r, cudaStream_t st, std::string*
     if (e == cudaSuccess) e = cudaMemsetAsync(r.out_sum_bs, 0, size_t(r.nchains) * 8, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(r.out_flips, 0, size_t(r.nchains) * 8, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(base, 0, 256 + fbytes, st);     // error word + flags
-    if (e == cudaSuccess) e = cudaMemsetAsync(nlx, 0, nbytes, st);            // partial bytes 64..127 stay zero
     if (e != cudaSuccess) {
         if (why) *why = std::string("memset: ") + cudaGetErrorString(e);
         return -2;
@@ -1571,7 +1770,7 @@ int f4_run(TensorInstance* ti, const TensorRun& r, cudaStream_t st, std::string*
     cfg.blockDim = dim3(kF4Threads);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = st;
-    if (e == cudaSuccess) e = cudaLaunchKernelEx(&cfg, fn, mapD, mapNL, mapJ, P);
+    if (e == cudaSuccess) e = cudaLaunchKernelEx(&cfg, fn, mapJ, P);
     if (e != cudaSuccess) {
         if (why) *why = std::string("launch: ") + cudaGetErrorString(e);
         return -2;
