@@ -437,7 +437,7 @@ constexpr int kResStages = 5;
 constexpr int kResMmaWarp = kDW + kResPW;
 constexpr int kResThreads = (kDW + kResPW + 1) * 32;
 constexpr int kResChunks = 17;            // 16 D chunks + 1 n_lin chunk per (step, group)
-constexpr int kErrFlag = 4, kErrJ = 5, kErrInit = 6;
+constexpr int kErrFlag = 4, kErrJ = 5, kErrInit = 6, kErrRead = 7;
 
 struct ResParams {
     int n, S, npairs;
@@ -478,8 +478,8 @@ __global__ void __launch_bounds__(kResThreads, 1)
     uint8_t* ones = smem + 16 * JCHUNK;                     // 2 KB: row 0 = 128 x int8(1), rows 1..15 = 0
     uint8_t* stages = ones + 2048;                          // kResStages x 16 KB (1024-aligned)
     uint64_t* bars = reinterpret_cast<uint64_t*>(stages + kResStages * TILE);
-    // bars: full[5], empty[5], hready[2], jbar
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kResStages + 4);   // bars: ... jbar, init
+    // bars: full[5], empty[5], hready[2], jbar, init, fields read[2]
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kResStages + 6);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int cs = int(blockIdx.x % kResSlices);
@@ -489,6 +489,9 @@ __global__ void __launch_bounds__(kResThreads, 1)
     const uint32_t bar_full = smem_u32(bars), bar_empty = smem_u32(bars + kResStages);
     const uint32_t bar_h0 = smem_u32(bars + 2 * kResStages), bar_j = smem_u32(bars + 2 * kResStages + 2);
     const uint32_t bar_init = smem_u32(bars + 2 * kResStages + 3);   // decision warps: fields of a new pair set
+    // decision warps: group g's fields for step m have been read, so its step-m tiles may now be accumulated (other
+    // slices can publish step m before this CTA has read the fields it decides step m from)
+    const uint32_t bar_rd0 = smem_u32(bars + 2 * kResStages + 4);
 
     if (tid == 0) {
         for (int s = 0; s < kResStages; ++s) {
@@ -497,6 +500,8 @@ __global__ void __launch_bounds__(kResThreads, 1)
         }
         mbar_init(bar_h0, 1);
         mbar_init(bar_h0 + 8, 1);
+        mbar_init(bar_rd0, 1);
+        mbar_init(bar_rd0 + 8, 1);
         mbar_init(bar_j, 1);
         mbar_init(bar_init, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -526,6 +531,7 @@ __global__ void __launch_bounds__(kResThreads, 1)
     uint32_t q = 0;                        // running chunk index (producers, MMA)
     bool jready = false;
     uint32_t iph = 0u;                     // MMA thread: completed "fields set" phases
+    uint32_t rph[2] = {0u, 0u};            // MMA thread: completed "fields read" phases per group
     const bool prof = P.prof != nullptr;
     long long pr[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     const long long t_loop0 = clock64();
@@ -668,7 +674,10 @@ __global__ void __launch_bounds__(kResThreads, 1)
                     tc_fence_before();
                     if (prof) { const long long t1 = clock64(); pr[1] += t1 - t0; t0 = t1; }
                     asm volatile("bar.sync 1, %0;" ::"r"(kDW * 32) : "memory");
-                    if (tid == 0) flag_publish(P.flags + G[g] * kResSlices + cs, uint32_t(m + 2));
+                    if (tid == 0) {
+                        mbar_arrive(bar_rd0 + 8 * g);
+                        flag_publish(P.flags + G[g] * kResSlices + cs, uint32_t(m + 2));
+                    }
                     if (prof) pr[2] += clock64() - t0;
                 }
             }
@@ -736,6 +745,11 @@ __global__ void __launch_bounds__(kResThreads, 1)
                 for (int m = -1; m < S; ++m) {
                     for (int g = 0; g < 2; ++g) {
                         const long long t0 = prof ? clock64() : 0;
+                        if (m >= 0) {
+                            if (!err_set(err)) mbar_wait(bar_rd0 + 8 * g, rph[g] & 1u, err, kErrRead);
+                            ++rph[g];
+                            tc_fence_after();
+                        }
                         for (int c = 0; c < kResChunks; ++c, ++q) {
                             const int s = int(q % kResStages);
                             const uint32_t u = q / kResStages;
@@ -1506,7 +1520,7 @@ int max_clusters_t(int* out) {
 }
 
 size_t res_smem_bytes() {
-    return 1024 + 16 * size_t(kResYS) * kKChunk + 2048 + size_t(kResStages) * kM * kKChunk + (2 * kResStages + 4) * 8 + 16;
+    return 1024 + 16 * size_t(kResYS) * kKChunk + 2048 + size_t(kResStages) * kM * kKChunk + (2 * kResStages + 6) * 8 + 16;
 }
 
 // Concurrent pair slots of the resident kernel (32 co-resident CTAs each).

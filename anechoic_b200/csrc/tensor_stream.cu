@@ -39,7 +39,7 @@ constexpr int kSStages = 4;
 constexpr uint32_t kSTile = 128 * 128;     // 16 KB
 constexpr uint32_t kSStage = 3 * kSTile;   // J tile + two dS tiles
 constexpr int kSChunks = kSSlices + 2;     // dS chunks + 2 n_lin chunks per step
-constexpr int kErrFull = 1, kErrEmpty = 2, kErrHready = 3, kErrFlag = 4, kErrInit = 6;
+constexpr int kErrFull = 1, kErrEmpty = 2, kErrHready = 3, kErrFlag = 4, kErrInit = 6, kErrRead = 7;
 
 struct StreamParams {
     int n, R, S;
@@ -75,8 +75,8 @@ __global__ void __launch_bounds__(kSThreads, 1)
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t* stages = smem;                                 // kSStages x (J, dS0, dS1)
     uint8_t* ones = stages + kSStages * kSStage;            // 2 KB: row 0 = 128 x int8(1)
-    uint64_t* bars = reinterpret_cast<uint64_t*>(ones + 2048);   // full[4], empty[4], hready, init
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kSStages + 2);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(ones + 2048);   // full[4], empty[4], hready, init, fields read
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kSStages + 3);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int cs = int(blockIdx.x);
@@ -85,6 +85,9 @@ __global__ void __launch_bounds__(kSThreads, 1)
     const uint32_t bar_full = smem_u32(bars), bar_empty = smem_u32(bars + kSStages);
     const uint32_t bar_h = smem_u32(bars + 2 * kSStages);
     const uint32_t bar_init = smem_u32(bars + 2 * kSStages + 1);   // decision warps: fields of a new pair set
+    // decision warps: the fields of step m have been read, so step m's tiles may now be accumulated (other slices
+    // can publish step m before this CTA has read the fields it decides step m from)
+    const uint32_t bar_rd = smem_u32(bars + 2 * kSStages + 2);
 
     if (tid == 0) {
         for (int s = 0; s < kSStages; ++s) {
@@ -93,6 +96,7 @@ __global__ void __launch_bounds__(kSThreads, 1)
         }
         mbar_init(bar_h, 1);
         mbar_init(bar_init, 1);
+        mbar_init(bar_rd, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     for (int i = tid; i < 2048; i += blockDim.x) ones[i] = i < 128 ? 1 : 0;
@@ -112,7 +116,7 @@ __global__ void __launch_bounds__(kSThreads, 1)
     const bool prof = P.prof != nullptr;
     long long pa = 0, pb = 0, pc = 0;
     const long long t_loop0 = clock64();
-    uint32_t hph = 0u, q = 0u;
+    uint32_t hph = 0u, q = 0u, rph = 0u;
 
     for (int pr = 0; pr < P.npairs; ++pr) {
         if (warp < kSDW) {
@@ -282,10 +286,12 @@ __global__ void __launch_bounds__(kSThreads, 1)
                 tc_fence_before();
                 if (prof) { const long long t1 = clock64(); pb += t1 - t0; t0 = t1; }
                 asm volatile("bar.sync 1, %0;" ::"r"(kSDW * 32) : "memory");
-                if (tid == 0)
+                if (tid == 0) {
+                    mbar_arrive(bar_rd);
                     asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(P.flags + pr * kSSlices + cs),
                                  "r"(uint32_t(m + 2))
                                  : "memory");
+                }
                 if (prof) pc += clock64() - t0;
             }
             tc_fence_before();
@@ -358,6 +364,11 @@ __global__ void __launch_bounds__(kSThreads, 1)
                 tc_fence_after();
                 for (int m = -1; m < S; ++m) {
                     const long long t0 = prof ? clock64() : 0;
+                    if (m >= 0) {
+                        if (!err_set(err)) mbar_wait(bar_rd, rph & 1u, err, kErrRead);
+                        ++rph;
+                        tc_fence_after();
+                    }
                     for (int c = 0; c < kSChunks; ++c, ++q) {
                         const int s = int(q % kSStages);
                         const uint32_t u = q / kSStages;
@@ -410,7 +421,7 @@ __global__ void __launch_bounds__(kSThreads, 1)
     }
 }
 
-size_t stream_smem_bytes() { return 1024 + size_t(kSStages) * kSStage + 2048 + (2 * kSStages + 2) * 8 + 16; }
+size_t stream_smem_bytes() { return 1024 + size_t(kSStages) * kSStage + 2048 + (2 * kSStages + 3) * 8 + 16; }
 
 }  // namespace
 
