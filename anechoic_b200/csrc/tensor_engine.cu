@@ -837,7 +837,7 @@ constexpr int kF4Tiles = 8;               // D tiles per step (2048 fp4 = 1024 b
 constexpr int kF4MmaWarp = kF4DW;
 constexpr int kF4PollWarp = kF4DW + 1;   // watches the group's 16 slice flags for the whole CTA
 constexpr int kF4Threads = (kF4DW + 2) * 32;
-constexpr int kF4Cluster = 4;            // CTAs per cluster: a quarter of a replica group on one GPC
+constexpr int kF4Cluster = 1;            // CTAs per cluster (1: the scheduler spreads a group's slices; 4 GPC-local measured slower)
 constexpr int kF4SfCol = 160;             // TMEM columns 144..255 hold scale factors 0x7F (1.0)
 constexpr int kF4RngCol = 256;            // TMEM columns 256..319: RNG lane states, 32 per half hf
 constexpr int kF4TmemCols = 512;
@@ -1262,19 +1262,20 @@ __global__ void __launch_bounds__(kF4Threads, 1)
                 const int par = m & 1;
                 uint4 dq[2];
                 uint32_t nlb = 0u;
+                uint32_t hv0[32], hv1[32];            // the two quarters' fields, loaded together
+                tmem_ld32(tmem + tl + uint32_t(hf * 64), hv0);
+                tmem_ld32(tmem + tl + uint32_t(hf * 64 + 32), hv1);
+                tmem_wait_ld();
 #pragma unroll
                 for (int e = 0; e < 2; ++e) {
-                    uint32_t hv[32];                  // the quarter's fields
-                    tmem_ld32(tmem + tl + uint32_t(hf * 64 + 32 * e), hv);
-                    tmem_wait_ld();
                     const uint32_t downs = ~sw[e];    // bit set: s = -1, the field's sign flips
                     uint32_t fm, lm;                  // flip mask, linear-band mask
                     if (e == 0) {
-                        if (P.hclamp > 0) f4_decide<true, 0>(pk, hv, downs, dw[0], xs, twocorr, fourT, c1, lw, hclf, fm, lm);
-                        else f4_decide<false, 0>(pk, hv, downs, dw[0], xs, twocorr, fourT, c1, lw, hclf, fm, lm);
+                        if (P.hclamp > 0) f4_decide<true, 0>(pk, hv0, downs, dw[0], xs, twocorr, fourT, c1, lw, hclf, fm, lm);
+                        else f4_decide<false, 0>(pk, hv0, downs, dw[0], xs, twocorr, fourT, c1, lw, hclf, fm, lm);
                     } else {
-                        if (P.hclamp > 0) f4_decide<true, 1>(pk, hv, downs, dw[1], xs, twocorr, fourT, c1, lw, hclf, fm, lm);
-                        else f4_decide<false, 1>(pk, hv, downs, dw[1], xs, twocorr, fourT, c1, lw, hclf, fm, lm);
+                        if (P.hclamp > 0) f4_decide<true, 1>(pk, hv1, downs, dw[1], xs, twocorr, fourT, c1, lw, hclf, fm, lm);
+                        else f4_decide<false, 1>(pk, hv1, downs, dw[1], xs, twocorr, fourT, c1, lw, hclf, fm, lm);
                     }
                     fm &= vmask[e];
                     lm &= vmask[e];
