@@ -6,10 +6,12 @@ so check_ref-style replays and the estimators (anechoic_b200.analyze) read them 
         --output PREFIX [--chains B] [--batches NB] [--seed S] [--offset O] [--trace 0|1]
         [--steps S --t0 T0 --t1 T1 --q Q --lambda L --tec-jv JV --tecT KAPPA --ramp]
         [--target CUT | --target-energy E] [--wide auto|0|1] [--check-fields 0|1] [--engine auto|plain|tensor]
-        [--info]
+        [--warmup W] [--info]
 
-The reference's kernel-geometry flags (--cs, --groups, --clusters, --warmup, --burn, --r, --preg) are accepted and
-recorded; the engines here pick their own geometry. Success: cut >= --target (b = 0; default 33000 for a --graph
+The reference's kernel-geometry flags (--cs, --groups, --clusters, --burn, --r, --preg) are accepted and recorded;
+the engines here pick their own geometry. --warmup W (default 1) runs W untimed launches first, on trial ids
+0xF0000000 + 65536 i far outside any cohort, with results discarded, as the reference CLIs do
+(sca_gpu.cu:712-713), so batch 0 is timed like the rest. Success: cut >= --target (b = 0; default 33000 for a --graph
 instance without bias, the reference's K2000 target) or energy <= --target-energy.
 
 Files (PREFIX = --output):
@@ -32,13 +34,13 @@ from . import _lib, analyze
 from .engine import DeviceInstance, Schedule, Tables, parse_schedule_flag, run, tdiv
 from .instances import load, read_bias
 
-GEOMETRY_FLAGS = ("--cs", "--groups", "--clusters", "--warmup", "--burn", "--r", "--preg")
+GEOMETRY_FLAGS = ("--cs", "--groups", "--clusters", "--burn", "--r", "--preg")
 
 
 def parse(argv):
     o = dict(jkind=None, jpath=None, bias=None, kbits=0, output=None, chains=1024, batches=1, seed=20261004, offset=0,
              trace=0, target=None, target_energy=None, wide="auto", check_fields=0, engine="auto", info=False,
-             geometry={})
+             warmup=1, geometry={})
     sc = Schedule()
     a = 0
     while a < len(argv):
@@ -62,7 +64,7 @@ def parse(argv):
             o["kbits"] = int(v)
         elif k == "--output":
             o["output"] = v
-        elif k in ("--chains", "--batches", "--trace", "--check-fields"):
+        elif k in ("--chains", "--batches", "--trace", "--check-fields", "--warmup"):
             o[k[2:].replace("-", "_")] = int(v)
         elif k == "--seed":
             o["seed"] = int(v)
@@ -120,6 +122,8 @@ def main(argv=None) -> int:
         succ = batch_succ = mism = fmis_total = 0
         dms, hms = [], []
         kernel = None
+        for i in range(max(0, o["warmup"])):
+            run(dev, tb, o["seed"], 0xF0000000 + 65536 * i, B, engine=o["engine"], wide=wide)
         with open(out + ".trials.jsonl", "w") as ftr, open(out + ".batches.jsonl", "w") as fb, \
                 open(out + ".spins.bin", "wb") as fsp, (open(out + ".trace.bin", "wb") if o["trace"] else _Null()) as ftc:
             for b in range(nb):
@@ -167,6 +171,7 @@ def main(argv=None) -> int:
         t = sum(dms) / nb
         p, Pb = succ / (B * nb), batch_succ / nb
         summary = dict(device=_device_name(), n=inst.n, engine=o["engine"], kernel=kernel, geometry=o["geometry"],
+                       warmup=o["warmup"],
                        chains=B, batches=nb, seed=o["seed"], trial_offset=o["offset"], steps=sc.S, t0=sc.t0, t1=sc.t1,
                        q=sc.q, **{"lambda": sc.lam}, ramp=sc.ramp, tec_jv=sc.jv, tecT_kappa=sc.kappa, trace=o["trace"],
                        target=target, target_energy=target_e, successes=succ, trials=B * nb, p=p,
