@@ -13,9 +13,9 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG, "libanechoic.so")
 
 ANC_OK, ANC_EINVAL, ANC_ECUDA, ANC_ETIMEOUT, ANC_EMISMATCH = 0, -1, -2, -3, -4
-ENGINES = {"auto": 0, "plain": 1, "tensor": 2}
+ENGINES = {"auto": 0, "plain": 1, "tensor": 2, "cluster": 3}
 TENSOR_KINDS = {"auto": 0, "int8": 1, "fp4": 2}
-KERNELS = {0: None, 1: "plain", 2: "tensor-int8", 3: "tensor-fp4"}
+KERNELS = {0: None, 1: "plain", 2: "tensor-int8", 3: "tensor-fp4", 4: "plain-cluster"}
 
 EXPORTS = ("anc_instance_create", "anc_instance_create_csr", "anc_instance_get_info", "anc_instance_destroy",
            "anc_tables_create", "anc_tables_from_schedule", "anc_tables_steps", "anc_tables_read", "anc_tables_destroy",
@@ -132,7 +132,8 @@ PROFILE_FIELDS = ("wait_fields", "decide", "publish", "draw", "exchange", "mma_w
 
 
 def last_kernel():
-    """Kernel of this thread's last single-instance run: "plain", "tensor-int8", "tensor-fp4" (None before any)."""
+    """Kernel of this thread's last single-instance run: "plain", "plain-cluster", "tensor-int8", "tensor-fp4" (None
+    before any)."""
     return KERNELS[load().anc_last_kernel()]
 
 

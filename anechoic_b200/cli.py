@@ -5,7 +5,7 @@ so check_ref-style replays and the estimators (anechoic_b200.analyze) read them 
     python -m anechoic_b200.cli (--graph F | --gset F | --jint8 F) [--bias F] [--kbits K]
         --output PREFIX [--chains B] [--batches NB] [--seed S] [--offset O] [--trace 0|1]
         [--steps S --t0 T0 --t1 T1 --q Q --lambda L --tec-jv JV --tecT KAPPA --ramp]
-        [--target CUT | --target-energy E] [--wide auto|0|1] [--check-fields 0|1] [--engine auto|plain|tensor]
+        [--target CUT | --target-energy E] [--wide auto|0|1] [--check-fields 0|1] [--engine auto|plain|tensor|cluster]
         [--warmup W] [--info]
 
 The reference's kernel-geometry flags (--cs, --groups, --clusters, --burn, --r, --preg) are accepted and recorded;

@@ -72,6 +72,7 @@ struct anc_instance {
     std::vector<int8_t> dense;                    // host copy of dense couplings (tensor engine packs lazily)
     anc::TensorInstance tensor;                   // tensor-engine operands (built on first use)
     bool tensor_ready = false;
+    int cluster_wave = -1;                        // co-resident clusters of the cluster variant (-1: not queried)
     // per-handle workspace for single-job launches
     DevBuf<int> counter;
     DevBuf<uint32_t> w_spins;
@@ -262,13 +263,29 @@ int launch_plain_single(anc_instance* I, const anc::PlainJob& job, cudaStream_t 
     return ANC_OK;
 }
 
+// Clusters of the cluster variant co-resident on the device (queried once per instance; 0 if unavailable).
+int cluster_wave(anc_instance* I) {
+    if (I->cluster_wave < 0) {
+        int w = 0;
+        if (anc::plain_cluster_max_active(&w) != 0) {
+            cudaGetLastError();
+            w = 0;
+        }
+        I->cluster_wave = w;
+    }
+    return I->cluster_wave;
+}
+
 int pick_engine(anc_instance* I, anc_tables* tb, int nchains, const anc_run_opts* o) {
     const int e = o ? o->engine : ANC_ENGINE_AUTO;
-    if (e == ANC_ENGINE_PLAIN || e == ANC_ENGINE_TENSOR) return e;
-    return !I->dense.empty() && anc::tensor_supported(I->n, I->K, nchains) &&
-                   anc::tensor_prefer(I->n, I->K, nchains, tb->S)
-               ? ANC_ENGINE_TENSOR
-               : ANC_ENGINE_PLAIN;
+    if (e == ANC_ENGINE_PLAIN || e == ANC_ENGINE_TENSOR || e == ANC_ENGINE_CLUSTER) return e;
+    if (!I->dense.empty() && anc::tensor_supported(I->n, I->K, nchains) &&
+        anc::tensor_prefer(I->n, I->K, nchains, tb->S))
+        return ANC_ENGINE_TENSOR;
+    // the cluster variant runs in waves of co-resident clusters, ~3.2 ms per wave for N = 2000 x 1000 steps; the
+    // one-CTA plain engine takes ~11.2 ms for up to one anneal per SM: clusters win up to three waves
+    if (anc::plain_cluster_supported(I->K, I->np) && nchains <= 3 * cluster_wave(I)) return ANC_ENGINE_CLUSTER;
+    return ANC_ENGINE_PLAIN;
 }
 
 int ensure_tensor(anc_instance* I) {
@@ -330,6 +347,15 @@ int run_device_impl(anc_instance* I, anc_tables* tb, uint64_t seed, uint32_t off
         return ANC_OK;
     }
     const anc::PlainJob job = make_job(I, tb, seed, off, nchains, hclamp, out);
+    if (engine == ANC_ENGINE_CLUSTER) {
+        if (!anc::plain_cluster_supported(I->K, I->np))
+            return fail(ANC_EINVAL, "the cluster engine needs dense 1-bit couplings with n <= 2048 (n=%d K=%d)", I->n,
+                        I->K);
+        rc = anc::plain_cluster_launch(job, st);
+        if (rc) return cuda_fail(cudaError_t(rc), "cluster engine launch");
+        g_last_kernel = ANC_KERNEL_PLAIN_CLUSTER;
+        return ANC_OK;
+    }
     rc = launch_plain_single(I, job, st);
     if (rc == ANC_OK) g_last_kernel = ANC_KERNEL_PLAIN;
     return rc;

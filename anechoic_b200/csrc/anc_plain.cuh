@@ -83,4 +83,10 @@ inline size_t plain_smem_plan(int np_max, int nwj_max, int K, int P, bool* strea
 int plain_launch(const PlainLaunch& L, int K, int P, int grid, size_t smem, cudaStream_t stream);
 int plain_max_blocks_per_sm(int K, int P, size_t smem, int* out, bool stream = false);
 
+// Cluster variant (plain_engine.cu): one anneal per cluster of 8 CTAs, dense K = 1 couplings with NP = 2048 only.
+// job.ntrials anneals, trial c = job.trial_offset + c; every output is written (no zeroing needed).
+bool plain_cluster_supported(int K, int np);
+int plain_cluster_launch(const PlainJob& job, cudaStream_t stream);
+int plain_cluster_max_active(int* out);      // clusters co-resident on this device
+
 }  // namespace anc

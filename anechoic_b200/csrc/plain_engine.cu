@@ -409,6 +409,241 @@ __global__ void __launch_bounds__(T, 1) plain_kernel(const __grid_constant__ Pla
     }
 }
 
+// ------------------------------------------------------------------------------------------------ cluster variant
+// One anneal spread over a cluster of kCR = 8 CTAs (dense K = 1, NP = 2048), for the lowest latency per anneal.
+// CTA r owns RNG lanes 32r .. 32r+31, i.e. spin word k*8 + r of every round k. Per step:
+//   1. warp 0 decides its 32 lanes x 8 rounds exactly as plain_kernel (fields in registers), building per round the
+//      flip word and the new-sign word (flipped from +1) with two ballots, and the n_lin partial;
+//   2. lanes 0..16 store the 8 flip words, 8 new-sign words and the partial into every CTA's receive slot for this
+//      pass's parity (st.shared::cluster), and one cluster barrier (release / acquire) makes them visible;
+//   3. every CTA turns the 64 flip words into the step's flip list (the same list in every CTA) and counts, for its
+//      8 owned words, the flipped rows x with s'_x J_xy = +1 in bit-sliced carry-save counters. Its 8 words of every
+//      J row (64 KB) stay in shared memory, so no row is read from L2 during the anneal;
+//   4. the deciders add the counts into their fields at the start of the next step (dense_delta, as plain_kernel).
+// The receive slots alternate by pass parity: a slot is rewritten two passes later, after every CTA has passed the
+// cluster barrier of the pass in between, so one barrier per step suffices. No CTA waits on anything but cluster
+// and CTA barriers, which every thread of every CTA reaches the same number of times.
+constexpr int kCT = 256;                  // threads per CTA
+constexpr int kCR = 8;                    // CTAs per anneal
+constexpr int kCW = 20;                   // receive words per source CTA: 8 flip, 8 new-sign, n_lin partial, spare
+constexpr size_t kClusterSmem = 116 * 1024;   // above half an SM's shared memory: one CTA per SM
+
+__device__ __forceinline__ uint32_t sm_addr(const void* p) { return uint32_t(__cvta_generic_to_shared(p)); }
+__device__ __forceinline__ uint32_t cl_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ uint32_t cl_id() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%clusterid.x;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ uint32_t cl_map(uint32_t local, uint32_t rank) {
+    uint32_t a;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(a) : "r"(local), "r"(rank));
+    return a;
+}
+__device__ __forceinline__ void cl_store(uint32_t addr, uint32_t v) {
+    asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
+}
+__device__ __forceinline__ void cl_sync() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+template <int P>
+__global__ void __cluster_dims__(kCR, 1, 1) __launch_bounds__(kCT, 1)
+    plain_cluster_kernel(const __grid_constant__ PlainJob job) {
+    constexpr int R = 8, NWJ = 64;
+    extern __shared__ __align__(16) uint8_t smem_raw[];
+    uint32_t* Jl = reinterpret_cast<uint32_t*>(smem_raw);   // [2048][8]: owned words of every J row
+    uint32_t* flist = Jl + 2048 * 8;                        // [2048]: flipped slot | new spin -1 << 31
+    uint32_t* recv = flist + 2048;                          // [2][kCR][kCW]
+    uint32_t* comb = recv + 2 * kCR * kCW;                  // [8 warps][8 words][P]
+    uint32_t* res = comb + 8 * 8 * P;                       // [8 words][P]
+    __shared__ int s_cnt[2];
+    __shared__ long long s_part[kCR][2];                    // rank 0: every rank's sum of s*h and of b*s
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t rank = cl_rank();
+    const int c = int(cl_id());                             // anneal index within the launch
+    const int n = job.n, nw = job.nw, S = job.tab.S;
+    const int32_t hclamp = job.hclamp;
+    const int32_t* __restrict__ bias = job.bias;
+
+    for (int e = tid; e < 2048 * 8; e += kCT) Jl[e] = __ldg(job.planes + size_t(e >> 3) * NWJ + (e & 7) * 8 + rank);
+    cl_sync();                                              // every CTA's shared memory is set up before any store
+
+    // decider state (warp 0): lane l of this CTA owns slots i_k = k*256 + 32 rank + lane
+    Xoshiro rng;
+    int32_t hv[R];
+    uint32_t sup = 0u, dif = 0u, vm = 0u;                   // bit k: spin +1 / flipped last pass / active slot
+    uint32_t Fw[R], Nw[R];
+    int32_t nlin_prev = 0, nl = 0;
+    long long flips = 0;
+    if (warp == 0) {
+        rng_seed(rng, job.seed, job.trial_offset + uint32_t(c), 32u * rank + uint32_t(lane));
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+            const uint32_t rv = rng_next(rng);
+            const int i = k * kLanes + 32 * int(rank) + lane;
+            const bool valid = i < n;
+            const uint32_t sbit = valid ? (rv >> 31) : 1u;
+            sup |= sbit << k;
+            if (valid) vm |= 1u << k;
+            if (valid && !sbit) dif |= 1u << k;             // s_prev = +1 initially
+            hv[k] = (valid && bias) ? bias[i] : 0;
+            Fw[k] = __ballot_sync(FULL, valid);             // initial pass: F = active slots, new spin = s0
+            Nw[k] = __ballot_sync(FULL, valid && !sbit);
+        }
+    }
+    int pass_nf = 0, pass_mult = 1;
+    bool pass_init = true;
+    for (int t = -1; t < S; ++t) {
+        const int par = (t + 1) & 1;
+        if (t >= 0 && warp == 0) {
+            const int32_t fourT = __ldg(job.tab.fourT + t), twoT = fourT >> 1, qv = __ldg(job.tab.q + t);
+            const int32_t corr = step_corr(nlin_prev, __ldg(job.tab.kcorr + t), __ldg(job.tab.kconst + t));
+            const uint32_t lw = uint32_t(2 * twoT - 1);
+            nl = 0;
+#pragma unroll
+            for (int k = 0; k < R; ++k) {
+                const uint32_t u = rng_next(rng);
+                const bool valid = (vm >> k) & 1u, s_up = (sup >> k) & 1u, df = (dif >> k) & 1u;
+                hv[k] += pass_mult * dense_delta<1, P>(res + k * P, 8, 0, lane, pass_nf, pass_init || df, s_up);
+                int32_t hs = s_up ? hv[k] : -hv[k];
+                if (hclamp > 0) hs = max(-hclamp, min(hs, hclamp));
+                const int32_t x = qv + (df ? corr : -corr);
+                const int32_t zt = hs * 65536 + x;
+                const bool fl = valid && (zt - threshold16(u, fourT) < 0);
+                const bool ln = valid && (uint32_t(zt + twoT - 1) < lw);
+                const uint32_t fb = __ballot_sync(FULL, fl);
+                Fw[k] = fb;
+                Nw[k] = fb & __ballot_sync(FULL, s_up);     // flipped from +1: new spin -1
+                nl += __popc(__ballot_sync(FULL, ln));
+                if (fl) sup ^= 1u << k;
+                dif = (dif & ~(1u << k)) | (uint32_t(fl) << k);
+            }
+        }
+        if (warp == 0 && lane <= 16) {
+            uint32_t v = uint32_t(nl);
+#pragma unroll
+            for (int k = 0; k < R; ++k) {
+                if (lane == k) v = Fw[k];
+                if (lane == 8 + k) v = Nw[k];
+            }
+            const uint32_t local = sm_addr(recv + (par * kCR + rank) * kCW + lane);
+#pragma unroll
+            for (int r = 0; r < kCR; ++r) cl_store(cl_map(local, uint32_t(r)), v);
+        }
+        cl_sync();
+        // the pass's flip list, the same in every CTA: word wi = k*8 + r (round k, source CTA r) holds slots 32 wi + b
+        if (tid < 64) {
+            const uint32_t* src = recv + (par * kCR + (tid & 7)) * kCW;
+            const uint32_t F = src[tid >> 3], N = src[8 + (tid >> 3)];
+            const int cnt = __popc(F);
+            int incl = cnt;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(FULL, incl, o);
+                if (lane >= o) incl += y;
+            }
+            if (lane == 31) s_cnt[warp] = incl;
+            __syncwarp();
+            asm volatile("bar.sync 1, 64;" ::: "memory");
+            int pos = incl - cnt + (warp == 1 ? s_cnt[0] : 0);
+            uint32_t m = F;
+            while (m) {
+                const int b = __ffs(m) - 1;
+                m &= m - 1;
+                flist[pos++] = uint32_t(32 * tid + b) | (((N >> b) & 1u) << 31);
+            }
+        }
+        __syncthreads();
+        const int nf = s_cnt[0] + s_cnt[1];
+        if (t >= 0) {
+            int32_t nlin = 0;
+#pragma unroll
+            for (int r = 0; r < kCR; ++r) nlin += int32_t(recv[(par * kCR + r) * kCW + 16]);
+            nlin_prev = nlin;
+            flips += nf;
+            if (rank == 0 && tid == 0 && job.trace && job.out_trace) job.out_trace[size_t(c) * S + t] = nlin;
+        }
+        // counts of the owned words: warp w, lane (sub = lane / 8, word = lane % 8) takes rows f0 + sub + 4j
+        {
+            const int sub = lane >> 3, w = lane & 7;
+            BitCounter<P> cnt;
+            cnt.clear();
+            for (int f0 = warp * 32; f0 < nf; f0 += 8 * 32) {
+                uint32_t a[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const int f = f0 + sub + 4 * j;
+                    if (f < nf) {
+                        const uint32_t e = flist[f];
+                        a[j] = Jl[(e & 0x7fffffffu) * 8 + w] ^ ((e >> 31) ? FULL : 0u);
+                    } else {
+                        a[j] = 0u;
+                    }
+                }
+                cnt.add8(a);
+            }
+#pragma unroll
+            for (int o = 8; o <= 16; o <<= 1) {
+                uint32_t other[P];
+#pragma unroll
+                for (int p = 0; p < P; ++p) other[p] = __shfl_xor_sync(FULL, cnt.c[p], o);
+                cnt.add_planes(other);
+            }
+            if (sub == 0) cnt.store(comb + (warp * 8 + w) * P);
+            __syncthreads();
+            if (tid < 8) {
+                BitCounter<P> acc;
+                acc.clear();
+                for (int v = 0; v < 8; ++v) acc.add_planes(comb + (v * 8 + tid) * P);
+                acc.store(res + tid * P);
+            }
+            __syncthreads();
+        }
+        pass_nf = nf;
+        pass_mult = t >= 0 ? 2 : 1;
+        pass_init = t < 0;
+    }
+    // the last pass's counts, then the outputs
+    long long sh = 0, bs = 0;
+    if (warp == 0) {
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+            const bool valid = (vm >> k) & 1u, s_up = (sup >> k) & 1u, df = (dif >> k) & 1u;
+            hv[k] += pass_mult * dense_delta<1, P>(res + k * P, 8, 0, lane, pass_nf, pass_init || df, s_up);
+            const int i = k * kLanes + 32 * int(rank) + lane;
+            const uint32_t sword = __ballot_sync(FULL, s_up);
+            if (valid) {
+                sh += s_up ? hv[k] : -hv[k];
+                if (bias) bs += s_up ? bias[i] : -bias[i];
+                if (job.out_h) job.out_h[size_t(c) * n + i] = hv[k];
+            }
+            const int wi = k * 8 + int(rank);
+            if (lane == 0 && wi < nw) job.out_spins[size_t(c) * nw + wi] = sword & valid_mask(wi, n);
+        }
+        sh = warp_sum64(sh);
+        bs = warp_sum64(bs);
+        if (lane == 0) {
+            const uint32_t a = cl_map(sm_addr(&s_part[rank][0]), 0u);
+            asm volatile("st.shared::cluster.u64 [%0], %1;" ::"r"(a), "l"(sh) : "memory");
+            asm volatile("st.shared::cluster.u64 [%0], %1;" ::"r"(a + 8u), "l"(bs) : "memory");
+        }
+    }
+    cl_sync();
+    if (rank == 0 && tid == 0) {
+        long long a = 0, b = 0;
+        for (int r = 0; r < kCR; ++r) { a += s_part[r][0]; b += s_part[r][1]; }
+        job.out_sum_sh[c] = a;
+        if (job.out_sum_bs) job.out_sum_bs[c] = b;
+        job.out_flips[c] = flips;
+    }
+}
+
 template <int K, int P, bool SPARSE, bool STREAM = false>
 int launch_t(const PlainLaunch& L, int grid, size_t smem, cudaStream_t st) {
     auto fn = plain_kernel<K, P, SPARSE, STREAM>;
@@ -447,6 +682,34 @@ int plain_launch(const PlainLaunch& L, int K, int P, int grid, size_t smem, cuda
         if (K == 4) return launch_t<4, 16, false>(L, grid, smem, st);
     }
     return int(cudaErrorInvalidValue);
+}
+
+bool plain_cluster_supported(int K, int np) { return K == 1 && np == 2048; }
+
+int plain_cluster_launch(const PlainJob& job, cudaStream_t st) {
+    auto fn = plain_cluster_kernel<12>;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kClusterSmem));
+    if (e != cudaSuccess) return int(e);
+    fn<<<job.ntrials * kCR, kCT, kClusterSmem, st>>>(job);
+    return int(cudaGetLastError());
+}
+
+int plain_cluster_max_active(int* out) {
+    auto fn = plain_cluster_kernel<12>;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kClusterSmem));
+    if (e != cudaSuccess) return int(e);
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = kCR;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cfg.gridDim = dim3(kCR);
+    cfg.blockDim = dim3(kCT);
+    cfg.dynamicSmemBytes = kClusterSmem;
+    return int(cudaOccupancyMaxActiveClusters(out, fn, &cfg));
 }
 
 int plain_max_blocks_per_sm(int K, int P, size_t smem, int* out, bool stream) {

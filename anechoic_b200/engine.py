@@ -193,7 +193,7 @@ class RunResult:
     fields: Optional[np.ndarray] = None
     device_ms: float = 0.0
     profile: Optional[dict] = None
-    kernel: Optional[str] = None     # "plain", "tensor-int8" or "tensor-fp4"
+    kernel: Optional[str] = None     # "plain", "plain-cluster", "tensor-int8" or "tensor-fp4"
 
     def cuts(self, sumw: int) -> np.ndarray:
         """Device cut = (sumw + sum_sh / 2) / 2 with C++ truncating division (sca_ref.hpp:153)."""
@@ -213,9 +213,10 @@ def tdiv(a, b: int):
 def run(dev: DeviceInstance, tb: Tables, seed: int, trial_offset: int, nchains: int, trace: bool = False,
         fields: bool = False, engine: str = "auto", wide="auto", profile: bool = False,
         tensor_kind: str = "auto") -> RunResult:
-    """nchains anneals (trial ids trial_offset .. trial_offset + nchains - 1) in one launch. profile=True records
-    the tensor engine's per-phase cycle counters (RunResult.profile); tensor_kind picks the tensor engine's operand
-    format ("auto", "int8", "fp4")."""
+    """nchains anneals (trial ids trial_offset .. trial_offset + nchains - 1) in one launch. engine: "auto",
+    "plain" (one CTA per anneal), "cluster" (one anneal per 8-CTA cluster; dense 1-bit couplings, n <= 2048) or
+    "tensor" (replicas sharing J). profile=True records the tensor engine's per-phase cycle counters
+    (RunResult.profile); tensor_kind picks the tensor engine's operand format ("auto", "int8", "fp4")."""
     L = load()
     n = dev.n
     W = spin_words(n)

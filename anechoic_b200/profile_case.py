@@ -17,7 +17,7 @@ import anechoic_b200 as A
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--engine", default="plain", choices=["auto", "plain", "tensor"])
+    ap.add_argument("--engine", default="plain", choices=["auto", "plain", "tensor", "cluster"])
     ap.add_argument("--chains", type=int, default=148)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--n", type=int, default=2000)

@@ -8,7 +8,7 @@ Target cut: 0.995 x the best cut of 1000 long anneals (S = 5000, same correction
 exact engine outside the timed region. TTS99: primary t_batch ln(0.01)/ln(1 - P_batch), secondary
 t_batch ln(0.01)/(B ln(1 - p)) (reference estimators, gpu/onsager_v2_20261007/src/analyze.py:15-47).
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--engine auto|plain|tensor] [--tensor-kind auto|int8|fp4]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--engine auto|plain|tensor|cluster] [--tensor-kind auto|int8|fp4]
                   [--impl ours|reference]
 
 --impl reference times the reference's own CPU golden model (sca::run_trial_bias compiled unmodified into
@@ -466,7 +466,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--engine", default="auto", choices=["auto", "plain", "tensor"])
+    ap.add_argument("--engine", default="auto", choices=["auto", "plain", "tensor", "cluster"])
     ap.add_argument("--tensor-kind", default="auto", choices=["auto", "int8", "fp4"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-engine comparison run")

@@ -38,6 +38,10 @@ extern "C" {
 #define ANC_ENGINE_AUTO 0   /* pick per launch (autotuned crossover) */
 #define ANC_ENGINE_PLAIN 1  /* bit-column engine: one CTA per anneal, bit-packed couplings, flipped columns only */
 #define ANC_ENGINE_TENSOR 2 /* batched engine: replicas sharing J, tcgen05 int8 J * dS update */
+#define ANC_ENGINE_CLUSTER 3 /* bit-column engine with each anneal spread over a cluster of 8 CTAs (dense K = 1,
+                               n <= 2048): the lowest latency per anneal. The reference's engine keeps one anneal on
+                               an 8-CTA cluster too (gpu/onsager_v2_20261007/src/sca_gpu.cu:223-295); AUTO picks it
+                               for up to three waves of co-resident clusters */
 
 #define ANC_TENSOR_AUTO 0   /* fp4 when exact for the instance (NP = 2048, |J| <= 1, small fields), else int8 */
 #define ANC_TENSOR_INT8 1   /* tcgen05.mma kind::i8, int32 accumulation (any K) */
@@ -244,6 +248,7 @@ ANC_API double anc_last_device_ms(void);
 #define ANC_KERNEL_PLAIN 1        /* bit-column engine */
 #define ANC_KERNEL_TENSOR_INT8 2  /* tcgen05 kind::i8 engine */
 #define ANC_KERNEL_TENSOR_FP4 3   /* tcgen05 kind::mxf4 engine */
+#define ANC_KERNEL_PLAIN_CLUSTER 4 /* bit-column engine, one anneal per 8-CTA cluster */
 ANC_API int anc_last_kernel(void);
 
 /* Message of the calling thread's last failure ("" if none). */
