@@ -42,7 +42,7 @@ class InstanceInfo(C.Structure):
 
 class RunOpts(C.Structure):
     _fields_ = [("engine", C.c_int), ("wide", C.c_int), ("threads", C.c_int), ("profile", C.c_int),
-                ("tensor_kind", C.c_int), ("reserved", C.c_int * 3)]
+                ("tensor_kind", C.c_int), ("flip_permille", C.c_int), ("reserved", C.c_int * 2)]
 
 
 class Job(C.Structure):
@@ -87,6 +87,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         L.anc_run_fields.argtypes = [_vp, _vp, _u64, _u32, _i, C.POINTER(RunOpts), _vp, _vp, _vp, _vp, _vp, _vp]
         L.anc_run_device.argtypes = [_vp, _vp, _u64, _u32, _i, C.POINTER(RunOpts), _vp, _vp, _vp, _vp, _vp, _vp]
         L.anc_run_batch.argtypes = [_i, C.POINTER(Job), C.POINTER(RunOpts)]
+        L.anc_auto_estimate.argtypes = [_i, _i, _i, _i, _d, _i, _vp, _vp]
+        L.anc_auto_choice.argtypes = [_vp, _vp, _i, C.POINTER(RunOpts), _vp, _vp, _vp]
         L.anc_last_device_ms.argtypes = []
         L.anc_last_device_ms.restype = C.c_double
         L.anc_last_kernel.argtypes = []
@@ -106,13 +108,15 @@ def check(rc: int):
         raise AncError(rc, msg)
 
 
-def opts(engine: str = "auto", wide="auto", profile: bool = False, tensor_kind: str = "auto") -> RunOpts:
+def opts(engine: str = "auto", wide="auto", profile: bool = False, tensor_kind: str = "auto",
+         flip_fraction=None) -> RunOpts:
     o = RunOpts()
     o.engine = ENGINES[engine]
     o.tensor_kind = TENSOR_KINDS[tensor_kind]
     o.wide = {"auto": -1, 0: 0, 1: 1, False: 0, True: 1, "0": 0, "1": 1}[wide]
     o.threads = 0
     o.profile = int(bool(profile))
+    o.flip_permille = 0 if flip_fraction is None else max(1, min(1000, int(round(1000 * flip_fraction))))
     return o
 
 

@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -59,6 +60,57 @@ struct DevBuf {
 
 int pad_np(int n) { return std::max(2048, ((n + 255) / 256) * 256); }
 
+// ---- ANC_ENGINE_AUTO: a cost model of one launch ----
+// Device time per annealing step, in microseconds, fitted to B200 measurements: +-1 complete graphs with
+// n = 500 ... 10000 and dense 2- and 4-bit instances, under schedules whose flip fractions phi (flips per spin per step)
+// span 0.05 ... 0.41.
+//   plain    a_K (NP / 2048)^1.5 + c_K phi n^2   a fixed part per step (decisions, n_lin, step barriers); then every
+//                                               flip rewrites n fields from one row of bit planes (K planes);
+//                                               a_1 = a_2 = 4.5, a_4 = 11.7, c_1 = 6.5e-6, c_2 = 1.65e-5, c_4 = 3.4e-5
+//   cluster  2.2 + 3.2 phi n / 2048              (1-bit couplings, NP = 2048: the rows split over 8 CTAs)
+//   tensor   a constant per kernel: the MMA chain and the decisions cost the same whatever flips: fp4 8.6 (9.2 with
+//            more than one replica group per wave), int8 22.7 at NP = 2048, 21.6 and 27.5 at NP = 3072 and 4096,
+//            streaming 98.5 (measured 98.6 at NP = 10240 and 98 at NP = 16384: bound by its step latency, not by
+//            reading J)
+// Each engine advances a fixed number of anneals at once (per_wave); a launch of more takes further waves.
+constexpr double kPhiPrior = 0.25;   // flip fraction assumed before any run of these tables on this instance
+
+double plain_step_us(int n, int K, double phi) {
+    const double np = double(pad_np(n)), a0 = 4.5 * std::pow(np / 2048.0, 1.5);
+    const double a = K == 4 ? 2.6 * a0 : a0;
+    const double c = K == 4 ? 3.4e-5 : K == 2 ? 1.65e-5 : 6.5e-6;
+    return a + c * phi * double(n) * double(n);
+}
+
+double tensor_step_us(int n, bool fp4, int groups_per_wave) {
+    const int R = pad_np(n) / 256;
+    if (anc::stream_supported(n)) return 98.5;
+    if (R == 8) return fp4 ? (groups_per_wave > 1 ? 9.2 : 8.6) : 22.7;
+    return R == 12 ? 21.6 : 27.5;
+}
+
+// us[ANC_ENGINE_*] for nchains anneals of S steps (-1: engine unavailable, per_wave[e] == 0); returns the engine with
+// the least estimate (ties: plain, then tensor, then cluster).
+int estimate_engines(int n, int K, int nchains, int S, double phi, bool fp4, const int* per_wave, double* us) {
+    phi = std::min(1.0, std::max(0.0, phi));
+    for (int e = 0; e < 4; ++e) us[e] = -1.0;
+    auto waves = [&](int e) { return double((nchains + per_wave[e] - 1) / per_wave[e]); };
+    if (per_wave[ANC_ENGINE_PLAIN] > 0)
+        us[ANC_ENGINE_PLAIN] = waves(ANC_ENGINE_PLAIN) * S * plain_step_us(n, K, phi);
+    if (per_wave[ANC_ENGINE_TENSOR] > 0) {
+        const int groups = std::min(nchains, per_wave[ANC_ENGINE_TENSOR]);
+        us[ANC_ENGINE_TENSOR] = waves(ANC_ENGINE_TENSOR) * S * tensor_step_us(n, fp4, (groups + 127) / 128);
+    }
+    if (per_wave[ANC_ENGINE_CLUSTER] > 0)
+        us[ANC_ENGINE_CLUSTER] = waves(ANC_ENGINE_CLUSTER) * S * (2.2 + 3.2 * phi * double(n) / 2048.0);
+    int best = ANC_ENGINE_PLAIN;
+    for (int e : {ANC_ENGINE_PLAIN, ANC_ENGINE_TENSOR, ANC_ENGINE_CLUSTER})
+        if (us[e] >= 0 && (us[best] < 0 || us[e] < us[best])) best = e;
+    return best;
+}
+
+std::atomic<uint64_t> g_next_uid{1};
+
 }  // namespace
 
 struct anc_instance {
@@ -72,7 +124,8 @@ struct anc_instance {
     std::vector<int8_t> dense;                    // host copy of dense couplings (tensor engine packs lazily)
     anc::TensorInstance tensor;                   // tensor-engine operands (built on first use)
     bool tensor_ready = false;
-    int cluster_wave = -1;                        // co-resident clusters of the cluster variant (-1: not queried)
+    int per_wave[4] = {-1, -1, -1, -1};           // anneals per wave of each engine (ANC_ENGINE_*; -1: not queried)
+    uint64_t uid = g_next_uid.fetch_add(1);       // identifies the instance to the tables' flip record
     // per-handle workspace for single-job launches
     DevBuf<int> counter;
     DevBuf<uint32_t> w_spins;
@@ -92,6 +145,9 @@ struct anc_instance {
 
 struct anc_tables {
     int S = 0;
+    // flip fraction of the last host-output run of these tables (parts per million) and the instance it ran on
+    std::atomic<uint64_t> seen_uid{0};
+    std::atomic<uint32_t> seen_ppm{0};
     std::vector<int32_t> fourT, q, kconst;
     std::vector<int64_t> kcorr;
     DevBuf<int32_t> d_fourT, d_q, d_kconst;
@@ -238,6 +294,17 @@ anc::PlainJob make_job(anc_instance* I, anc_tables* tb, uint64_t seed, uint32_t 
     return j;
 }
 
+// Shared memory plan and co-resident CTAs per SM of the one-CTA plain engine for this instance.
+int plain_residency(const anc_instance* I, int P, size_t* smem, bool* stream, int* per_sm) {
+    *smem = anc::plain_smem_plan(I->np, I->K == 0 ? I->nw : I->nwj, I->K, P, stream);
+    if (*smem > 227 * 1024)
+        return fail(ANC_EINVAL, "instance too large for the plain engine (%zu B shared memory)", *smem);
+    const int rc = anc::plain_max_blocks_per_sm(I->K, P, *smem, per_sm, *stream);
+    if (rc) return cuda_fail(cudaError_t(rc), "occupancy");
+    if (*per_sm < 1) return fail(ANC_EINVAL, "plain engine cannot be resident (smem %zu)", *smem);
+    return ANC_OK;
+}
+
 int launch_plain_single(anc_instance* I, const anc::PlainJob& job, cudaStream_t st) {
     anc::PlainLaunch L{};
     L.job0 = job;
@@ -249,13 +316,11 @@ int launch_plain_single(anc_instance* I, const anc::PlainJob& job, cudaStream_t 
     L.nwj_max = I->K == 0 ? I->nw : I->nwj;
     const int P = plain_P(I->np);
     bool stream = false;
-    const size_t smem = anc::plain_smem_plan(L.np_max, L.nwj_max, I->K, P, &stream);
-    if (smem > 227 * 1024) return fail(ANC_EINVAL, "instance too large for the plain engine (%zu B shared memory)", smem);
-    L.stream = stream ? 1 : 0;
+    size_t smem = 0;
     int per_sm = 0;
-    int rc = anc::plain_max_blocks_per_sm(I->K, P, smem, &per_sm, stream);
-    if (rc) return cuda_fail(cudaError_t(rc), "occupancy");
-    if (per_sm < 1) return fail(ANC_EINVAL, "plain engine cannot be resident (smem %zu)", smem);
+    int rc = plain_residency(I, P, &smem, &stream, &per_sm);
+    if (rc) return rc;
+    L.stream = stream ? 1 : 0;
     const int grid = std::max(1, std::min(job.ntrials, per_sm * I->sms));
     CK(cudaMemsetAsync(I->counter.p, 0, sizeof(int), st));
     rc = anc::plain_launch(L, I->K, P, grid, smem, st);
@@ -263,29 +328,52 @@ int launch_plain_single(anc_instance* I, const anc::PlainJob& job, cudaStream_t 
     return ANC_OK;
 }
 
-// Clusters of the cluster variant co-resident on the device (queried once per instance; 0 if unavailable).
-int cluster_wave(anc_instance* I) {
-    if (I->cluster_wave < 0) {
-        int w = 0;
-        if (anc::plain_cluster_max_active(&w) != 0) {
-            cudaGetLastError();
-            w = 0;
-        }
-        I->cluster_wave = w;
-    }
-    return I->cluster_wave;
+// Whether the tensor engine would run this instance on the fp4 kernel (tensor_fp4_eligible, from the host statistics).
+bool fp4_candidate(const anc_instance* I) {
+    return !I->dense.empty() && I->np == 2048 && I->info.maxabs <= 1 &&
+           I->info.hmax + int64_t(I->info.bmax) < (int64_t(1) << 14);
 }
 
-int pick_engine(anc_instance* I, anc_tables* tb, int nchains, const anc_run_opts* o) {
+// Anneals per wave of each engine on this device (0: the engine cannot run the instance); queried once per instance.
+const int* engine_waves(anc_instance* I) {
+    if (I->per_wave[0] < 0) {
+        int w[4] = {0, 0, 0, 0};
+        size_t smem = 0;
+        bool stream = false;
+        int per_sm = 0;
+        if (plain_residency(I, plain_P(I->np), &smem, &stream, &per_sm) == ANC_OK) w[ANC_ENGINE_PLAIN] = per_sm * I->sms;
+        int t = 0;
+        if (!I->dense.empty() && anc::tensor_supported(I->n, I->K, 1) &&
+            anc::tensor_wave_chains(I->n, fp4_candidate(I), &t) == 0)
+            w[ANC_ENGINE_TENSOR] = std::max(0, t);
+        int c = 0;
+        if (anc::plain_cluster_supported(I->K, I->np) && anc::plain_cluster_max_active(&c) == 0)
+            w[ANC_ENGINE_CLUSTER] = std::max(0, c);
+        cudaGetLastError();   // a failed capacity query only rules that engine out
+        g_err.clear();
+        std::copy(w, w + 4, I->per_wave);
+    }
+    return I->per_wave;
+}
+
+// Flip fraction AUTO assumes: the caller's hint, else what the last host-output run of these tables on this instance
+// saw, else the prior.
+double flip_fraction(const anc_instance* I, const anc_tables* tb, const anc_run_opts* o) {
+    if (o && o->flip_permille > 0) return o->flip_permille / 1000.0;
+    if (tb->seen_uid.load(std::memory_order_relaxed) == I->uid) return tb->seen_ppm.load(std::memory_order_relaxed) * 1e-6;
+    return kPhiPrior;
+}
+
+int pick_engine(anc_instance* I, anc_tables* tb, int nchains, const anc_run_opts* o, double* us = nullptr,
+                double* phi_used = nullptr) {
     const int e = o ? o->engine : ANC_ENGINE_AUTO;
     if (e == ANC_ENGINE_PLAIN || e == ANC_ENGINE_TENSOR || e == ANC_ENGINE_CLUSTER) return e;
-    if (!I->dense.empty() && anc::tensor_supported(I->n, I->K, nchains) &&
-        anc::tensor_prefer(I->n, I->K, nchains, tb->S))
-        return ANC_ENGINE_TENSOR;
-    // the cluster variant runs in waves of co-resident clusters, ~3.2 ms per wave for N = 2000 x 1000 steps; the
-    // one-CTA plain engine takes ~11.2 ms for up to one anneal per SM: clusters win up to three waves
-    if (anc::plain_cluster_supported(I->K, I->np) && nchains <= 3 * cluster_wave(I)) return ANC_ENGINE_CLUSTER;
-    return ANC_ENGINE_PLAIN;
+    const double phi = flip_fraction(I, tb, o);
+    double est[4];
+    const int best = estimate_engines(I->n, I->K, nchains, tb->S, phi, fp4_candidate(I), engine_waves(I), est);
+    if (us) std::copy(est, est + 4, us);
+    if (phi_used) *phi_used = phi;
+    return best;
 }
 
 int ensure_tensor(anc_instance* I) {
@@ -394,6 +482,14 @@ int run_host_impl(anc_instance* I, anc_tables* tb, uint64_t seed, uint32_t off, 
         I->tensor.last_err = nullptr;
         if (rc == -3) return fail(ANC_ETIMEOUT, "tensor engine: %s", why.c_str());
         if (rc) return fail(ANC_ECUDA, "tensor engine: %s", why.c_str());
+    }
+    // the flip fraction this run saw, for AUTO's next choice on these tables and this instance
+    if (flips && I->n > 0) {
+        double total = 0;
+        for (int c = 0; c < nchains; ++c) total += double(flips[c]);
+        const double phi = total / (double(nchains) * I->n * tb->S);
+        tb->seen_ppm.store(uint32_t(std::min(1.0, std::max(0.0, phi)) * 1e6 + 0.5), std::memory_order_relaxed);
+        tb->seen_uid.store(I->uid, std::memory_order_relaxed);
     }
     if (I->prof_ctas > 0) {
         const size_t ns = anc::kTensorProfSlots;
@@ -720,6 +816,29 @@ int anc_range_plan(const anc_instance* I, const anc_tables* tb, int* plain_ok, i
     if (plain_ok) *plain_ok = pl.plain_ok;
     if (hclamp) *hclamp = pl.hclamp;
     return ANC_OK;
+}
+
+int anc_auto_estimate(int n, int kbits, int nchains, int S, double phi, int fp4, const int* per_wave, double* us) {
+    if (n < 1 || nchains < 1 || S < 1 || !per_wave || !us || !(kbits == 0 || kbits == 1 || kbits == 2 || kbits == 4))
+        return fail(ANC_EINVAL, "anc_auto_estimate: n, nchains, S >= 1, kbits in {0, 1, 2, 4}, per_wave and us");
+    int w[4];
+    for (int e = 0; e < 4; ++e) w[e] = std::max(0, per_wave[e]);
+    if (w[ANC_ENGINE_PLAIN] + w[ANC_ENGINE_TENSOR] + w[ANC_ENGINE_CLUSTER] == 0)
+        return fail(ANC_EINVAL, "anc_auto_estimate: no engine available");
+    return estimate_engines(n, kbits, nchains, S, phi, fp4 != 0, w, us);
+}
+
+int anc_auto_choice(anc_instance* I, anc_tables* tb, int nchains, const anc_run_opts* o, double* us, int* per_wave,
+                    double* phi) {
+    if (!I || !tb || nchains < 1) return fail(ANC_EINVAL, "anc_auto_choice: handles and nchains >= 1 required");
+    anc_run_opts a = o ? *o : anc_run_opts{};
+    a.engine = ANC_ENGINE_AUTO;
+    double est[4], f = 0;
+    const int e = pick_engine(I, tb, nchains, &a, est, &f);
+    if (us) std::copy(est, est + 4, us);
+    if (per_wave) std::copy(I->per_wave, I->per_wave + 4, per_wave);
+    if (phi) *phi = f;
+    return e;
 }
 
 int anc_run(anc_instance* I, anc_tables* tb, uint64_t seed, uint32_t off, int nchains, const anc_run_opts* o,

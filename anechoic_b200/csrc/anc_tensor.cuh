@@ -56,7 +56,9 @@ struct TensorGeometry {
 int tensor_geometry(int n, int nchains, TensorGeometry* g);
 
 bool tensor_supported(int n, int K, int nchains);
-bool tensor_prefer(int n, int K, int nchains, int S);
+// Anneals one launch of the tensor kernel that runs this instance advances together (more anneals take further waves
+// of replica groups inside the launch): fp4 is whether the fp4 kernel would run it.
+int tensor_wave_chains(int n, bool fp4, int* out);
 int tensor_build_instance(const int8_t* J, int n, TensorInstance* out, std::string* why);
 int tensor_run(TensorInstance* ti, const TensorRun& r, cudaStream_t st, std::string* why);
 // Whether the fp4 kernel can run this instance with this bias bound exactly (the fields stay far inside the range
@@ -66,6 +68,7 @@ bool tensor_fp4_eligible(const TensorInstance* ti, int64_t bias_absmax);
 bool stream_supported(int n);
 void stream_permutation(int np, std::vector<int>* p);
 int stream_width();
+int stream_wave_chains();
 int stream_run(TensorInstance* ti, const TensorRun& r, const int32_t* bias_perm, cudaStream_t st, std::string* why);
 // After the stream has reached the launch: -3 if a bounded device wait expired, 0 otherwise.
 int tensor_check_error(TensorInstance* ti, cudaStream_t st, std::string* why);

@@ -1572,14 +1572,6 @@ bool tensor_supported(int n, int K, int nchains) {
     return nchains >= 1 && (R == 8 || R == 12 || R == 16 || stream_supported(n));
 }
 
-bool tensor_prefer(int n, int K, int nchains, int S) {
-    (void)S;
-    // the streaming kernel reads J once per step for two replica groups; the plain engine reads the flipped rows of
-    // every anneal, which no longer fit in L2 at these sizes
-    if (stream_supported(n)) return tensor_supported(n, K, nchains) && nchains >= 64;
-    return tensor_supported(n, K, nchains) && nchains >= 256;
-}
-
 int tensor_build_instance(const int8_t* J, int n, TensorInstance* out, std::string* why) {
     const int np = std::max(2048, ((n + 255) / 256) * 256);
     const int R = np / 256, nc = 16 * R;
@@ -1893,6 +1885,30 @@ int res_run(TensorInstance* ti, const TensorRun& r, cudaStream_t st, std::string
 
 }  // namespace
 
+int tensor_wave_chains(int n, bool fp4, int* out) {
+    const int R = std::max(2048, ((n + 255) / 256) * 256) / 256;
+    constexpr int kMany = 1 << 20;   // more groups than any device holds: the query returns the device's limit
+    int slots = 0, rc = 0;
+    *out = 0;
+    if (stream_supported(n)) {
+        *out = stream_wave_chains();
+        return 0;
+    }
+    if (R == 8 && fp4) {
+        rc = f4_group_slots(kMany, &slots);        // one group of kM anneals per 16-CTA slot
+        *out = slots * kM;
+    } else if (R == 8) {
+        rc = res_pair_slots(kMany, &slots);        // two groups per 32-CTA pair slot
+        *out = 2 * slots * kM;
+    } else if (R == 12 || R == 16) {
+        rc = R == 12 ? max_clusters_t<12>(&slots) : max_clusters_t<16>(&slots);   // one group per cluster
+        *out = slots * kM;
+    } else {
+        rc = int(cudaErrorInvalidValue);
+    }
+    return rc;
+}
+
 int tensor_run(TensorInstance* ti, const TensorRun& r, cudaStream_t st, std::string* why) {
     const int np = ti->np, R = np / 256;
     int rc0 = ensure_bias_perm(ti, r.bias, why);
@@ -1966,8 +1982,7 @@ int tensor_run(TensorInstance* ti, const TensorRun& r, cudaStream_t st, std::str
     P.err = err;
     P.prof = r.prof;
     int rc = -1;
-    if (R == 8) rc = launch_t<8>(P, groups, mapA, mapB, st, why);
-    else if (R == 12) rc = launch_t<12>(P, groups, mapA, mapB, st, why);
+    if (R == 12) rc = launch_t<12>(P, groups, mapA, mapB, st, why);   // NP = 2048 runs the resident kernel above
     else if (R == 16) rc = launch_t<16>(P, groups, mapA, mapB, st, why);
     if (rc) return rc;
     ti->last_err = err;

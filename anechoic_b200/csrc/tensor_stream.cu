@@ -441,6 +441,9 @@ void stream_permutation(int np, std::vector<int>* p) {
 
 int stream_width() { return kSNPP; }
 
+// The kernel advances one pair of replica groups at a time across all its CTAs.
+int stream_wave_chains() { return 2 * kSM; }
+
 int stream_run(TensorInstance* ti, const TensorRun& r, const int32_t* bias_perm, cudaStream_t st, std::string* why) {
     const int R = ti->np / 256;
     const int ngroups = (r.nchains + kSM - 1) / kSM;

@@ -212,10 +212,12 @@ def tdiv(a, b: int):
 
 def run(dev: DeviceInstance, tb: Tables, seed: int, trial_offset: int, nchains: int, trace: bool = False,
         fields: bool = False, engine: str = "auto", wide="auto", profile: bool = False,
-        tensor_kind: str = "auto") -> RunResult:
+        tensor_kind: str = "auto", flip_fraction: Optional[float] = None) -> RunResult:
     """nchains anneals (trial ids trial_offset .. trial_offset + nchains - 1) in one launch. engine: "auto",
     "plain" (one CTA per anneal), "cluster" (one anneal per 8-CTA cluster; dense 1-bit couplings, n <= 2048) or
-    "tensor" (replicas sharing J). profile=True records the tensor engine's per-phase cycle counters
+    "tensor" (replicas sharing J). "auto" runs the engine with the least estimated device time (auto_estimate);
+    flip_fraction (flips per spin per step) overrides the fraction it assumes, which is otherwise what the last run
+    of these tables on this instance saw. profile=True records the tensor engine's per-phase cycle counters
     (RunResult.profile); tensor_kind picks the tensor engine's operand format ("auto", "int8", "fp4")."""
     L = load()
     n = dev.n
@@ -225,7 +227,7 @@ def run(dev: DeviceInstance, tb: Tables, seed: int, trial_offset: int, nchains: 
     S = tb.S
     tr = np.zeros((nchains, S), np.int32) if trace else None
     hf = np.zeros((nchains, n), np.int32) if fields else None
-    o = _lib.opts(engine, wide, profile, tensor_kind)
+    o = _lib.opts(engine, wide, profile, tensor_kind, flip_fraction)
     args = (dev._h, tb._h, C.c_uint64(seed), C.c_uint32(trial_offset), nchains, C.byref(o), spins.ctypes.data,
             sh.ctypes.data, bs.ctypes.data, fl.ctypes.data, tr.ctypes.data if trace else None)
     if fields:
@@ -237,6 +239,39 @@ def run(dev: DeviceInstance, tb: Tables, seed: int, trial_offset: int, nchains: 
     if profile:
         res.profile = _lib.last_profile()
     return res
+
+
+_ENGINE_NAMES = {v: k for k, v in _lib.ENGINES.items()}
+
+
+def auto_estimate(n: int, kbits: int, nchains: int, S: int, flip_fraction: float, per_wave: dict,
+                  fp4: bool = False) -> dict:
+    """The cost model behind engine="auto", host-only: estimated device time (ms) of one launch on each engine
+    available (per_wave: anneals each engine advances at once, e.g. {"plain": 148, "tensor": 1152, "cluster": 15}),
+    and under "pick" the engine with the least."""
+    w = (C.c_int * 4)(0, *(int(per_wave.get(e, 0)) for e in ("plain", "tensor", "cluster")))
+    us = (C.c_double * 4)()
+    e = load().anc_auto_estimate(n, kbits, nchains, S, float(flip_fraction), int(bool(fp4)), w, us)
+    if e < 0:
+        check(e)
+    out = {_ENGINE_NAMES[i]: us[i] / 1000.0 for i in (1, 2, 3) if us[i] >= 0}
+    out["pick"] = _ENGINE_NAMES[e]
+    return out
+
+
+def auto_choice(dev: DeviceInstance, tb: Tables, nchains: int, flip_fraction: Optional[float] = None) -> dict:
+    """The engine engine="auto" would run for run(dev, tb, ..., nchains), with the estimates (ms), the anneals per
+    wave of each engine on this device and the flip fraction it assumed."""
+    us = (C.c_double * 4)()
+    w = (C.c_int * 4)()
+    phi = C.c_double()
+    o = _lib.opts("auto", flip_fraction=flip_fraction)
+    e = load().anc_auto_choice(dev._h, tb._h, nchains, C.byref(o), us, w, C.byref(phi))
+    if e < 0:
+        check(e)
+    names = ("plain", "tensor", "cluster")
+    return {"pick": _ENGINE_NAMES[e], "ms": {k: us[i + 1] / 1000.0 for i, k in enumerate(names) if us[i + 1] >= 0},
+            "per_wave": {k: w[i + 1] for i, k in enumerate(names)}, "flip_fraction": phi.value}
 
 
 def run_batch(jobs: List[dict], engine: str = "auto", wide="auto") -> List[RunResult]:

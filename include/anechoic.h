@@ -35,13 +35,12 @@ extern "C" {
 #define ANC_ETIMEOUT (-3)  /* a bounded device-side wait gave up (the kernel returned an error status) */
 #define ANC_EMISMATCH (-4) /* internal consistency check failed (reference: cut mismatch, exit 2) */
 
-#define ANC_ENGINE_AUTO 0   /* pick per launch (autotuned crossover) */
+#define ANC_ENGINE_AUTO 0   /* pick per launch: the engine with the least estimated device time (anc_auto_estimate) */
 #define ANC_ENGINE_PLAIN 1  /* bit-column engine: one CTA per anneal, bit-packed couplings, flipped columns only */
 #define ANC_ENGINE_TENSOR 2 /* batched engine: replicas sharing J, tcgen05 int8 J * dS update */
 #define ANC_ENGINE_CLUSTER 3 /* bit-column engine with each anneal spread over a cluster of 8 CTAs (dense K = 1,
                                n <= 2048): the lowest latency per anneal. The reference's engine keeps one anneal on
-                               an 8-CTA cluster too (gpu/onsager_v2_20261007/src/sca_gpu.cu:223-295); AUTO picks it
-                               for up to three waves of co-resident clusters */
+                               an 8-CTA cluster too (gpu/onsager_v2_20261007/src/sca_gpu.cu:223-295) */
 
 #define ANC_TENSOR_AUTO 0   /* fp4 when exact for the instance (NP = 2048, |J| <= 1, small fields), else int8 */
 #define ANC_TENSOR_INT8 1   /* tcgen05.mma kind::i8, int32 accumulation (any K) */
@@ -114,8 +113,24 @@ typedef struct {
     int threads;     /* host threads for rescoring; 0 = default */
     int profile;     /* 1: record per-phase cycle counters of the tensor engine (anc_last_profile) */
     int tensor_kind; /* ANC_TENSOR_*: operand format of the tensor engine's field update */
-    int reserved[3];
+    int flip_permille; /* AUTO's flip fraction (flips per spin per step) x 1000; 0 = the fraction the last anc_run /
+                          anc_run_fields of these tables on this instance saw, else 0.25 */
+    int reserved[2];
 } anc_run_opts;
+
+/* No counterpart in the reference (its CLI has one engine). The cost model behind ANC_ENGINE_AUTO, host-only: the
+ * estimated device time in microseconds of nchains anneals of S steps on each engine, for n spins with kbits-bit dense
+ * couplings (0 = sparse rows), flip fraction phi (mean flips per spin per step), fp4 = whether the tensor engine would
+ * run its fp4 kernel, and per_wave[e] = the anneals engine e advances at once on the device (0 = unavailable; index
+ * ANC_ENGINE_*, entry 0 unused). Writes us[ANC_ENGINE_PLAIN / _TENSOR / _CLUSTER] (-1 = unavailable) and returns the
+ * engine with the least estimate. Per-step costs are fitted to B200 measurements (anc_api.cu). */
+ANC_API int anc_auto_estimate(int n, int kbits, int nchains, int S, double phi, int fp4, const int* per_wave,
+                              double* us);
+
+/* The engine AUTO would pick for anc_run(inst, tb, ..., nchains, opts), with the inputs it used: us[4] as above,
+ * per_wave[4] queried on the current device, phi the flip fraction assumed. Any output may be NULL. */
+ANC_API int anc_auto_choice(anc_instance* inst, anc_tables* tb, int nchains, const anc_run_opts* opts, double* us,
+                            int* per_wave, double* phi);
 
 /* Phase profile of the calling thread's last synchronous tensor-engine run with opts.profile = 1 (the counterpart
  * of the reference's SCA_PROFILE build, sca_gpu.cu:163-168): out[0..8] = mean SM cycles per step of
