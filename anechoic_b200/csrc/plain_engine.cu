@@ -76,6 +76,53 @@ __device__ __forceinline__ void append_flip(bool flag, int i, uint32_t neg, uint
     if (flag) flist[base + __popc(b & lanemask_lt())] = uint32_t(i) | (neg << 31);
 }
 
+// The flip list of a step, built after the decisions from the flip words Dw (bit set = slot flipped this step) and the
+// new spin words Sw: a block-wide exclusive scan of the words' popcounts places each word's flips, in slot order, at
+// its offset; entry = slot | (new spin -1) << 31. The deciding warps thus write only two words per round and take no
+// shared-memory atomic. Called by every thread; returns the list's length; ends with a CTA barrier.
+__device__ __forceinline__ int build_flip_list(const uint32_t* Sw, const uint32_t* Dw, int nw, uint32_t* flist,
+                                               int* s_wsum) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    // each thread takes cb consecutive slots: 4, 8 or 16 bits of one word while the words are few (NP <= 8192),
+    // else whole words
+    int cb = 32;
+    if (32 * nw <= 16 * T) {
+        cb = 4;
+        while (cb * T < 32 * nw) cb <<= 1;
+    }
+    const int per = cb < 32 ? 1 : (nw + T - 1) / T;
+    const int w0 = cb < 32 ? min((tid * cb) >> 5, nw) : min(tid * per, nw), w1 = min(w0 + per, nw);
+    const uint32_t part = cb < 32 ? (((1u << cb) - 1u) << ((tid * cb) & 31)) : FULL;
+    int c = 0;
+    for (int w = w0; w < w1; ++w) c += __popc(Dw[w] & part);
+    int incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += v;
+    }
+    if (lane == 31) s_wsum[warp] = incl;
+    __syncthreads();
+    int pos = incl - c, total = 0;
+#pragma unroll
+    for (int j = 0; j < T / 32; ++j) {
+        const int v = s_wsum[j];
+        pos += j < warp ? v : 0;
+        total += v;
+    }
+    for (int w = w0; w < w1; ++w) {
+        uint32_t d = Dw[w] & part;
+        const uint32_t up = Sw[w];
+        while (d) {
+            const int bit = __ffs(d) - 1;
+            d &= d - 1;
+            flist[pos++] = uint32_t(32 * w + bit) | (((up >> bit) & 1u) ? 0u : 0x80000000u);
+        }
+    }
+    __syncthreads();
+    return total;
+}
+
 __device__ __forceinline__ int64_t warp_sum64(int64_t v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
@@ -213,6 +260,53 @@ __device__ __forceinline__ void dense_pass(const uint32_t* __restrict__ planes, 
     }
 }
 
+// Lanes per flipped row in sparse_pass: the power of two nearest above the rows' mean degree, at most 32 (log2).
+__device__ __forceinline__ int sparse_lanes_log2(int nnz, int n) {
+    const int deg = (nnz + n - 1) / max(n, 1);
+    int lg = 0;
+    while (lg < 5 && (1 << lg) < deg) ++lg;
+    return lg;
+}
+
+// Sparse field pass: h_y += m J_xy over the CSR rows x of the nf flipped slots in flist (m = mult with the sign of
+// the new spin). Groups of 2^lg lanes take one row each, and each group first fetches the bounds of kSparseBatch rows
+// and the first edge of each, so a warp keeps 32 / 2^lg * kSparseBatch row fetches in flight where a loop over rows
+// would keep one: the pass is bound by L2 latency, not bandwidth. Integer adds in any order: bit-exact.
+constexpr int kSparseBatch = 4;
+__device__ __forceinline__ void sparse_pass(const int32_t* __restrict__ row_ptr, const uint32_t* __restrict__ adj,
+                                            const uint32_t* flist, int nf, int lg, int32_t* h, int mult) {
+    const int G = 1 << lg, sub = threadIdx.x & (G - 1), NG = T >> lg;
+    for (int f0 = threadIdx.x >> lg; f0 < nf; f0 += NG * kSparseBatch) {
+        int k0[kSparseBatch], k1[kSparseBatch];
+        int32_t m[kSparseBatch];
+        uint32_t a0[kSparseBatch];
+#pragma unroll
+        for (int b = 0; b < kSparseBatch; ++b) {
+            const int f = f0 + b * NG;
+            k0[b] = 0;
+            k1[b] = 0;
+            m[b] = 0;
+            if (f < nf) {
+                const uint32_t e = flist[f];
+                const int x = int(e & 0x7fffffffu);
+                m[b] = (e >> 31) ? -mult : mult;
+                k0[b] = __ldg(row_ptr + x) + sub;
+                k1[b] = __ldg(row_ptr + x + 1);
+            }
+        }
+#pragma unroll
+        for (int b = 0; b < kSparseBatch; ++b) a0[b] = k0[b] < k1[b] ? __ldg(adj + k0[b]) : 0u;
+#pragma unroll
+        for (int b = 0; b < kSparseBatch; ++b) {
+            if (k0[b] < k1[b]) atomicAdd(&h[a0[b] >> 8], m[b] * int32_t(int8_t(a0[b] & 0xffu)));
+            for (int k = k0[b] + G; k < k1[b]; k += G) {
+                const uint32_t a = __ldg(adj + k);
+                atomicAdd(&h[a >> 8], m[b] * int32_t(int8_t(a & 0xffu)));
+            }
+        }
+    }
+}
+
 // Field change of slot (wi, lane) from the last dense pass: sum_{x in F} s'_x J_xy, with the K = 1 diagonal and
 // membership corrections (in_f: y was in the pass's F; s_up: y's current spin is +1).
 template <int K, int P>
@@ -238,7 +332,7 @@ __device__ __forceinline__ int32_t dense_delta(const uint32_t* res, int nwj, int
 template <int K, int P, bool SPARSE, bool STREAM>
 __global__ void __launch_bounds__(T, 1) plain_kernel(const __grid_constant__ PlainLaunch L) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
-    __shared__ int s_item, s_nf[2], s_lin[8];
+    __shared__ int s_item, s_nf, s_lin[8], s_wsum[T / 32];
     __shared__ long long s_red[2][16];
     int32_t* h = reinterpret_cast<int32_t*>(smem_raw);
     uint32_t* flist = reinterpret_cast<uint32_t*>(h + L.np_max);
@@ -271,7 +365,7 @@ __global__ void __launch_bounds__(T, 1) plain_kernel(const __grid_constant__ Pla
         int32_t* trace_out = (job.trace && job.out_trace) ? job.out_trace + size_t(c) * S : nullptr;
 
         for (int i = tid; i < np; i += T) h[i] = (i < n && bias) ? bias[i] : 0;
-        if (tid == 0) { s_nf[0] = 0; s_nf[1] = 0; }
+        if (tid == 0) s_nf = 0;
         __syncthreads();
 
         // seed, initial spins (draw >> 31; padding +1), s_prev = +1 everywhere, initial flip list = all active slots
@@ -286,23 +380,16 @@ __global__ void __launch_bounds__(T, 1) plain_kernel(const __grid_constant__ Pla
                 const uint32_t sw = __ballot_sync(FULL, sbit != 0);
                 const uint32_t dw = __ballot_sync(FULL, valid && !sbit);
                 if (lane == 0) { Sw[k * 8 + warp] = sw; Dw[k * 8 + warp] = dw; }
-                append_flip(valid, i, sbit ^ 1u, flist, &s_nf[0], lane);
+                append_flip(valid, i, sbit ^ 1u, flist, &s_nf, lane);
             }
         }
         __syncthreads();
-        int pass_nf = s_nf[0];
+        int pass_nf = s_nf;
         int pass_mult = 1;
         bool pass_init = true, pass_pending = false;
+        const int sparse_lg = SPARSE ? sparse_lanes_log2(__ldg(job.row_ptr + n), n) : 0;
         if (SPARSE) {
-            for (int f = warp; f < pass_nf; f += T / 32) {
-                const uint32_t e = flist[f];
-                const int x = int(e & 0x7fffffffu);
-                const int32_t m = (e >> 31) ? -1 : 1;
-                for (int k = job.row_ptr[x] + lane; k < job.row_ptr[x + 1]; k += 32) {
-                    const uint32_t a = __ldg(job.adj + k);
-                    atomicAdd(&h[a >> 8], m * int32_t(int8_t(a & 0xffu)));
-                }
-            }
+            sparse_pass(job.row_ptr, job.adj, flist, pass_nf, sparse_lg, h, 1);
         } else {
             dense_pass<K, P, STREAM>(planes, plane_stride, nwj, pass_nf, flist, comb, res, h, n, 1);
             pass_pending = !STREAM;
@@ -312,8 +399,6 @@ __global__ void __launch_bounds__(T, 1) plain_kernel(const __grid_constant__ Pla
         int32_t nlin_prev = 0;
         long long flips = 0;
         for (int t = 0; t < S; ++t) {
-            const int buf = (t + 1) & 1;
-            if (tid == 0) s_nf[t & 1] = 0;   // buffer of step t-1 (or of the initial pass); step t appends to buf
             if (decider) {
                 const int32_t fourT = __ldg(fourT_t + t), twoT = fourT >> 1, qv = __ldg(q_t + t);
                 const int32_t corr = step_corr(nlin_prev, __ldg(kcorr_t + t), __ldg(kconst_t + t));
@@ -340,12 +425,11 @@ __global__ void __launch_bounds__(T, 1) plain_kernel(const __grid_constant__ Pla
                     const uint32_t fb = __ballot_sync(FULL, fl);
                     nl += __popc(__ballot_sync(FULL, ln));
                     if (lane == 0) { Sw[wi] = Sword ^ fb; Dw[wi] = fb; }
-                    append_flip(fl, i, s_up ? 1u : 0u, flist, &s_nf[buf], lane);
                 }
                 if (lane == 0) s_lin[warp] = nl;
             }
             __syncthreads();
-            const int nf = s_nf[buf];
+            const int nf = build_flip_list(Sw, Dw, nw, flist, s_wsum);
             int32_t nlin = 0;
 #pragma unroll
             for (int w = 0; w < 8; ++w) nlin += s_lin[w];
@@ -360,15 +444,7 @@ __global__ void __launch_bounds__(T, 1) plain_kernel(const __grid_constant__ Pla
             pass_pending = false;
             if (nf > 0) {
                 if (SPARSE) {
-                    for (int f = warp; f < nf; f += T / 32) {
-                        const uint32_t e = flist[f];
-                        const int x = int(e & 0x7fffffffu);
-                        const int32_t m = (e >> 31) ? -2 : 2;
-                        for (int k = job.row_ptr[x] + lane; k < job.row_ptr[x + 1]; k += 32) {
-                            const uint32_t a = __ldg(job.adj + k);
-                            atomicAdd(&h[a >> 8], m * int32_t(int8_t(a & 0xffu)));
-                        }
-                    }
+                    sparse_pass(job.row_ptr, job.adj, flist, nf, sparse_lg, h, 2);
                 } else {
                     dense_pass<K, P, STREAM>(planes, plane_stride, nwj, nf, flist, comb, res, h, n, 2);
                     pass_pending = !STREAM;
