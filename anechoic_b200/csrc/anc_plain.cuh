@@ -14,9 +14,9 @@
 //      extracts y's count at the start of the next step, when it reads h_y. When the counters of all 2(K-1)
 //      sign/magnitude sets do not fit in shared memory (N = 16384, K = 4), each set is added into the fields as soon
 //      as it is complete (streaming layout, one result buffer).
-//      Sparse couplings (CSR rows) are scattered with shared-memory atomics: a group of lanes (the rows' mean degree,
-//      rounded up to a power of two) per flipped row, each group fetching several rows' bounds and first edges
-//      before it applies any, so many L2 fetches are in flight per warp.
+//      Sparse couplings (CSR rows) are scattered with shared-memory atomics: a group of lanes per flipped row (an
+//      eighth of the rows' mean degree, rounded up to a power of two), each lane fetching up to 8 edges before it
+//      applies any, so many L2 fetches are in flight per warp.
 //   The initial field h = b + J s0 reuses step 2 with F = all active slots and factor 1.
 // All arithmetic is integer and order-independent, so the result is bit-exact with the golden model.
 #pragma once

@@ -260,26 +260,37 @@ __device__ __forceinline__ void dense_pass(const uint32_t* __restrict__ planes, 
     }
 }
 
-// Lanes per flipped row in sparse_pass: the power of two nearest above the rows' mean degree, at most 32 (log2).
+// Sparse field pass: h_y += m J_xy over the CSR rows x of the nf flipped slots in flist (m = mult with the sign of
+// the new spin). Groups of 2^lg lanes take one row each, with lanes enough for the rows' mean degree at kSparseEdges
+// edges per lane. Each group first fetches the bounds of kSparseBatch rows, then kSparseEdges edges per lane of each,
+// and only then applies them, so a warp keeps 32 / 2^lg * kSparseBatch rows and kSparseEdges * kSparseBatch edge
+// fetches per lane in flight where a loop over rows would keep one: the pass is bound by L2 latency, not bandwidth.
+// Integer adds in any order: bit-exact. On a B200, over the 51-instance sparse batch (degrees 4 ... 48), one row per
+// group with 8 edges per lane took 134 ms per launch; 4 rows x 2 edges 208 ms; a warp per row, one row at a time,
+// 393 ms.
+#ifndef ANC_SPARSE_BATCH
+#define ANC_SPARSE_BATCH 1
+#endif
+#ifndef ANC_SPARSE_EDGES
+#define ANC_SPARSE_EDGES 8
+#endif
+constexpr int kSparseBatch = ANC_SPARSE_BATCH, kSparseEdges = ANC_SPARSE_EDGES;
+
+// log2 of the lanes per row: the power of two at or above mean degree / kSparseEdges, at most 32.
 __device__ __forceinline__ int sparse_lanes_log2(int nnz, int n) {
-    const int deg = (nnz + n - 1) / max(n, 1);
+    const int deg = (nnz + kSparseEdges * n - 1) / (kSparseEdges * max(n, 1));
     int lg = 0;
     while (lg < 5 && (1 << lg) < deg) ++lg;
     return lg;
 }
 
-// Sparse field pass: h_y += m J_xy over the CSR rows x of the nf flipped slots in flist (m = mult with the sign of
-// the new spin). Groups of 2^lg lanes take one row each, and each group first fetches the bounds of kSparseBatch rows
-// and the first edge of each, so a warp keeps 32 / 2^lg * kSparseBatch row fetches in flight where a loop over rows
-// would keep one: the pass is bound by L2 latency, not bandwidth. Integer adds in any order: bit-exact.
-constexpr int kSparseBatch = 4;
 __device__ __forceinline__ void sparse_pass(const int32_t* __restrict__ row_ptr, const uint32_t* __restrict__ adj,
                                             const uint32_t* flist, int nf, int lg, int32_t* h, int mult) {
     const int G = 1 << lg, sub = threadIdx.x & (G - 1), NG = T >> lg;
     for (int f0 = threadIdx.x >> lg; f0 < nf; f0 += NG * kSparseBatch) {
         int k0[kSparseBatch], k1[kSparseBatch];
         int32_t m[kSparseBatch];
-        uint32_t a0[kSparseBatch];
+        uint32_t a[kSparseBatch][kSparseEdges];
 #pragma unroll
         for (int b = 0; b < kSparseBatch; ++b) {
             const int f = f0 + b * NG;
@@ -295,20 +306,22 @@ __device__ __forceinline__ void sparse_pass(const int32_t* __restrict__ row_ptr,
             }
         }
 #pragma unroll
-        for (int b = 0; b < kSparseBatch; ++b) a0[b] = k0[b] < k1[b] ? __ldg(adj + k0[b]) : 0u;
+        for (int b = 0; b < kSparseBatch; ++b)
+#pragma unroll
+            for (int e = 0; e < kSparseEdges; ++e) a[b][e] = k0[b] + e * G < k1[b] ? __ldg(adj + k0[b] + e * G) : 0u;
 #pragma unroll
         for (int b = 0; b < kSparseBatch; ++b) {
-            if (k0[b] < k1[b]) atomicAdd(&h[a0[b] >> 8], m[b] * int32_t(int8_t(a0[b] & 0xffu)));
-            for (int k = k0[b] + G; k < k1[b]; k += G) {
-                const uint32_t a = __ldg(adj + k);
-                atomicAdd(&h[a >> 8], m[b] * int32_t(int8_t(a & 0xffu)));
+#pragma unroll
+            for (int e = 0; e < kSparseEdges; ++e)
+                if (k0[b] + e * G < k1[b]) atomicAdd(&h[a[b][e] >> 8], m[b] * int32_t(int8_t(a[b][e] & 0xffu)));
+            for (int k = k0[b] + kSparseEdges * G; k < k1[b]; k += G) {
+                const uint32_t v = __ldg(adj + k);
+                atomicAdd(&h[v >> 8], m[b] * int32_t(int8_t(v & 0xffu)));
             }
         }
     }
 }
 
-// Field change of slot (wi, lane) from the last dense pass: sum_{x in F} s'_x J_xy, with the K = 1 diagonal and
-// membership corrections (in_f: y was in the pass's F; s_up: y's current spin is +1).
 template <int K, int P>
 __device__ __forceinline__ int32_t dense_delta(const uint32_t* res, int nwj, int wi, int lane, int nfp, bool in_f,
                                                bool s_up) {
