@@ -154,34 +154,61 @@ __device__ __forceinline__ void dense_pass(const uint32_t* __restrict__ planes, 
         BitCounter<P> cnt[NC];
 #pragma unroll
         for (int cc = 0; cc < NC; ++cc) cnt[cc].clear();
-        if (active) {
-            for (int f0 = g; f0 < nf; f0 += 8 * G) {
-                uint32_t a[NC][8];
+        if (active && K <= 1) {
+            // one plane: the next 8 rows are fetched before the current 8 are counted, so the counting overlaps
+            // the L2 latency of the fetches
+            uint32_t cur[8], nxt[8];
+            auto load8 = [&](int fb, uint32_t (&a)[8]) {
 #pragma unroll
                 for (int j = 0; j < 8; ++j) {
-                    const int f = f0 + j * G;
+                    const int f = fb + j * G;
+                    uint32_t v = 0u;
+                    if (f < nf) {
+                        const uint32_t e = flist[f];
+                        v = __ldg(planes + size_t(e & 0x7fffffffu) * nwj + w) ^ ((e >> 31) ? FULL : 0u);
+                    }
+                    a[j] = v;
+                }
+            };
+            if (g < nf) load8(g, nxt);
+            for (int f0 = g; f0 < nf; f0 += 8 * G) {
+#pragma unroll
+                for (int j = 0; j < 8; ++j) cur[j] = nxt[j];
+                if (f0 + 8 * G < nf) load8(f0 + 8 * G, nxt);
+                cnt[0].add8(cur);
+            }
+        } else if (active) {
+            constexpr int RB = 1;
+            for (int f0 = g; f0 < nf; f0 += 8 * RB * G) {
+                uint32_t a[RB][NC][8];
+#pragma unroll
+                for (int jj = 0; jj < 8 * RB; ++jj) {
+                    const int j = jj & 7, rb = jj >> 3;
+                    const int f = f0 + jj * G;
                     if (f < nf) {
                         const uint32_t e = flist[f];
                         const uint32_t neg = (e >> 31) ? FULL : 0u;
                         const uint32_t* row = planes + size_t(e & 0x7fffffffu) * nwj + w;
                         if (K <= 1) {
-                            a[0][j] = __ldg(row) ^ neg;
+                            a[rb][0][j] = __ldg(row) ^ neg;
                         } else {
                             const uint32_t t = __ldg(row) ^ neg;   // 1 where s'_x * sign(J_xy) = -1
 #pragma unroll
                             for (int b = 1; b < (K <= 1 ? 2 : K); ++b) {
                                 const uint32_t m = __ldg(row + size_t(b) * plane_stride);
-                                a[2 * (b - 1)][j] = m & ~t;
-                                a[2 * (b - 1) + 1][j] = m & t;
+                                a[rb][2 * (b - 1)][j] = m & ~t;
+                                a[rb][2 * (b - 1) + 1][j] = m & t;
                             }
                         }
                     } else {
 #pragma unroll
-                        for (int cc = 0; cc < NC; ++cc) a[cc][j] = 0u;
+                        for (int cc = 0; cc < NC; ++cc) a[rb][cc][j] = 0u;
                     }
                 }
 #pragma unroll
-                for (int cc = 0; cc < NC; ++cc) cnt[cc].add8(a[cc]);
+                for (int rb = 0; rb < RB; ++rb)
+#pragma unroll
+                    for (int cc = 0; cc < NC; ++cc) cnt[cc].add8(a[rb][cc]);
             }
         }
         if (G == 1) {
