@@ -982,8 +982,9 @@ int anc_run_batch(int njobs, const anc_job* jobs, const anc_run_opts* o) {
 }  // extern "C"
 
 // ---------------------------------------------------------------------------------------------------------------------
-// Allocation-free batch entry point (anc_run_batch_noalloc). Its scratch lives in one file-scope device array; host
-// staging uses file-scope arrays, so no call here allocates.
+// Allocation-free batch entry point (anc_run_batch_noalloc). Its scratch lives in one file-scope device array, and
+// the job table reaches it as the parameter block of a setup kernel, so no call here allocates or leaves a pointer to
+// host memory in the stream: a CUDA graph that captured a call replays it as it was.
 namespace {
 
 constexpr int kNaMaxJobs = ANC_NOALLOC_MAX_JOBS;
@@ -995,10 +996,31 @@ static_assert(kNaBytes <= ANC_NOALLOC_SCRATCH_BYTES, "scratch larger than the si
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaBytes];
 
-std::mutex g_na_mu;                       // guards the host staging arrays and the address table
+std::mutex g_na_mu;                       // guards the address table
 void* g_na_addr[256] = {};                // device address of g_noalloc_scratch, per device ordinal
-anc::PlainJob g_na_jobs[kNaMaxJobs];
-int2 g_na_items[kNaMaxAnneals];
+
+// One call's job table, passed by value to na_setup_kernel (sm_70+ kernels take parameter blocks up to 32764 bytes).
+// Jobs are ordered by kernel kind; job k owns work items [first[k], first[k + 1]).
+struct NaSetup {
+    int njobs, nitems;
+    int first[kNaMaxJobs + 1];
+    anc::PlainJob jobs[kNaMaxJobs];
+};
+static_assert(sizeof(NaSetup) <= 32764, "job table exceeds the kernel parameter limit");
+
+// Writes the job table into the scratch array and expands it into (job, anneal) work items.
+__global__ void na_setup_kernel(const __grid_constant__ NaSetup s, anc::PlainJob* jobs, int2* items) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < s.njobs) jobs[t] = s.jobs[t];
+    for (int i = t; i < s.nitems; i += gridDim.x * blockDim.x) {
+        int lo = 0, hi = s.njobs - 1;   // the last job with first[k] <= i
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (s.first[mid] <= i) lo = mid; else hi = mid - 1;
+        }
+        items[i] = make_int2(lo, i - s.first[lo]);
+    }
+}
 
 }  // namespace
 
@@ -1032,55 +1054,66 @@ extern "C" int anc_run_batch_noalloc(int njobs, const anc_device_job* jobs, void
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     uint8_t* base = static_cast<uint8_t*>(g_na_addr[dev]);
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    for (int k = 0; k < njobs; ++k) {
-        const anc_device_job& j = jobs[k];
-        anc::PlainJob& p = g_na_jobs[k];
-        p = anc::PlainJob{};
-        p.n = j.n;
-        p.np = pad_np(j.n);
-        p.nw = p.np / 32;
-        p.nwj = ((p.nw + 31) / 32) * 32;
-        p.K = j.kbits;
-        p.planes = j.planes;
-        p.row_ptr = j.row_ptr;
-        p.adj = j.adj;
-        p.bias = j.bias;
-        p.tab.fourT = j.fourT;
-        p.tab.q = j.q;
-        p.tab.kcorr = j.kcorr;
-        p.tab.kconst = j.kconst;
-        p.tab.S = j.S;
-        p.seed = j.seed;
-        p.trial_offset = j.trial_offset;
-        p.ntrials = j.nchains;
-        p.trace = j.trace != nullptr;
-        p.hclamp = j.hclamp;
-        p.out_spins = reinterpret_cast<uint32_t*>(j.spins);
-        p.out_sum_sh = j.sum_sh;
-        p.out_sum_bs = j.sum_bs;
-        p.out_flips = j.flips;
-        p.out_trace = j.trace;
-        p.out_h = nullptr;
-    }
-    CK(cudaMemcpyAsync(base + kNaJobsOff, g_na_jobs, sizeof(anc::PlainJob) * njobs, cudaMemcpyHostToDevice, st));
-    CK(cudaMemsetAsync(base, 0, 256, st));   // the counters must start at zero on every call
+    static thread_local NaSetup setup;   // 12 KB: kept off the stack
+    NaSetup& S = setup;
+    S.njobs = njobs;
     const int kinds[4] = {0, 1, 2, 4};
-    int item_off = 0;
+    int kind_first[5] = {0, 0, 0, 0, 0}, kind_np[4] = {0, 0, 0, 0}, kind_nwj[4] = {0, 0, 0, 0};
+    int slot = 0, items = 0;
+    for (int ki = 0; ki < 4; ++ki) {
+        kind_first[ki] = items;
+        for (int k = 0; k < njobs; ++k) {
+            const anc_device_job& j = jobs[k];
+            if (j.kbits != kinds[ki]) continue;
+            anc::PlainJob& p = S.jobs[slot];
+            p = anc::PlainJob{};
+            p.n = j.n;
+            p.np = pad_np(j.n);
+            p.nw = p.np / 32;
+            p.nwj = ((p.nw + 31) / 32) * 32;
+            p.K = j.kbits;
+            p.planes = j.planes;
+            p.row_ptr = j.row_ptr;
+            p.adj = j.adj;
+            p.bias = j.bias;
+            p.tab.fourT = j.fourT;
+            p.tab.q = j.q;
+            p.tab.kcorr = j.kcorr;
+            p.tab.kconst = j.kconst;
+            p.tab.S = j.S;
+            p.seed = j.seed;
+            p.trial_offset = j.trial_offset;
+            p.ntrials = j.nchains;
+            p.trace = j.trace != nullptr;
+            p.hclamp = j.hclamp;
+            p.out_spins = reinterpret_cast<uint32_t*>(j.spins);
+            p.out_sum_sh = j.sum_sh;
+            p.out_sum_bs = j.sum_bs;
+            p.out_flips = j.flips;
+            p.out_trace = j.trace;
+            p.out_h = nullptr;
+            kind_np[ki] = std::max(kind_np[ki], p.np);
+            kind_nwj[ki] = std::max(kind_nwj[ki], p.K == 0 ? p.nw : p.nwj);
+            S.first[slot++] = items;
+            items += j.nchains;
+        }
+    }
+    kind_first[4] = items;
+    S.first[njobs] = items;
+    S.nitems = items;
+    auto* d_jobs = reinterpret_cast<anc::PlainJob*>(base + kNaJobsOff);
+    auto* d_items = reinterpret_cast<int2*>(base + kNaItemsOff);
+    na_setup_kernel<<<(items + 255) / 256, 256, 0, st>>>(S, d_jobs, d_items);
+    CK(cudaGetLastError());
+    CK(cudaMemsetAsync(base, 0, 256, st));   // the counters must start at zero on every call
     for (int ki = 0; ki < 4; ++ki) {
         const int K = kinds[ki];
-        int cnt = 0, np_max = 0, nwj_max = 0;
-        for (int k = 0; k < njobs; ++k) {
-            if (g_na_jobs[k].K != K) continue;
-            np_max = std::max(np_max, g_na_jobs[k].np);
-            nwj_max = std::max(nwj_max, K == 0 ? g_na_jobs[k].nw : g_na_jobs[k].nwj);
-            for (int c = 0; c < jobs[k].nchains; ++c) g_na_items[item_off + cnt++] = make_int2(k, c);
-        }
+        const int cnt = kind_first[ki + 1] - kind_first[ki], item_off = kind_first[ki];
+        const int np_max = kind_np[ki], nwj_max = kind_nwj[ki];
         if (!cnt) continue;
-        CK(cudaMemcpyAsync(base + kNaItemsOff + size_t(item_off) * sizeof(int2), g_na_items + item_off,
-                           size_t(cnt) * sizeof(int2), cudaMemcpyHostToDevice, st));
         anc::PlainLaunch L{};
-        L.jobs = reinterpret_cast<const anc::PlainJob*>(base + kNaJobsOff);
-        L.items = reinterpret_cast<const int2*>(base + kNaItemsOff) + item_off;
+        L.jobs = d_jobs;
+        L.items = d_items + item_off;
         L.nitems = cnt;
         L.next_item = reinterpret_cast<int*>(base) + ki;
         L.np_max = np_max;
@@ -1096,7 +1129,6 @@ extern "C" int anc_run_batch_noalloc(int njobs, const anc_device_job* jobs, void
         if (per_sm < 1) return fail(ANC_EINVAL, "plain engine cannot be resident");
         rc = anc::plain_launch(L, K, P, std::max(1, std::min(cnt, per_sm * sms)), smem, st);
         if (rc) return cuda_fail(cudaError_t(rc), "plain engine launch");
-        item_off += cnt;
     }
     return ANC_OK;
 }

@@ -193,7 +193,9 @@ ANC_API int anc_run_batch(int njobs, const anc_job* jobs, const anc_run_opts* op
  * holds until exit. The first call on a device looks that array up (cudaGetSymbolAddress) with the device current.
  * Limits: at most ANC_NOALLOC_MAX_JOBS jobs and ANC_NOALLOC_MAX_ANNEALS anneals (sum of nchains) per call; larger
  * requests return ANC_EINVAL. Every call reuses the same array and resets its counters: calls that overlap on the GPU
- * (different streams, or several host threads) race; calls in order on one stream do not.
+ * (different streams, or several host threads) race; calls in order on one stream do not. The job table travels as
+ * a kernel parameter block, so the call leaves no reference to host memory in the stream: it can be captured into a
+ * CUDA graph, and every replay runs the captured jobs.
  * Job layout:
  *   kbits 1/2/4: planes = [kbits][NP][NWJ] uint32 with NP = anc_np(n), NWJ = ceil(NP/32) rounded up to a multiple of
  *   32; word x*NWJ + y/32, bit y%32 of plane p describes J_xy: kbits 1 -> [J_xy = +1] (a +-1 complete graph);
