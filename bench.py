@@ -6,7 +6,9 @@ Workload (one "step" = one batch): the N = 2000 +-1 complete graph (J_xy = J_yx 
 lambda = 1.05 with ramp, reference default schedule t0 = 30, t1 = 5, q = 4, S = 1000 steps, seed 20261004.
 Target cut: 0.995 x the best cut of 1000 long anneals (S = 5000, same correction) of the same instance, run on the
 exact engine outside the timed region. TTS99: primary t_batch ln(0.01)/ln(1 - P_batch), secondary
-t_batch ln(0.01)/(B ln(1 - p)) (reference estimators, gpu/onsager_v2_20261007/src/analyze.py:15-47).
+t_batch ln(0.01)/(B ln(1 - p)) (reference estimators, gpu/onsager_v2_20261007/src/analyze.py:15-47). Outside the
+timed region the same schedule also runs at step budgets S = 100 ... 2000 ("tts99_by_budget": device time per batch,
+success probability and secondary TTS99 per budget).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--engine auto|plain|tensor|cluster] [--tensor-kind auto|int8|fp4]
                   [--impl ours|reference]
@@ -36,6 +38,7 @@ CHAINS = 1024
 SCHED = dict(S=1000, t0=30.0, t1=5.0, q=4.0, lam=1.05, ramp=True)
 TARGET_SCHED = dict(S=5000, t0=30.0, t1=5.0, q=4.0, lam=1.05, ramp=True)
 TARGET_ANNEALS = 1000
+BUDGETS = (100, 200, 500, 1000, 2000)   # the metric's step budgets (S) for the TTS99 sweep
 METRIC = "TTS99 (µs) to target cut and anneals/sec, batched vs plain engine, 1 B200"
 
 
@@ -114,6 +117,17 @@ def profile_traffic(kernel: str):
     return e.get("bytes_per_launch") if e else None
 
 
+def finite(obj):
+    """The JSON line holds no inf or nan (strict JSON): a non-finite number (e.g. TTS99 with no success) becomes null."""
+    if isinstance(obj, float):
+        return obj if math.isfinite(obj) else None
+    if isinstance(obj, dict):
+        return {k: finite(v) for k, v in obj.items()}
+    if isinstance(obj, (list, tuple)):
+        return [finite(v) for v in obj]
+    return obj
+
+
 def tts99(P: float, t: float) -> float:
     if P >= 1.0:
         return t
@@ -164,7 +178,7 @@ def bench_reference(args, ws, rank):
             "cpu_baseline": {"value": value, "unit": "anneals/s", "cores": cores, "kind": "reference",
                              "sample": f"{sample} anneals x {SCHED['S']} steps per step on {cores} threads"},
             "e2e": {"value": value, "unit": "anneals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(line))
+    print(json.dumps(finite(line)))
     return 0
 
 
@@ -318,6 +332,23 @@ def bench_ours(args, ws, rank, local):
                  "tts99_us_primary": 1000.0 * tts99(p_sb / (args.steps * ws), p_ms),
                  "tts99_us_secondary": 1000.0 * tts99_secondary(p_succ / (CHAINS * args.steps * ws), CHAINS, p_ms)}
 
+    # the metric's step budgets: the same schedule stretched to S = 100 ... 2000, two batches each, device-timed (the
+    # launch's CUDA events) and scored against the same target; secondary TTS99 per budget (outside the timed region)
+    budgets = {}
+    if not args.no_budget_sweep:
+        for Sb in BUDGETS:
+            tbb = A.Tables.from_schedule(A.Schedule(**dict(SCHED, S=Sb)))
+            A.run(dev, tbb, RUN_SEED, 0xD0000000, CHAINS, engine=engine, tensor_kind=kind)
+            bms, bs = [], 0
+            for k in range(2):
+                r = A.run(dev, tbb, RUN_SEED, 0xD0000000 + (k + 1) * CHAINS, CHAINS, engine=engine, tensor_kind=kind)
+                bms.append(r.device_ms)
+                bs += int((r.cuts(sumw) >= target).sum())
+            pb, tb_ms = bs / (2 * CHAINS), sum(bms) / len(bms)
+            tts = 1000.0 * tts99_secondary(pb, CHAINS, tb_ms)
+            budgets[str(Sb)] = {"ms_per_batch": tb_ms, "p": pb,
+                                "tts99_us_secondary": tts if math.isfinite(tts) else None}   # None: no success
+
     # e2e: the same batch through the public C ABI with host buffers -- schedule tables uploaded from host memory
     # and results (spins, sum s*h, sum b*s, flips) read back to host memory inside every timed step
     arrays = tb.arrays()
@@ -358,6 +389,7 @@ def bench_ours(args, ws, rank, local):
         "tts99_us": {"primary": 1000.0 * tts99(P_batch, t_batch_ms), "secondary": 1000.0 * tts99_secondary(p, B, t_batch_ms),
                      "target_cut": target, "best_cut": best, "p": p, "P_batch": P_batch, "t_batch_us": 1000 * t_batch_ms},
         "plain_engine": plain,
+        "tts99_by_budget": budgets or None,
         "us_per_anneal_step": 1000.0 * t_batch_ms / S, "ns_per_chain_step": 1e6 * t_batch_ms / (S * B),
         "ms_per_step_spread": [min(ms), max(ms)],
         "roofline": roofline(kernel, t_batch_ms, B, S, mean_flips, L.anc_np(N_SPINS)),
@@ -368,7 +400,7 @@ def bench_ours(args, ws, rank, local):
     }
     if ws == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample()
-    print(json.dumps(line))
+    print(json.dumps(finite(line)))
     if dist:
         dist.destroy_process_group()
     return 0
@@ -456,7 +488,7 @@ def bench_workload(args, ws, rank, local):
             "roofline": roof,
             "gpu_launches": args.steps, "clocks": clk.summary()}
     if rank == 0:
-        print(json.dumps(line))
+        print(json.dumps(finite(line)))
     return 0
 
 
@@ -470,6 +502,7 @@ def main():
     ap.add_argument("--tensor-kind", default="auto", choices=["auto", "int8", "fp4"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-engine comparison run")
+    ap.add_argument("--no-budget-sweep", action="store_true", help="skip the TTS99 sweep over step budgets")
     ap.add_argument("--workload", default="pm1", choices=["pm1", "sparse51", "dense16k"],
                     help="pm1: the headline line (default); the others print their own opt-in line")
     args = ap.parse_args()
