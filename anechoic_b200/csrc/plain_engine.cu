@@ -369,6 +369,19 @@ __device__ __forceinline__ int32_t dense_delta(const uint32_t* res, int nwj, int
     }
 }
 
+// Adds the counts of the dense pass just completed into the fields, on every thread (slots tid, tid + T, ...):
+// h_y += mult * dense_delta_y, with y's membership in the pass's F and its current spin from Dw / Sw. Running this
+// right after the pass, on all 512 threads, keeps the bit-plane reads out of the deciding warps' rounds.
+template <int K, int P>
+__device__ __forceinline__ void apply_dense(const uint32_t* res, int nwj, const uint32_t* Sw, const uint32_t* Dw,
+                                            int32_t* h, int n, int nf, bool init, int mult) {
+    for (int i = threadIdx.x; i < n; i += T) {
+        const int wi = i >> 5, lane = i & 31;
+        const bool s_up = (Sw[wi] >> lane) & 1u, dif = (Dw[wi] >> lane) & 1u;
+        h[i] += mult * dense_delta<K, P>(res, nwj, wi, lane, nf, init || dif, s_up);
+    }
+}
+
 template <int K, int P, bool SPARSE, bool STREAM>
 __global__ void __launch_bounds__(T, 1) plain_kernel(const __grid_constant__ PlainLaunch L) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
@@ -424,15 +437,16 @@ __global__ void __launch_bounds__(T, 1) plain_kernel(const __grid_constant__ Pla
             }
         }
         __syncthreads();
-        int pass_nf = s_nf;
-        int pass_mult = 1;
-        bool pass_init = true, pass_pending = false;
+        const int nf0 = s_nf;
         const int sparse_lg = SPARSE ? sparse_lanes_log2(__ldg(job.row_ptr + n), n) : 0;
         if (SPARSE) {
-            sparse_pass(job.row_ptr, job.adj, flist, pass_nf, sparse_lg, h, 1);
+            sparse_pass(job.row_ptr, job.adj, flist, nf0, sparse_lg, h, 1);
         } else {
-            dense_pass<K, P, STREAM>(planes, plane_stride, nwj, pass_nf, flist, comb, res, h, n, 1);
-            pass_pending = !STREAM;
+            dense_pass<K, P, STREAM>(planes, plane_stride, nwj, nf0, flist, comb, res, h, n, 1);
+            if (!STREAM) {
+                __syncthreads();
+                apply_dense<K, P>(res, nwj, Sw, Dw, h, n, nf0, true, 1);
+            }
         }
         __syncthreads();
 
@@ -450,11 +464,7 @@ __global__ void __launch_bounds__(T, 1) plain_kernel(const __grid_constant__ Pla
                     const bool valid = i < n;
                     const uint32_t Sword = Sw[wi], Dword = Dw[wi];
                     const bool s_up = (Sword >> lane) & 1u, dif = (Dword >> lane) & 1u;
-                    int32_t hv = h[i];
-                    if (!SPARSE && pass_pending) {
-                        hv += pass_mult * dense_delta<K, P>(res, nwj, wi, lane, pass_nf, pass_init || dif, s_up);
-                        if (valid) h[i] = hv;
-                    }
+                    const int32_t hv = h[i];
                     int32_t hs = s_up ? hv : -hv;
                     if (hclamp > 0) hs = max(-hclamp, min(hs, hclamp));
                     const int32_t x = qv + (dif ? corr : -corr);      // q - (s == s_prev ? corr : -corr)
@@ -478,29 +488,19 @@ __global__ void __launch_bounds__(T, 1) plain_kernel(const __grid_constant__ Pla
                 if (trace_out) trace_out[t] = nlin;
             }
             nlin_prev = nlin;
-            pass_nf = nf;
-            pass_mult = 2;
-            pass_init = false;
-            pass_pending = false;
             if (nf > 0) {
                 if (SPARSE) {
                     sparse_pass(job.row_ptr, job.adj, flist, nf, sparse_lg, h, 2);
                 } else {
                     dense_pass<K, P, STREAM>(planes, plane_stride, nwj, nf, flist, comb, res, h, n, 2);
-                    pass_pending = !STREAM;
+                    if (!STREAM) {
+                        __syncthreads();
+                        apply_dense<K, P>(res, nwj, Sw, Dw, h, n, nf, false, 2);
+                    }
                 }
             }
             __syncthreads();
         }
-        // apply the last pending dense pass
-        if (!SPARSE && pass_pending && decider) {
-            for (int k = 0; k < R; ++k) {
-                const int i = k * kLanes + tid, wi = k * 8 + warp;
-                const bool s_up = (Sw[wi] >> lane) & 1u, dif = (Dw[wi] >> lane) & 1u;
-                if (i < n) h[i] += pass_mult * dense_delta<K, P>(res, nwj, wi, lane, pass_nf, pass_init || dif, s_up);
-            }
-        }
-        __syncthreads();
         // outputs
         long long sh = 0, bs = 0;
         for (int i = tid; i < n; i += T) {
