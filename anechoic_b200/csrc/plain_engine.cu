@@ -16,8 +16,8 @@ struct BitCounter {
 #pragma unroll
         for (int p = 0; p < P; ++p) c[p] = 0;
     }
-    // add 8 words (Harley-Seal: 7 carry-save adders, then the weight-8 carry ripples upward while any lane has one)
-    __device__ __forceinline__ void add8(const uint32_t (&a)[8]) {
+    // 8 words into planes 0-2 (Harley-Seal: 7 carry-save adders); returns the weight-8 carry word
+    __device__ __forceinline__ uint32_t add8_low(const uint32_t (&a)[8]) {
         uint32_t t1a, t1b, t2a, t2b, t3;
         csa(c[0], t1a, c[0], a[0], a[1]);
         csa(c[0], t1b, c[0], a[2], a[3]);
@@ -26,13 +26,27 @@ struct BitCounter {
         csa(c[0], t1b, c[0], a[6], a[7]);
         csa(c[1], t2b, c[1], t1a, t1b);
         csa(c[2], t3, c[2], t2a, t2b);
+        return t3;
+    }
+    // a carry word of weight 2^p0 ripples upward while any lane has one
+    __device__ __forceinline__ void ripple(uint32_t t, int p0) {
 #pragma unroll
         for (int p = 3; p < P; ++p) {
-            if (!__any_sync(FULL, t3)) break;
-            const uint32_t k = c[p] & t3;
-            c[p] ^= t3;
-            t3 = k;
+            if (p < p0) continue;
+            if (!__any_sync(FULL, t)) break;
+            const uint32_t k = c[p] & t;
+            c[p] ^= t;
+            t = k;
         }
+    }
+    // add 8 words: the weight-8 carry ripples from plane 3
+    __device__ __forceinline__ void add8(const uint32_t (&a)[8]) { ripple(add8_low(a), 3); }
+    // two weight-8 carry words (of two add8_low calls) into plane 3; the weight-16 carry ripples from plane 4, so
+    // the vote-guarded ripple runs once per 16 words
+    __device__ __forceinline__ void add_w8_pair(uint32_t x, uint32_t y) {
+        uint32_t t4;
+        csa(c[3], t4, c[3], x, y);
+        ripple(t4, 4);
     }
     // c += other (ripple-carry over the planes; the total stays below 2^P by construction)
     __device__ __forceinline__ void add_planes(const uint32_t* o) {
@@ -171,11 +185,19 @@ __device__ __forceinline__ void dense_pass(const uint32_t* __restrict__ planes, 
                 }
             };
             if (g < nf) load8(g, nxt);
-            for (int f0 = g; f0 < nf; f0 += 8 * G) {
+            for (int f0 = g; f0 < nf; f0 += 16 * G) {   // 16 rows per iteration, the second 8 possibly empty
 #pragma unroll
                 for (int j = 0; j < 8; ++j) cur[j] = nxt[j];
                 if (f0 + 8 * G < nf) load8(f0 + 8 * G, nxt);
-                cnt[0].add8(cur);
+                const uint32_t w8a = cnt[0].add8_low(cur);
+                uint32_t w8b = 0u;
+                if (f0 + 8 * G < nf) {
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) cur[j] = nxt[j];
+                    if (f0 + 16 * G < nf) load8(f0 + 16 * G, nxt);
+                    w8b = cnt[0].add8_low(cur);
+                }
+                cnt[0].add_w8_pair(w8a, w8b);
             }
         } else if (active) {
             constexpr int RB = 1;
