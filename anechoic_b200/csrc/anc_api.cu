@@ -66,8 +66,9 @@ int pad_np(int n) { return std::max(2048, ((n + 255) / 256) * 256); }
 // span 0.05 ... 0.41.
 //   plain    a_K (NP / 2048)^1.5 + c_K phi n^2   a fixed part per step (decisions, n_lin, step barriers); then every
 //                                               flip rewrites n fields from one row of bit planes (K planes);
-//                                               a_1 = a_2 = 4.5, a_4 = 11.7, c_1 = 6.5e-6, c_2 = 1.65e-5, c_4 = 3.4e-5
-//   cluster  2.2 + 3.2 phi n / 2048              (1-bit couplings, NP = 2048: the rows split over 8 CTAs)
+//                                               a_1 = 3.4, a_2 = 5.1, a_4 = 10.2, c_1 = 5.4e-6, c_2 = 1.6e-5,
+//                                               c_4 = 3.3e-5 (least squares in log time over the one-wave launches)
+//   cluster  2.35 + 3.0 phi n / 2048             (1-bit couplings, NP = 2048: the rows split over 8 CTAs)
 //   tensor   a constant per kernel: the MMA chain and the decisions cost the same whatever flips: fp4 8.6 (9.2 with
 //            more than one replica group per wave), int8 22.7 at NP = 2048, 21.6 and 27.5 at NP = 3072 and 4096,
 //            streaming 98.5 (measured 98.6 at NP = 10240 and 98 at NP = 16384: bound by its step latency, not by
@@ -76,10 +77,9 @@ int pad_np(int n) { return std::max(2048, ((n + 255) / 256) * 256); }
 constexpr double kPhiPrior = 0.25;   // flip fraction assumed before any run of these tables on this instance
 
 double plain_step_us(int n, int K, double phi) {
-    const double np = double(pad_np(n)), a0 = 4.5 * std::pow(np / 2048.0, 1.5);
-    const double a = K == 4 ? 2.6 * a0 : a0;
-    const double c = K == 4 ? 3.4e-5 : K == 2 ? 1.65e-5 : 6.5e-6;
-    return a + c * phi * double(n) * double(n);
+    const double a = K == 4 ? 10.2 : K == 2 ? 5.1 : 3.4;
+    const double c = K == 4 ? 3.3e-5 : K == 2 ? 1.6e-5 : 5.4e-6;
+    return a * std::pow(double(pad_np(n)) / 2048.0, 1.5) + c * phi * double(n) * double(n);
 }
 
 double tensor_step_us(int n, bool fp4, int groups_per_wave) {
@@ -102,7 +102,7 @@ int estimate_engines(int n, int K, int nchains, int S, double phi, bool fp4, con
         us[ANC_ENGINE_TENSOR] = waves(ANC_ENGINE_TENSOR) * S * tensor_step_us(n, fp4, (groups + 127) / 128);
     }
     if (per_wave[ANC_ENGINE_CLUSTER] > 0)
-        us[ANC_ENGINE_CLUSTER] = waves(ANC_ENGINE_CLUSTER) * S * (2.2 + 3.2 * phi * double(n) / 2048.0);
+        us[ANC_ENGINE_CLUSTER] = waves(ANC_ENGINE_CLUSTER) * S * (2.35 + 3.0 * phi * double(n) / 2048.0);
     int best = ANC_ENGINE_PLAIN;
     for (int e : {ANC_ENGINE_PLAIN, ANC_ENGINE_TENSOR, ANC_ENGINE_CLUSTER})
         if (us[e] >= 0 && (us[best] < 0 || us[e] < us[best])) best = e;

