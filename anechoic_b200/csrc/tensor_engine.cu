@@ -967,19 +967,20 @@ __device__ __forceinline__ void cp_async_wait(int n) {
 // q .. q+7, by the 256 decision threads: warp w copies tile rows 16w .. 16w+15, its copy instruction c covering the
 // four whole 128-byte rows 16w + 4c .. 16w + 4c + 3 (lane: row + lane / 8, 16-byte chunk lane % 8), so each
 // instruction touches four cache lines. Copies are asynchronous,
-// one commit group per tile. Tiles 0-5 go out at once (the previous step's MMAs freed every stage before its fields
-// were ready); tiles 0-3 are marked full as they land, so that the MMAs which free the stages of tiles 6 and 7 run
-// meanwhile; then 6 and 7 go out and 4-7 are marked full in order. A tile is marked full once its group has
-// landed: the thread fences the async proxy and its warp arrives on the stage's barrier. Returns the replica's n_lin
-// (the sum of its 64 partial bytes) when want_nlin, else 0. ok (warp-uniform) is false once this warp saw an error;
-// every wait is bounded, and after an error the warp stops copying and arriving but still waits for the copies it
-// has in flight.
+// one commit group per tile. Ring position t holds K chunk (t + rot) mod 8, so a CTA starts with the tile holding its
+// own slice. Tile t goes out as soon as its two slices are published, and tile t - 1 is marked full right after, so
+// the MMAs start on the first tile while later slices are still being published (marking tiles 0-3 full only after
+// tiles 0-5 had gone out cost 6 % of the step). Tile 6 and 7 wait for the MMAs of tiles 0 and 1 to free their
+// stages; those tiles were marked full before. A tile is marked full once its group has landed: the thread fences the
+// async proxy and its warp arrives on the stage's barrier. Returns the replica's n_lin (the sum of its 64 partial
+// bytes) when want_nlin, else 0. ok (warp-uniform) is false once this warp saw an error; every wait is bounded, and
+// after an error the warp stops copying and arriving but still waits for the copies it has in flight.
 __device__ __forceinline__ int32_t f4_exchange(const F4Params& P, int g, int m, uint32_t stages_u32, uint32_t bar_full,
                                                uint32_t bar_empty, uint32_t q, int tid, int r, bool want_nlin,
-                                               const uint32_t* s_flag, uint32_t tbase, bool& ok, bool prof,
+                                               const uint32_t* s_flag, uint32_t tbase, int rot, bool& ok, bool prof,
                                                F4ExMarks& mk) {
     constexpr uint32_t TILE = kM * kKChunk;
-    static_assert(kF4Stages == 6 && kF4Tiles == 8, "the issue order below is written for 8 tiles on 6 stages");
+    static_assert(kF4Stages >= 2 && kF4Tiles == 8, "rotation by a 3-bit mask, and two stages in flight");
     const int lane = tid & 31;
     int* err = P.err;
     const int par = m & 1;
@@ -992,11 +993,12 @@ __device__ __forceinline__ int32_t f4_exchange(const F4Params& P, int g, int m, 
     // copy tile t into its stage once its slices are published (and, for t >= 6, its stage is free)
     auto issue = [&](int t) {
         const uint32_t qt = q + uint32_t(t), s = qt % kF4Stages, u = qt / kF4Stages;
+        const int tk = (t + rot) & (kF4Tiles - 1);     // K chunk of ring position t (the CTA's own tile first)
         if (ok && u >= 1) ok = __all_sync(0xffffffffu, mbar_wait(bar_empty + 8 * s, (u - 1) & 1u, err, kErrEmpty));
         if (ok) {
             // both slices published: every lane acquires the poller's mirror of their flags (cta scope; the poller
             // acquired them at gpu scope)
-            const uint32_t fa = smem_u32(s_flag + 2 * t), fb = smem_u32(s_flag + 2 * t + 1);
+            const uint32_t fa = smem_u32(s_flag + 2 * tk), fb = smem_u32(s_flag + 2 * tk + 1);
             const uint64_t t0 = globaltimer();
             bool seen = false;
             for (uint32_t k = 1;; ++k) {
@@ -1019,7 +1021,7 @@ __device__ __forceinline__ int32_t f4_exchange(const F4Params& P, int g, int m, 
             const uint32_t st = stages_u32 + s * TILE;
 #pragma unroll
             for (int c = 0; c < 4; ++c)
-                cp_async16(st + uint32_t(c * 512) + ((c & 1) ? dst1 : dst0), src + size_t(c) * 4096 + t * 128);
+                cp_async16(st + uint32_t(c * 512) + ((c & 1) ? dst1 : dst0), src + size_t(c) * 4096 + tk * 128);
         }
         cp_async_commit();          // one group per tile, empty when the copies were skipped
     };
@@ -1036,18 +1038,13 @@ __device__ __forceinline__ int32_t f4_exchange(const F4Params& P, int g, int m, 
             if (t == kF4Tiles - 1) mk.stored7 = clock64();
         }
     };
+    issue(0);
 #pragma unroll
-    for (int t = 0; t < 6; ++t) issue(t);
-    arrive(0, 5);
-    arrive(1, 4);
-    arrive(2, 3);
-    arrive(3, 2);
-    issue(6);
-    issue(7);
-    arrive(4, 3);
-    arrive(5, 2);
-    arrive(6, 1);
-    arrive(7, 0);
+    for (int t = 1; t < kF4Tiles; ++t) {
+        issue(t);
+        arrive(t - 1, 1);
+    }
+    arrive(kF4Tiles - 1, 0);
     int32_t nl = 0;
     if (ok && want_nlin) {
         // every warp saw all 16 flags before its last tile
@@ -1200,7 +1197,7 @@ __global__ void __launch_bounds__(kF4Threads, 1)
             const bool eok = !err_set(err);
             f4_draw(trng, pk);
             bool ok = __all_sync(0xffffffffu, eok);
-            int32_t nlin_next = f4_exchange(P, g, -1, smem_u32(stages), bar_full, bar_empty, q, tid, r, false, s_flag, tbase,
+            int32_t nlin_next = f4_exchange(P, g, -1, smem_u32(stages), bar_full, bar_empty, q, tid, r, false, s_flag, tbase, cs >> 1,
                                             ok, false, mk);
             q += kF4Tiles;
             const float hclf = float(P.hclamp);
@@ -1305,7 +1302,7 @@ __global__ void __launch_bounds__(kF4Threads, 1)
                 if (m + 1 < S) f4_draw(trng, pk);
                 ok = ok && __all_sync(0xffffffffu, eok2);
                 if (prof) { const long long t1 = clock64(); pd += t1 - t0; t0 = t1; }
-                nlin_next = f4_exchange(P, g, m, smem_u32(stages), bar_full, bar_empty, q, tid, r, true, s_flag, tbase,
+                nlin_next = f4_exchange(P, g, m, smem_u32(stages), bar_full, bar_empty, q, tid, r, true, s_flag, tbase, cs >> 1,
                                         ok, prof, mk);
                 q += kF4Tiles;
                 if (prof) {
@@ -1347,7 +1344,7 @@ __global__ void __launch_bounds__(kF4Threads, 1)
                         const long long i0 = prof ? clock64() : 0;
                         if (ok) {
                             const uint32_t a0 = smem_u32(stages + size_t(s) * TILE);
-                            const uint32_t b0 = smem_u32(jres + t * TILE);
+                            const uint32_t b0 = smem_u32(jres + ((t + (cs >> 1)) & (kF4Tiles - 1)) * TILE);
 #pragma unroll
                             for (int kk = 0; kk < kKChunk / 32; ++kk)
                                 mma_mxf4(tmem, sw128_desc(a0 + 32 * kk), sw128_desc(b0 + 32 * kk), IDESC_F4,
