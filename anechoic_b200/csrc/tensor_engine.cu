@@ -868,9 +868,10 @@ struct F4Params {
 };
 
 // The step's draws for the thread's eight RNG lanes (quarter e = jj / 4, lane j = jj % 4; 8 rounds each, every
-// lane's stream in round order), kept as their top 16 bits: pk[16e + 4j + k/2] holds column j*8 + k of quarter e in
-// its high half for even k and in its low half for odd k. The lane states live in TMEM (32 columns at taddr:
-// a, b, c, d of lanes jj = 0..7), loaded, advanced and stored back here.
+// lane's stream in round order), kept as their top 16 bits with the top bit flipped (u16 - 32768 as a signed
+// 16-bit value): pk[16e + 4j + k/2] holds column j*8 + k of quarter e in its high half for even k and in its low half
+// for odd k. The lane states live in TMEM (32 columns at taddr: a, b, c, d of lanes jj = 0..7), loaded, advanced and
+// stored back here.
 __device__ __forceinline__ void f4_draw(uint32_t taddr, uint32_t (&pk)[32]) {
     uint32_t st[32];
     tmem_ld32(taddr, st);
@@ -884,8 +885,8 @@ __device__ __forceinline__ void f4_draw(uint32_t taddr, uint32_t (&pk)[32]) {
         for (int jj = 0; jj < 8; ++jj) {
             const uint32_t u = rng_next(rng[jj]);
             uint32_t& w = pk[16 * (jj >> 2) + 4 * (jj & 3) + k / 2];
-            if (k & 1) w |= u >> 16;
-            else w = u & 0xffff0000u;
+            if (k & 1) w |= (u >> 16) ^ 0x8000u;
+            else w = (u & 0xffff0000u) ^ 0x80000000u;
         }
 #pragma unroll
     for (int jj = 0; jj < 8; ++jj) {
@@ -914,8 +915,8 @@ __device__ __forceinline__ void f4_decide(const uint32_t (&pk)[32], const uint32
     for (int col = 0; col < 32; ++col) {
         const int j = col >> 3, k = col & 7;
         const uint32_t w = pk[16 * E + 4 * j + k / 2];
-        const uint32_t u16 = (k & 1) ? (w << 16) : (w & 0xffff0000u);
-        const int32_t thr = __mulhi(int32_t(u16 ^ 0x80000000u), fourT);
+        const uint32_t a16 = (k & 1) ? (w << 16) : (w & 0xffff0000u);     // (u16 - 32768) << 16
+        const int32_t thr = __mulhi(int32_t(a16), fourT);
         float hsf = __uint_as_float(hv[col] ^ ((downs << (31 - col)) & 0x80000000u));
         if (CLAMP) hsf = fminf(fmaxf(hsf, -hclf), hclf);
         const int32_t zb = __float_as_int(hsf + 12582912.0f);
