@@ -315,8 +315,8 @@ __device__ __forceinline__ void dense_pass(const uint32_t* __restrict__ planes, 
 // and only then applies them, so a warp keeps 32 / 2^lg * kSparseBatch rows and kSparseEdges * kSparseBatch edge
 // fetches per lane in flight where a loop over rows would keep one: the pass is bound by L2 latency, not bandwidth.
 // Integer adds in any order: bit-exact. On a B200, over the 51-instance sparse batch (degrees 4 ... 48), one row per
-// group with 8 edges per lane took 134 ms per launch; 4 rows x 2 edges 208 ms; a warp per row, one row at a time,
-// 393 ms.
+// group with 8 edges per lane took 134 ms per launch and 4 rows x 2 edges 208 ms; a warp per row, one row at a time,
+// took 684 ms.
 #ifndef ANC_SPARSE_BATCH
 #define ANC_SPARSE_BATCH 1
 #endif
