@@ -599,7 +599,7 @@ __global__ void __cluster_dims__(kCR, 1, 1) __launch_bounds__(kCT, 1)
     uint32_t* recv = flist + 2048;                          // [2][kCR][kCW]
     uint32_t* comb = recv + 2 * kCR * kCW;                  // [8 warps][8 words][P]
     uint32_t* res = comb + 8 * 8 * P;                       // [8 words][P]
-    __shared__ int s_cnt[2];
+    __shared__ int s_cnt[kCT / 32];
     __shared__ long long s_part[kCR][2];                    // rank 0: every rank's sum of s*h and of b*s
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -675,10 +675,13 @@ __global__ void __cluster_dims__(kCR, 1, 1) __launch_bounds__(kCT, 1)
             for (int r = 0; r < kCR; ++r) cl_store(cl_map(local, uint32_t(r)), v);
         }
         cl_sync();
-        // the pass's flip list, the same in every CTA: word wi = k*8 + r (round k, source CTA r) holds slots 32 wi + b
-        if (tid < 64) {
-            const uint32_t* src = recv + (par * kCR + (tid & 7)) * kCW;
-            const uint32_t F = src[tid >> 3], N = src[8 + (tid >> 3)];
+        // the pass's flip list, the same in every CTA: word wi = k*8 + r (round k, source CTA r) holds slots 32 wi + b;
+        // thread tid places the flips of byte tid % 4 of word tid / 4, after a block-wide scan of the byte counts
+        int nf = 0;
+        {
+            const int wd = tid >> 2, sh = 8 * (tid & 3);
+            const uint32_t* src = recv + (par * kCR + (wd & 7)) * kCW;
+            const uint32_t F = (src[wd >> 3] >> sh) & 0xFFu, N = src[8 + (wd >> 3)] >> sh;
             const int cnt = __popc(F);
             int incl = cnt;
 #pragma unroll
@@ -687,18 +690,22 @@ __global__ void __cluster_dims__(kCR, 1, 1) __launch_bounds__(kCT, 1)
                 if (lane >= o) incl += y;
             }
             if (lane == 31) s_cnt[warp] = incl;
-            __syncwarp();
-            asm volatile("bar.sync 1, 64;" ::: "memory");
-            int pos = incl - cnt + (warp == 1 ? s_cnt[0] : 0);
+            __syncthreads();
+            int pos = incl - cnt;
+#pragma unroll
+            for (int w2 = 0; w2 < kCT / 32; ++w2) {
+                const int v = s_cnt[w2];
+                pos += w2 < warp ? v : 0;
+                nf += v;
+            }
             uint32_t m = F;
             while (m) {
                 const int b = __ffs(m) - 1;
                 m &= m - 1;
-                flist[pos++] = uint32_t(32 * tid + b) | (((N >> b) & 1u) << 31);
+                flist[pos++] = uint32_t(32 * wd + sh + b) | (((N >> b) & 1u) << 31);
             }
         }
         __syncthreads();
-        const int nf = s_cnt[0] + s_cnt[1];
         if (t >= 0) {
             int32_t nlin = 0;
 #pragma unroll
