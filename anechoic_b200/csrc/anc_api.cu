@@ -68,7 +68,7 @@ int pad_np(int n) { return std::max(2048, ((n + 255) / 256) * 256); }
 //                                               flip rewrites n fields from one row of bit planes (K planes);
 //                                               a_1 = 3.4, a_2 = 5.1, a_4 = 10.2, c_1 = 5.4e-6, c_2 = 1.6e-5,
 //                                               c_4 = 3.3e-5 (least squares in log time over the one-wave launches)
-//   cluster  2.35 + 3.0 phi n / 2048             (1-bit couplings, NP = 2048: the rows split over 8 CTAs)
+//   cluster  2.2 + 2.1 phi n / 2048              (1-bit couplings, NP = 2048: the rows split over 8 CTAs)
 //   tensor   a constant per kernel: the MMA chain and the decisions cost the same whatever flips: fp4 8.6 (9.2 with
 //            more than one replica group per wave), int8 22.7 at NP = 2048, 21.6 and 27.5 at NP = 3072 and 4096,
 //            streaming 98.5 (measured 98.6 at NP = 10240 and 98 at NP = 16384: bound by its step latency, not by
@@ -102,7 +102,7 @@ int estimate_engines(int n, int K, int nchains, int S, double phi, bool fp4, con
         us[ANC_ENGINE_TENSOR] = waves(ANC_ENGINE_TENSOR) * S * tensor_step_us(n, fp4, (groups + 127) / 128);
     }
     if (per_wave[ANC_ENGINE_CLUSTER] > 0)
-        us[ANC_ENGINE_CLUSTER] = waves(ANC_ENGINE_CLUSTER) * S * (2.35 + 3.0 * phi * double(n) / 2048.0);
+        us[ANC_ENGINE_CLUSTER] = waves(ANC_ENGINE_CLUSTER) * S * (2.2 + 2.1 * phi * double(n) / 2048.0);
     int best = ANC_ENGINE_PLAIN;
     for (int e : {ANC_ENGINE_PLAIN, ANC_ENGINE_TENSOR, ANC_ENGINE_CLUSTER})
         if (us[e] >= 0 && (us[best] < 0 || us[e] < us[best])) best = e;
