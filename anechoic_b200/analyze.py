@@ -33,13 +33,22 @@ def wilson(k: float, n: float):
     return (max(0.0, mid - rad), min(1.0, mid + rad))
 
 
+def _log1m(P: float) -> float:
+    """ln(1 - P), or None when it rounds to 0 (P within rounding of 0: the time to solution is then unbounded).
+    The reference's estimators divide by it and raise ZeroDivisionError there (e.g. the Wilson lower bound of a
+    cohort without successes); these return infinity instead."""
+    v = math.log(1.0 - P)
+    return v if v != 0.0 else None
+
+
 def tts99(P: float, t: float) -> float:
     """Time to solution at 99 % from a per-batch success probability P and batch time t."""
     if P >= 1.0:
         return t
     if P <= 0.0:
         return math.inf
-    return t * LN01 / math.log(1.0 - P)
+    d = _log1m(P)
+    return math.inf if d is None else t * LN01 / d
 
 
 def tts99_secondary(p: float, B: int, t: float) -> float:
@@ -48,7 +57,8 @@ def tts99_secondary(p: float, B: int, t: float) -> float:
         return math.inf
     if p >= 1.0:
         return 0.0
-    return t * LN01 / (B * math.log(1.0 - p))
+    d = _log1m(p)
+    return math.inf if d is None else t * LN01 / (B * d)
 
 
 def tts99_whole(P: float, t: float) -> float:
@@ -57,7 +67,8 @@ def tts99_whole(P: float, t: float) -> float:
         return t
     if P <= 0.0:
         return math.inf
-    return t * max(1, math.ceil(LN01 / math.log(1.0 - P)))
+    d = _log1m(P)
+    return math.inf if d is None else t * max(1, math.ceil(LN01 / d))
 
 
 def load_run(prefix: str):
@@ -69,7 +80,8 @@ def load_run(prefix: str):
 
 
 def estimate(prefix: str) -> dict:
-    """Estimators of one run from its files (the fields of the reference's estimate())."""
+    """Estimators of one run from its files: every field of the reference's estimate() under the same names
+    (analyze.py:56-80), plus t1, engine, kernel and n."""
     s, bat = load_run(prefix)
     B, nb = int(s["chains"]), len(bat)
     t = sum(b["device_ms"] for b in bat) / nb
@@ -79,8 +91,9 @@ def estimate(prefix: str) -> dict:
     nt = B * nb
     Pb, p = kb / nb, kt / nt
     Pb_ci, p_ci = wilson(kb, nb), wilson(kt, nt)
-    out = {k: s.get(k) for k in ("steps", "t0", "t1", "q", "lambda", "ramp", "tec_jv", "tecT_kappa", "trial_offset",
-                                  "engine", "kernel", "n")}
+    out = {k: s.get(k) for k in ("cs", "groups", "steps", "t0", "t1", "q", "ramp", "tec_jv", "trial_offset",
+                                  "engine", "kernel", "n", "gpu_before", "gpu_after")}
+    out.update(lam=s.get("lambda"), kappa=s.get("tecT_kappa"))
     out.update(prefix=os.path.basename(prefix), B=B, batches=nb, successes=kt, trials=nt, p=p, p_wilson95=list(p_ci),
                batches_with_success=kb, P_batch=Pb, P_batch_wilson95=list(Pb_ci), t_batch_ms=t,
                t_batch_min_ms=min(b["device_ms"] for b in bat), t_batch_max_ms=max(b["device_ms"] for b in bat),

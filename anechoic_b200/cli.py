@@ -6,7 +6,7 @@ so check_ref-style replays and the estimators (anechoic_b200.analyze) read them 
         --output PREFIX [--chains B] [--batches NB] [--seed S] [--offset O] [--trace 0|1]
         [--steps S --t0 T0 --t1 T1 --q Q --lambda L --tec-jv JV --tecT KAPPA --ramp]
         [--target CUT | --target-energy E] [--wide auto|0|1] [--check-fields 0|1] [--engine auto|plain|tensor|cluster]
-        [--warmup W] [--info]
+        [--tensor-kind auto|int8|fp4] [--warmup W] [--info]
 
 The reference's kernel-geometry flags (--cs, --groups, --clusters, --burn, --r, --preg) are accepted and recorded;
 the engines here pick their own geometry. --warmup W (default 1) runs W untimed launches first, on trial ids
@@ -39,7 +39,8 @@ GEOMETRY_FLAGS = ("--cs", "--groups", "--clusters", "--burn", "--r", "--preg")
 
 def parse(argv):
     o = dict(jkind=None, jpath=None, bias=None, kbits=0, output=None, chains=1024, batches=1, seed=20261004, offset=0,
-             trace=0, target=None, target_energy=None, wide="auto", check_fields=0, engine="auto", info=False,
+             trace=0, target=None, target_energy=None, wide="auto", check_fields=0, engine="auto", tensor_kind="auto",
+             info=False,
              warmup=1, geometry={})
     sc = Schedule()
     a = 0
@@ -78,6 +79,8 @@ def parse(argv):
             o["wide"] = v
         elif k == "--engine":
             o["engine"] = v
+        elif k == "--tensor-kind":
+            o["tensor_kind"] = v
         elif k in GEOMETRY_FLAGS:
             o["geometry"][k[2:]] = v
         else:
@@ -122,15 +125,17 @@ def main(argv=None) -> int:
         succ = batch_succ = mism = fmis_total = 0
         dms, hms = [], []
         kernel = None
+        gpu_before = gpu_status()
         for i in range(max(0, o["warmup"])):
-            run(dev, tb, o["seed"], 0xF0000000 + 65536 * i, B, engine=o["engine"], wide=wide)
+            run(dev, tb, o["seed"], 0xF0000000 + 65536 * i, B, engine=o["engine"], wide=wide,
+                tensor_kind=o["tensor_kind"])
         with open(out + ".trials.jsonl", "w") as ftr, open(out + ".batches.jsonl", "w") as fb, \
                 open(out + ".spins.bin", "wb") as fsp, (open(out + ".trace.bin", "wb") if o["trace"] else _Null()) as ftc:
             for b in range(nb):
                 off = o["offset"] + b * B
                 h0 = time.perf_counter()
                 r = run(dev, tb, o["seed"], off, B, trace=bool(o["trace"]), fields=bool(o["check_fields"]),
-                        engine=o["engine"], wide=wide)
+                        engine=o["engine"], wide=wide, tensor_kind=o["tensor_kind"])
                 h1 = time.perf_counter()
                 kernel = r.kernel
                 dms.append(r.device_ms)
@@ -168,19 +173,8 @@ def main(argv=None) -> int:
                 batch_succ += bs > 0
                 fb.write(json.dumps(dict(batch=b, chains=B, trial_offset=off, device_ms=r.device_ms,
                                          host_ms=hms[-1], successes=bs), separators=(",", ":")) + "\n")
-        t = sum(dms) / nb
-        p, Pb = succ / (B * nb), batch_succ / nb
-        summary = dict(device=_device_name(), n=inst.n, engine=o["engine"], kernel=kernel, geometry=o["geometry"],
-                       warmup=o["warmup"],
-                       chains=B, batches=nb, seed=o["seed"], trial_offset=o["offset"], steps=sc.S, t0=sc.t0, t1=sc.t1,
-                       q=sc.q, **{"lambda": sc.lam}, ramp=sc.ramp, tec_jv=sc.jv, tecT_kappa=sc.kappa, trace=o["trace"],
-                       target=target, target_energy=target_e, successes=succ, trials=B * nb, p=p,
-                       batches_with_success=batch_succ, P_batch=Pb, p_wilson95=list(analyze.wilson(succ, B * nb)),
-                       P_batch_wilson95=list(analyze.wilson(batch_succ, nb)), device_ms_mean=t,
-                       device_ms_min=min(dms), device_ms_max=max(dms), host_ms_mean=sum(hms) / nb,
-                       tts99_primary_ms=_finite(analyze.tts99(Pb, t)),
-                       tts99_secondary_ms=_finite(analyze.tts99_secondary(p, B, t)), cut_mismatches=mism,
-                       field_mismatches=fmis_total if o["check_fields"] else None)
+        summary = make_summary(o, sc, inst.n, kernel, succ, batch_succ, dms, hms, mism,
+                               fmis_total if o["check_fields"] else None, target, target_e, gpu_before)
         with open(out + ".summary.json", "w") as f:
             f.write(json.dumps(summary) + "\n")
         print(json.dumps(summary))
@@ -188,6 +182,50 @@ def main(argv=None) -> int:
     except (ValueError, OSError, _lib.AncError) as e:
         print("FAIL: " + str(e), file=sys.stderr)
         return 1
+
+
+def make_summary(o: dict, sc: Schedule, n: int, kernel, succ: int, batch_succ: int, dms, hms, mism: int,
+                 field_mismatches, target, target_e, gpu_before: str) -> dict:
+    """The PREFIX.summary.json record. It carries every field the reference's runner writes
+    (gpu/onsager_v2_20261007/src/sca_gpu.cu:769-781), so the reference's estimators (its analyze.py estimate(),
+    which reads cs, groups, chains, batches, successes, device_ms_min / _max, gpu_before / _after among others)
+    read this CLI's files unchanged. The reference's kernel-geometry flags (--cs, --groups, --clusters) are recorded
+    as given (null when absent): the engines here pick their own geometry."""
+    B, nb = o["chains"], o["batches"]
+    t = sum(dms) / nb
+    p, Pb = succ / (B * nb), batch_succ / nb
+    geo = o["geometry"]
+
+    def geo_int(k):
+        try:
+            return int(geo[k]) if k in geo else None
+        except ValueError:
+            return None
+
+    return dict(device=_device_name(), uuid=_device_uuid(), n=n, engine=o["engine"], kernel=kernel,
+                tensor_kind=o.get("tensor_kind", "auto"), geometry=geo, cs=geo_int("cs"), groups=geo_int("groups"),
+                clusters=geo_int("clusters"), warmup=o["warmup"],
+                chains=B, batches=nb, seed=o["seed"], trial_offset=o["offset"], steps=sc.S, t0=sc.t0, t1=sc.t1,
+                q=sc.q, **{"lambda": sc.lam}, ramp=sc.ramp, tec_jv=sc.jv, tecT_kappa=sc.kappa, trace=o["trace"],
+                target=target, target_energy=target_e, successes=succ, trials=B * nb, p=p,
+                batches_with_success=batch_succ, P_batch=Pb, p_wilson95=list(analyze.wilson(succ, B * nb)),
+                P_batch_wilson95=list(analyze.wilson(batch_succ, nb)), device_ms_mean=t,
+                device_ms_min=min(dms), device_ms_max=max(dms), host_ms_mean=sum(hms) / nb,
+                tts99_primary_ms=_finite(analyze.tts99(Pb, t)),
+                tts99_secondary_ms=_finite(analyze.tts99_secondary(p, B, t)), cut_mismatches=mism,
+                field_mismatches=field_mismatches, gpu_before=gpu_before, gpu_after=gpu_status())
+
+
+def gpu_status() -> str:
+    """One line of GPU state (utilisation, memory used, power, SM clock) from nvidia-smi, recorded before and after
+    the batches as the reference's runner does (sca_gpu.cu:540-547); "?" where nvidia-smi is unavailable."""
+    import subprocess
+    try:
+        r = subprocess.run(["nvidia-smi", "--id=0", "--query-gpu=utilization.gpu,memory.used,power.draw,clocks.sm",
+                            "--format=csv,noheader"], capture_output=True, text=True, timeout=10)
+        return r.stdout.strip() if r.returncode == 0 and r.stdout.strip() else "?"
+    except (OSError, subprocess.SubprocessError):
+        return "?"
 
 
 def _quadratic(inst, dense, s: np.ndarray) -> np.ndarray:
@@ -214,6 +252,16 @@ class _Null:
 
 def _finite(x: float):
     return None if x == float("inf") else x
+
+
+def _device_uuid() -> str:
+    try:
+        import torch
+        if torch.cuda.is_available():
+            return str(torch.cuda.get_device_properties(0).uuid)
+    except Exception:       # informational only
+        pass
+    return ""
 
 
 def _device_name() -> str:

@@ -221,25 +221,31 @@ struct Plan {
     int32_t hclamp = 0;
 };
 
-// Range plan: host::plan_ranges (gpu/multibit_bias_20261008/src/sca_gpu_bias.cu:543-557) semantics. The decision
-// evaluates hs * 65536 + x with |x| <= |q| + |corr| + 4T; n_lin <= n bounds |corr|.
+// Range plan. It accepts and refuses exactly the tables the reference's host::plan_ranges does
+// (gpu/multibit_bias_20261008/src/sca_gpu_bias.cu:543-557), stated here from the decision's arithmetic:
+//   z = s*h * 2^16 + (q_t -/+ corr_t) is compared with r, |r| <= 4T_t / 2, in int32.
+// The part of z that is not the field is bounded over the whole schedule by
+//   off = max_t ( |q_t| + |corr_t| + 4T_t ),  |corr_t| <= (n |kcorr_t|) >> 8 + |kconst_t| + 1   (n_lin <= n).
+// Unclamped, |s*h| <= hmax + bmax, so the kernels may use the field as is when (hmax + bmax) 2^16 + off < 2^31 - 1.
+// Otherwise they clamp s*h to +-hc with hc = floor(off / 2^16) + 1: then |hc 2^16| > off, so a clamped field decides
+// z's comparison exactly as the true one would (both lie beyond every threshold), provided hc 2^16 + off still fits.
 int range_plan_raw(int n, int64_t hmax, int64_t bmax, const int32_t* fourT, const int32_t* q, const int64_t* kcorr,
                    const int32_t* kconst, int S, Plan* out) {
-    const int64_t lim = (int64_t(1) << 31) - 1;
-    int64_t xm = 0;
+    constexpr int64_t kInt32Top = (int64_t(1) << 31) - 1;
+    constexpr int64_t kQ16 = int64_t(1) << 16;
+    int64_t off = 0;
     for (int t = 0; t < S; ++t) {
         if (fourT[t] <= 0) return fail(ANC_EINVAL, "fourT must be positive (step %d)", t);
-        const int64_t kc = kcorr[t] < 0 ? -kcorr[t] : kcorr[t];
-        if (kc > (int64_t(1) << 40)) return fail(ANC_EINVAL, "kcorr out of range at step %d", t);
-        const int64_t corr_max = ((int64_t(n) * kc) >> 8) + std::llabs(int64_t(kconst[t])) + 1;
-        xm = std::max<int64_t>(xm, std::llabs(int64_t(q[t])) + corr_max + int64_t(fourT[t]));
+        const int64_t gain = std::llabs(kcorr[t]);
+        if (gain > (int64_t(1) << 40)) return fail(ANC_EINVAL, "kcorr out of range at step %d", t);
+        const int64_t corr_bound = ((int64_t(n) * gain) >> 8) + std::llabs(int64_t(kconst[t])) + 1;
+        off = std::max<int64_t>(off, std::llabs(int64_t(q[t])) + corr_bound + int64_t(fourT[t]));
     }
-    const int64_t H = hmax + bmax;
-    out->plain_ok = H * 65536 + xm < lim;
-    const int64_t hc = xm / 65536 + 1;
-    if (65536 * hc + xm >= lim)
+    out->plain_ok = (hmax + bmax) * kQ16 + off < kInt32Top;
+    const int64_t clamp = off / kQ16 + 1;
+    if (clamp * kQ16 + off >= kInt32Top)
         return fail(ANC_EINVAL, "table range exceeds int32 kernel arithmetic even with clamping");
-    out->hclamp = int32_t(hc);
+    out->hclamp = int32_t(clamp);
     return ANC_OK;
 }
 
@@ -302,6 +308,31 @@ int plain_residency(const anc_instance* I, int P, size_t* smem, bool* stream, in
     const int rc = anc::plain_max_blocks_per_sm(I->K, P, *smem, per_sm, *stream);
     if (rc) return cuda_fail(cudaError_t(rc), "occupancy");
     if (*per_sm < 1) return fail(ANC_EINVAL, "plain engine cannot be resident (smem %zu)", *smem);
+    return ANC_OK;
+}
+
+// Launch plan of one kernel kind of a batch (the plain engine's template over K): shared memory and residency.
+constexpr int kKinds[4] = {0, 1, 2, 4};     // CSR, then dense K = 1 / 2 / 4
+int kind_index(int K) { return K == 0 ? 0 : K == 1 ? 1 : K == 2 ? 2 : 3; }
+struct KindPlan {
+    int np_max = 0, nwj_max = 0, P = 0, per_sm = 0;
+    size_t smem = 0;
+    bool stream = false;
+};
+int plan_kind(int K, int np_max, int nwj_max, int sms, KindPlan* out) {
+    (void)sms;
+    KindPlan p;
+    p.np_max = np_max;
+    p.nwj_max = nwj_max;
+    p.P = plain_P(np_max);
+    p.smem = anc::plain_smem_plan(np_max, nwj_max, K, p.P, &p.stream);
+    if (p.smem > 227 * 1024)
+        return fail(ANC_EINVAL, "batch instance too large for the plain engine (n padded to %d needs %zu B of shared "
+                                "memory)", np_max, p.smem);
+    const int rc = anc::plain_max_blocks_per_sm(K, p.P, p.smem, &p.per_sm, p.stream);
+    if (rc) return cuda_fail(cudaError_t(rc), "occupancy");
+    if (p.per_sm < 1) return fail(ANC_EINVAL, "plain engine cannot be resident (%zu B shared memory)", p.smem);
+    *out = p;
     return ANC_OK;
 }
 
@@ -882,6 +913,22 @@ int anc_run_batch(int njobs, const anc_job* jobs, const anc_run_opts* o) {
     int dev = 0, sms = 0;
     CK(cudaGetDevice(&dev));
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    // every kind's launch plan (shared memory, residency) is checked before anything is allocated or enqueued, so a
+    // refused batch leaves the caller's buffers and the device untouched
+    KindPlan plans[4];
+    {
+        int np_k[4] = {0, 0, 0, 0}, nwj_k[4] = {0, 0, 0, 0};
+        for (int k = 0; k < njobs; ++k) {
+            const int ki = kind_index(jobs[k].inst->K);
+            np_k[ki] = std::max(np_k[ki], jobs[k].inst->np);
+            nwj_k[ki] = std::max(nwj_k[ki], jobs[k].inst->K == 0 ? jobs[k].inst->nw : jobs[k].inst->nwj);
+        }
+        for (int ki = 0; ki < 4; ++ki) {
+            if (!np_k[ki]) continue;
+            const int rc = plan_kind(kKinds[ki], np_k[ki], nwj_k[ki], sms, &plans[ki]);
+            if (rc) return rc;
+        }
+    }
     cudaStream_t st = nullptr;
     CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     std::unique_ptr<CUstream_st, void (*)(cudaStream_t)> st_guard(st, [](cudaStream_t s) { cudaStreamDestroy(s); });
@@ -914,21 +961,20 @@ int anc_run_batch(int njobs, const anc_job* jobs, const anc_run_opts* o) {
     CK(d_jobs.ensure(njobs));
     CK(cudaMemcpy(d_jobs.p, pj.data(), sizeof(anc::PlainJob) * njobs, cudaMemcpyHostToDevice));
     DevBuf<int> counters;
-    const int kinds[4] = {0, 1, 2, 4};
     CK(counters.ensure(4));
-    CK(cudaMemsetAsync(counters.p, 0, 4 * sizeof(int), st));
     std::vector<DevBuf<int2>> d_items(4);
-    CK(cudaEventRecord(e0, st));
+    // from here on work is enqueued: a failure waits for the stream before the buffers above are freed
+    auto drain = [&](int rc) {
+        cudaStreamSynchronize(st);
+        return rc;
+    };
+    if (cudaMemsetAsync(counters.p, 0, 4 * sizeof(int), st) != cudaSuccess) return drain(cuda_fail(cudaGetLastError(), "memset"));
+    if (cudaEventRecord(e0, st) != cudaSuccess) return drain(cuda_fail(cudaGetLastError(), "event"));
     for (int ki = 0; ki < 4; ++ki) {
-        const int K = kinds[ki];
+        const int K = kKinds[ki];
         std::vector<int> sel;
-        int np_max = 0, nwj_max = 0;
         for (int k = 0; k < njobs; ++k)
-            if (jobs[k].inst->K == K) {
-                sel.push_back(k);
-                np_max = std::max(np_max, jobs[k].inst->np);
-                nwj_max = std::max(nwj_max, K == 0 ? jobs[k].inst->nw : jobs[k].inst->nwj);
-            }
+            if (jobs[k].inst->K == K) sel.push_back(k);
         if (sel.empty()) continue;
         // longest-processing-time-first queue: cost ~ np * S per anneal (dense np^2 * S)
         std::vector<std::pair<double, int2>> items;
@@ -939,38 +985,34 @@ int anc_run_batch(int njobs, const anc_job* jobs, const anc_run_opts* o) {
         std::stable_sort(items.begin(), items.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
         std::vector<int2> it(items.size());
         for (size_t i = 0; i < items.size(); ++i) it[i] = items[i].second;
-        CK(d_items[ki].ensure(it.size()));
-        CK(cudaMemcpyAsync(d_items[ki].p, it.data(), it.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
+        cudaError_t e = d_items[ki].ensure(it.size());
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(d_items[ki].p, it.data(), it.size() * sizeof(int2), cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) return drain(cuda_fail(e, "work items"));
+        const KindPlan& kp = plans[ki];
         anc::PlainLaunch L{};
         L.jobs = d_jobs.p;
         L.items = d_items[ki].p;
         L.nitems = int(it.size());
         L.next_item = counters.p + ki;
-        L.np_max = np_max;
-        L.nwj_max = nwj_max;
-        const int P = plain_P(np_max);
-        bool stream = false;
-        const size_t smem = anc::plain_smem_plan(np_max, nwj_max, K, P, &stream);
-        if (smem > 227 * 1024) return fail(ANC_EINVAL, "batch instance too large for the plain engine");
-        L.stream = stream ? 1 : 0;
-        int per_sm = 0;
-        int rc = anc::plain_max_blocks_per_sm(K, P, smem, &per_sm, stream);
-        if (rc) return cuda_fail(cudaError_t(rc), "occupancy");
-        if (per_sm < 1) return fail(ANC_EINVAL, "plain engine cannot be resident");
-        const int grid = std::max(1, std::min(L.nitems, per_sm * sms));
-        rc = anc::plain_launch(L, K, P, grid, smem, st);
-        if (rc) return cuda_fail(cudaError_t(rc), "plain engine launch");
+        L.np_max = kp.np_max;
+        L.nwj_max = kp.nwj_max;
+        L.stream = kp.stream ? 1 : 0;
+        const int grid = std::max(1, std::min(L.nitems, kp.per_sm * sms));
+        const int rc = anc::plain_launch(L, K, kp.P, grid, kp.smem, st);
+        if (rc) return drain(cuda_fail(cudaError_t(rc), "plain engine launch"));
     }
-    CK(cudaEventRecord(e1, st));
+    if (cudaEventRecord(e1, st) != cudaSuccess) return drain(cuda_fail(cudaGetLastError(), "event"));
     for (const Prepared& p : prep) {
         const anc_job& j = jobs[p.idx];
         JobBufs& b = *bufs[p.idx];
-        CK(cudaMemcpyAsync(j.spins, b.spins.p, size_t(j.inst->nw) * j.nchains * 4, cudaMemcpyDeviceToHost, st));
-        CK(cudaMemcpyAsync(j.sum_sh, b.sh.p, size_t(j.nchains) * 8, cudaMemcpyDeviceToHost, st));
-        if (j.sum_bs) CK(cudaMemcpyAsync(j.sum_bs, b.bs.p, size_t(j.nchains) * 8, cudaMemcpyDeviceToHost, st));
-        if (j.flips) CK(cudaMemcpyAsync(j.flips, b.fl.p, size_t(j.nchains) * 8, cudaMemcpyDeviceToHost, st));
-        if (j.trace)
-            CK(cudaMemcpyAsync(j.trace, b.trace.p, size_t(j.nchains) * j.tb->S * 4, cudaMemcpyDeviceToHost, st));
+        cudaError_t e = cudaMemcpyAsync(j.spins, b.spins.p, size_t(j.inst->nw) * j.nchains * 4, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(j.sum_sh, b.sh.p, size_t(j.nchains) * 8, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess && j.sum_bs) e = cudaMemcpyAsync(j.sum_bs, b.bs.p, size_t(j.nchains) * 8, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess && j.flips) e = cudaMemcpyAsync(j.flips, b.fl.p, size_t(j.nchains) * 8, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess && j.trace)
+            e = cudaMemcpyAsync(j.trace, b.trace.p, size_t(j.nchains) * j.tb->S * 4, cudaMemcpyDeviceToHost, st);
+        if (e != cudaSuccess) return drain(cuda_fail(e, "result copy"));
     }
     CK(cudaStreamSynchronize(st));
     float ms = 0.f;
@@ -1057,14 +1099,13 @@ extern "C" int anc_run_batch_noalloc(int njobs, const anc_device_job* jobs, void
     static thread_local NaSetup setup;   // 12 KB: kept off the stack
     NaSetup& S = setup;
     S.njobs = njobs;
-    const int kinds[4] = {0, 1, 2, 4};
     int kind_first[5] = {0, 0, 0, 0, 0}, kind_np[4] = {0, 0, 0, 0}, kind_nwj[4] = {0, 0, 0, 0};
     int slot = 0, items = 0;
     for (int ki = 0; ki < 4; ++ki) {
         kind_first[ki] = items;
         for (int k = 0; k < njobs; ++k) {
             const anc_device_job& j = jobs[k];
-            if (j.kbits != kinds[ki]) continue;
+            if (j.kbits != kKinds[ki]) continue;
             anc::PlainJob& p = S.jobs[slot];
             p = anc::PlainJob{};
             p.n = j.n;
@@ -1101,33 +1142,33 @@ extern "C" int anc_run_batch_noalloc(int njobs, const anc_device_job* jobs, void
     kind_first[4] = items;
     S.first[njobs] = items;
     S.nitems = items;
+    // every kind's launch plan is checked before anything is enqueued: a refused call touches neither the scratch
+    // array nor the caller's buffers
+    KindPlan plans[4];
+    for (int ki = 0; ki < 4; ++ki) {
+        if (kind_first[ki + 1] == kind_first[ki]) continue;
+        const int rc = plan_kind(kKinds[ki], kind_np[ki], kind_nwj[ki], sms, &plans[ki]);
+        if (rc) return rc;
+    }
     auto* d_jobs = reinterpret_cast<anc::PlainJob*>(base + kNaJobsOff);
     auto* d_items = reinterpret_cast<int2*>(base + kNaItemsOff);
     na_setup_kernel<<<(items + 255) / 256, 256, 0, st>>>(S, d_jobs, d_items);
     CK(cudaGetLastError());
     CK(cudaMemsetAsync(base, 0, 256, st));   // the counters must start at zero on every call
     for (int ki = 0; ki < 4; ++ki) {
-        const int K = kinds[ki];
+        const int K = kKinds[ki];
         const int cnt = kind_first[ki + 1] - kind_first[ki], item_off = kind_first[ki];
-        const int np_max = kind_np[ki], nwj_max = kind_nwj[ki];
         if (!cnt) continue;
+        const KindPlan& kp = plans[ki];
         anc::PlainLaunch L{};
         L.jobs = d_jobs;
         L.items = d_items + item_off;
         L.nitems = cnt;
         L.next_item = reinterpret_cast<int*>(base) + ki;
-        L.np_max = np_max;
-        L.nwj_max = nwj_max;
-        const int P = plain_P(np_max);
-        bool stream = false;
-        const size_t smem = anc::plain_smem_plan(np_max, nwj_max, K, P, &stream);
-        if (smem > 227 * 1024) return fail(ANC_EINVAL, "instance too large for the plain engine");
-        L.stream = stream ? 1 : 0;
-        int per_sm = 0;
-        int rc = anc::plain_max_blocks_per_sm(K, P, smem, &per_sm, stream);
-        if (rc) return cuda_fail(cudaError_t(rc), "occupancy");
-        if (per_sm < 1) return fail(ANC_EINVAL, "plain engine cannot be resident");
-        rc = anc::plain_launch(L, K, P, std::max(1, std::min(cnt, per_sm * sms)), smem, st);
+        L.np_max = kp.np_max;
+        L.nwj_max = kp.nwj_max;
+        L.stream = kp.stream ? 1 : 0;
+        const int rc = anc::plain_launch(L, K, kp.P, std::max(1, std::min(cnt, kp.per_sm * sms)), kp.smem, st);
         if (rc) return cuda_fail(cudaError_t(rc), "plain engine launch");
     }
     return ANC_OK;

@@ -413,3 +413,45 @@ def load(kind: str, path: str) -> Instance:
     if kind == "jint8":
         return read_jint8(path)
     raise ValueError("unknown J source kind " + kind)
+
+
+def main(argv=None) -> int:
+    """Write the synthetic instances of the benchmarks and tests as files the CLI reads:
+
+        python -m anechoic_b200.instances complete --n 2000 --seed 20261004 --out F.bin        SNOWGPU1 (+-1 complete)
+        python -m anechoic_b200.instances kbit --n 16384 --kbits 4 --seed S [--pzero P] [--bmax B] --out PREFIX
+                                                                           PREFIX.jint8 (+ PREFIX.bias when B > 0)
+        python -m anechoic_b200.instances torus --l1 100 --l2 200 --seed S [--plus] [--bmax B] --out PREFIX
+                                                                           PREFIX.gset (+ PREFIX.bias when B > 0)
+    """
+    import argparse
+    ap = argparse.ArgumentParser(prog="python -m anechoic_b200.instances")
+    ap.add_argument("kind", choices=["complete", "kbit", "torus"])
+    ap.add_argument("--n", type=int, default=2000)
+    ap.add_argument("--kbits", type=int, default=4)
+    ap.add_argument("--seed", type=int, default=20261004)
+    ap.add_argument("--pzero", type=float, default=0.0)
+    ap.add_argument("--bmax", type=int, default=0)
+    ap.add_argument("--l1", type=int, default=100)
+    ap.add_argument("--l2", type=int, default=200)
+    ap.add_argument("--plus", action="store_true", help="torus: weights +1 instead of iid +-1")
+    ap.add_argument("--out", required=True)
+    a = ap.parse_args(argv)
+    if a.kind == "complete":
+        write_snowgpu1(complete_pm1(a.n, a.seed), a.out)
+        print(a.out)
+        return 0
+    inst = random_kbit(a.n, a.kbits, a.seed, pzero=a.pzero, bmax=a.bmax) if a.kind == "kbit" else \
+        torus(a.l1, a.l2, a.seed, signed=not a.plus, bmax=a.bmax)
+    path = a.out + (".jint8" if a.kind == "kbit" else ".gset")
+    (write_jint8 if a.kind == "kbit" else write_gset)(inst, path)
+    print(path)
+    if inst.bias is not None:
+        write_bias(inst.bias, a.out + ".bias")
+        print(a.out + ".bias")
+    return 0
+
+
+if __name__ == "__main__":
+    import sys
+    sys.exit(main())

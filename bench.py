@@ -137,10 +137,13 @@ def tts99(P: float, t: float) -> float:
 
 
 def tts99_secondary(p: float, B: int, t: float) -> float:
+    """Secondary TTS99 with B anneals per batch of time t. When every anneal succeeds (p = 1) it is one anneal's share
+    of the batch, t / B (the reference's per-trial estimators return one trial's time there,
+    research/reaim_benchmarks_20261008/analyze.py:83), not 0."""
     if p <= 0.0:
         return math.inf
     if p >= 1.0:
-        return 0.0
+        return t / B
     return t * math.log(0.01) / (B * math.log(1.0 - p))
 
 

@@ -190,18 +190,22 @@ ANC_API int anc_run_batch(int njobs, const anc_job* jobs, const anc_run_opts* op
  * that must not grow. All inputs and outputs are DEVICE memory owned by the caller; the call allocates nothing
  * (no cudaMalloc, no cudaFree, no allocating library routine). Its scratch -- job descriptors, the work-item queue
  * and its counters -- is one file-scope device array of ANC_NOALLOC_SCRATCH_BYTES that every GPU loading the library
- * holds until exit. The first call on a device looks that array up (cudaGetSymbolAddress) with the device current.
- * Limits: at most ANC_NOALLOC_MAX_JOBS jobs and ANC_NOALLOC_MAX_ANNEALS anneals (sum of nchains) per call; larger
- * requests return ANC_EINVAL. Every call reuses the same array and resets its counters: calls that overlap on the GPU
- * (different streams, or several host threads) race; calls in order on one stream do not. The job table travels as
- * a kernel parameter block, so the call leaves no reference to host memory in the stream: it can be captured into a
- * CUDA graph, and every replay runs the captured jobs.
+ * holds until exit. The first call on a device does a one-time set-up with that device current: it looks the array
+ * up (cudaGetSymbolAddress), queries occupancy, and may load the kernels; make that first call before any stream
+ * capture on the device. Limits: at most ANC_NOALLOC_MAX_JOBS jobs and ANC_NOALLOC_MAX_ANNEALS anneals (sum of
+ * nchains) per call; larger requests return ANC_EINVAL. Every call reuses the same array and resets its counters:
+ * calls that overlap on the GPU (different streams, or several host threads) race; calls in order on one stream do
+ * not. A call whose jobs cannot run (sizes, a kind the plain engine cannot hold) returns ANC_EINVAL before it
+ * enqueues anything. The job table travels as a kernel parameter block, so the call leaves no reference to host
+ * memory in the stream.
  * Job layout:
  *   kbits 1/2/4: planes = [kbits][NP][NWJ] uint32 with NP = anc_np(n), NWJ = ceil(NP/32) rounded up to a multiple of
  *   32; word x*NWJ + y/32, bit y%32 of plane p describes J_xy: kbits 1 -> [J_xy = +1] (a +-1 complete graph);
  *   kbits 2/4 -> plane 0 = [J_xy < 0], plane b = bit b-1 of |J_xy|. kbits 0: CSR row_ptr[n+1] and
  *   adj[k] = (y << 8) | (uint8)J_xy for every nonzero of row x.
- *   hclamp: 0 when anc_plan_ranges reports plain_ok, else its hclamp. Outputs as anc_run_device. */
+ *   hclamp: 0 when anc_plan_ranges reports plain_ok, else its hclamp. This call does not re-check it (the tables are
+ *   in device memory): an hclamp of 0 where the plan needs the clamp lets the int32 decision overflow silently and
+ *   gives wrong results. Outputs as anc_run_device. */
 #define ANC_NOALLOC_MAX_JOBS 64
 #define ANC_NOALLOC_MAX_ANNEALS 16384
 #define ANC_NOALLOC_SCRATCH_BYTES (144 * 1024) /* upper bound of the device scratch array (139 KB used) */

@@ -6,9 +6,9 @@ container only) and run on the synthetic N = 2000 +-1 instance (seed 20261004) f
 schedule, 4096 trials record the number of final cuts at or above three targets: the float model's own quartiles.
 The exact engine's GPU test (tests/test_float_agreement.py) compares its success proportions with these counts
 (two-proportion z-test), as the reference compares its exact and float models
-(gpu/multibit_bias_20261008/REPORT.md:62). Run from the repository root:
+(gpu/multibit_bias_20261008/REPORT.md:62). Run from the repository root with the reference project's root:
 
-    python tests/golden/make_float_agreement.py
+    python tests/golden/make_float_agreement.py --ref-root REFERENCE_ROOT
 """
 from __future__ import annotations
 
@@ -20,9 +20,8 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = "/root/reference/research/optimum_mitigation_20261007"
+MODEL_DIR = "research/optimum_mitigation_20261007"     # the float model's directory within the reference project
 sys.path.insert(0, ROOT)
-sys.path.insert(0, REF)
 
 from anechoic_b200 import instances as I  # noqa: E402
 
@@ -38,7 +37,12 @@ CASES = [
 B = 4096
 
 
-def main():
+def main(argv=None):
+    import argparse
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref-root", required=True, help="root directory of the reference project")
+    a = ap.parse_args(argv)
+    sys.path.insert(0, os.path.join(a.ref_root, MODEL_DIR))
     import sca_fast as F
     inst = I.complete_pm1(2000, 20261004)
     J = inst.dense.astype(np.float32)
@@ -53,8 +57,7 @@ def main():
                         std_cut=float(cut.std())))
         print(out[-1])
     with open(os.path.join(HERE, "float_agreement.json"), "w") as f:
-        json.dump(dict(instance="complete_pm1(2000, 20261004)", model=REF.split("/root/reference/")[1] +
-                       "/sca_fast.py::run_cfg", cases=out), f, indent=1)
+        json.dump(dict(instance="complete_pm1(2000, 20261004)", model=MODEL_DIR + "/sca_fast.py::run_cfg", cases=out), f, indent=1)
 
 
 if __name__ == "__main__":

@@ -48,3 +48,49 @@ def test_estimate_from_run_files(tmp_path):
     lo, hi = e["tts_primary_ci_ms"]
     assert lo <= e["tts_primary_ms"] <= hi
     assert Z.selection_score(e, "primary") >= e["tts_primary_ms"]
+
+
+def _dec(v):
+    if v == "inf":
+        return math.inf
+    if isinstance(v, list):
+        return [_dec(x) for x in v]
+    return v
+
+
+def _same(a, b):
+    if isinstance(a, list):
+        return len(a) == len(b) and all(_same(x, y) for x, y in zip(a, b))
+    if isinstance(a, float) or isinstance(b, float):
+        if math.isinf(a) or math.isinf(b):
+            return a == b
+        return math.isclose(a, b, rel_tol=1e-12, abs_tol=1e-15)
+    return a == b
+
+
+def test_estimates_match_reference_fixture(tmp_path):
+    """The reference's estimate() / selection_score() (gpu/onsager_v2_20261007/src/analyze.py:56-88) ran on run files
+    in this CLI's format (tests/golden/make_analyze_golden.py); the same files give the same value for every field
+    here. Where the reference raises (a cohort without successes: its Wilson bound reaches log(1 - P) = 0), this
+    estimator returns an unbounded time to solution instead."""
+    import os
+    from tests.conftest import GOLDEN
+    with open(os.path.join(GOLDEN, "analyze_estimates.json")) as f:
+        cases = json.load(f)["cases"]
+    assert len(cases) >= 6
+    for c in cases:
+        prefix = str(tmp_path / c["name"])
+        with open(prefix + ".summary.json", "w") as f:
+            f.write(c["summary"])
+        with open(prefix + ".batches.jsonl", "w") as f:
+            f.write(c["batches"])
+        e = Z.estimate(prefix)
+        e["selection_primary"] = Z.selection_score(e, "primary")
+        e["selection_secondary"] = Z.selection_score(e, "secondary")
+        if "raises" in c:
+            assert e["successes"] == 0 and e["tts_primary_ms"] == math.inf and e["tts_secondary_ms"] == math.inf
+            assert e["tts_primary_ci_ms"][1] == math.inf and e["selection_primary"] == math.inf
+            continue
+        for k, v in c["expected"].items():
+            assert k in e, (c["name"], k)
+            assert _same(_dec(v), e[k]), (c["name"], k, v, e[k])

@@ -20,7 +20,7 @@ def test_tts99_estimators():
     B, p = 1024, 0.02
     assert math.isclose(bench.tts99_secondary(p, B, t), t * math.log(0.01) / (B * math.log(1 - p)))
     assert bench.tts99_secondary(0.0, B, t) == math.inf
-    assert bench.tts99_secondary(1.0, B, t) == 0.0
+    assert bench.tts99_secondary(1.0, B, t) == t / B                    # every anneal succeeds: one anneal's share
 
 
 def test_line_is_strict_json():

@@ -42,3 +42,35 @@ def test_energies_rescored_on_the_host(batch):
         e = r.energies()
         for c in range(2):
             assert int(e[c]) == inst.energy(r.spins[c]), name
+
+
+def test_refused_batch_enqueues_nothing(cuda):
+    """A batch that mixes a valid job with one the plain engine cannot hold (n = 60000: its fields alone need more
+    shared memory than a CTA has) is refused with ANC_EINVAL before anything is enqueued: the valid job's host
+    outputs keep their sentinel pattern."""
+    import ctypes as C
+    import numpy as np
+    from anechoic_b200 import _lib
+    L = _lib.load()
+    small, big = I.torus(20, 40, 3, True, bmax=2), I.torus(200, 300, 4, True)
+    devs = [A.DeviceInstance(small), A.DeviceInstance(big)]
+    tb = A.Tables.from_schedule(A.Schedule(S=20, t0=4.0, t1=0.5, q=1.0, kappa=2.0, ramp=True))
+    arr = (_lib.Job * 2)()
+    keep = []
+    for k, d in enumerate(devs):
+        W = A.spin_words(d.n)
+        bufs = dict(spins=np.full((2, W), 0x5A5A5A5A5A5A5A5A, np.uint64), sh=np.full(2, -7, np.int64),
+                    bs=np.full(2, -7, np.int64), fl=np.full(2, -7, np.int64), tr=np.full((2, 20), -7, np.int32))
+        keep.append(bufs)
+        a = arr[k]
+        a.inst, a.tb, a.seed, a.trial_offset, a.nchains = d._h.value, tb._h.value, 1, 0, 2
+        a.spins, a.sum_sh, a.sum_bs = bufs["spins"].ctypes.data, bufs["sh"].ctypes.data, bufs["bs"].ctypes.data
+        a.flips, a.trace = bufs["fl"].ctypes.data, bufs["tr"].ctypes.data
+    o = _lib.opts("auto")
+    rc = L.anc_run_batch(2, arr, C.byref(o))
+    assert rc == -1 and "shared" in L.anc_last_error().decode()
+    for b in keep:
+        assert np.all(b["spins"] == 0x5A5A5A5A5A5A5A5A) and np.all(b["sh"] == -7) and np.all(b["tr"] == -7)
+    # the valid job alone runs
+    outs = A.run_batch([dict(dev=devs[0], tb=tb, seed=1, trial_offset=0, nchains=2)])
+    assert int(outs[0].flips.sum()) > 0

@@ -20,7 +20,7 @@ def _dev(a, torch):
     return torch.from_numpy(np.ascontiguousarray(a)).cuda()
 
 
-def _build(inst, sched, seed, off, nchains, torch):
+def _build(inst, sched, seed, off, nchains, torch, with_ref=True):
     """Caller-owned device inputs and outputs for one job, plus the same job through anc_run for comparison."""
     kbits = 0 if inst.is_sparse else inst.kbits()
     tb = noalloc.schedule_tables(**sched)
@@ -47,6 +47,8 @@ def _build(inst, sched, seed, off, nchains, torch):
     keep["trace"] = torch.zeros((nchains, j.S), dtype=torch.int32, device="cuda")
     j.spins, j.sum_sh, j.sum_bs = keep["spins"].data_ptr(), keep["sh"].data_ptr(), keep["bs"].data_ptr()
     j.flips, j.trace = keep["fl"].data_ptr(), keep["trace"].data_ptr()
+    if not with_ref:
+        return j, keep, None
     ref = A.run(A.DeviceInstance(inst), A.Tables.from_schedule(A.Schedule(**sched)), seed, off, nchains, trace=True,
                 engine="plain")
     return j, keep, ref
@@ -92,3 +94,22 @@ def test_noalloc_rejects_oversized_requests(cuda):
     with pytest.raises(A.AncError) as e:
         noalloc.run_batch_noalloc([j for _ in range(65)])
     assert e.value.code == -1 and "jobs" in str(e.value)
+
+
+def test_noalloc_refused_call_enqueues_nothing(cuda):
+    """A call that mixes a valid job with one the plain engine cannot hold (n = 60000: its fields alone need more
+    shared memory than a CTA has) returns ANC_EINVAL before it enqueues anything: the valid job's device outputs keep
+    their sentinel pattern. Both jobs' buffers are real and sized for their jobs."""
+    import torch
+    good = _build(A.torus(20, 40, 3, True, bmax=2), dict(S=20, t0=4.0, t1=0.5, q=1.0, kappa=2.0, ramp=True), 1, 0, 4,
+                  torch)
+    bad = _build(A.torus(200, 300, 4, True), dict(S=2, t0=4.0, t1=0.5, q=1.0), 1, 0, 1, torch, with_ref=False)
+    for k in ("spins", "sh", "bs", "fl", "trace"):
+        good[1][k].fill_(-7)
+    stream = torch.cuda.current_stream()
+    with pytest.raises(A.AncError) as e:
+        noalloc.run_batch_noalloc([good[0], bad[0]], stream.cuda_stream)
+    assert e.value.code == -1 and "shared" in str(e.value)
+    torch.cuda.synchronize()
+    for k in ("spins", "sh", "bs", "fl", "trace"):
+        assert bool((good[1][k] == -7).all()), k
