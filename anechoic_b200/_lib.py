@@ -23,7 +23,7 @@ EXPORTS = ("anc_instance_create", "anc_instance_create_csr", "anc_instance_get_i
            "anc_run_fields", "anc_run_device",
            "anc_run_batch", "anc_last_device_ms", "anc_last_kernel", "anc_last_error", "anc_last_profile", "anc_version",
            "anc_run_batch_noalloc", "anc_mf_create", "anc_mf_npad", "anc_mf_forward", "anc_mf_backward",
-           "anc_mf_check", "anc_mf_set_wait_ns", "anc_mf_destroy")
+           "anc_mf_check", "anc_mf_set_wait_ns", "anc_mf_destroy", "anc_set_wait_ns", "anc_get_wait_ns")
 
 
 class AncError(RuntimeError):
@@ -98,6 +98,9 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         L.anc_last_profile.argtypes = [C.POINTER(C.c_double), C.c_int]
         L.anc_version.argtypes = []
         L.anc_version.restype = C.c_char_p
+        L.anc_set_wait_ns.argtypes = [_u64]
+        L.anc_get_wait_ns.argtypes = []
+        L.anc_get_wait_ns.restype = _u64
         _lib = L
         return L
 

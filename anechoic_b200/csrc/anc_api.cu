@@ -23,6 +23,7 @@ thread_local std::string g_err;
 thread_local double g_dev_ms = 0.0;
 thread_local std::vector<double> g_prof;
 thread_local int g_last_kernel = 0;
+std::atomic<uint64_t> g_wait_ns{2000000000ull};   // limit of each device wait of the engines' kernels (anc_set_wait_ns)
 
 int fail(int code, const char* fmt, ...) {
     char buf[512];
@@ -447,6 +448,7 @@ int run_device_impl(anc_instance* I, anc_tables* tb, uint64_t seed, uint32_t off
         r.out_h = out.h;
         r.prof = nullptr;
         r.kind = o ? o->tensor_kind : ANC_TENSOR_AUTO;
+        r.wait_ns = g_wait_ns.load();
         I->prof_ctas = 0;
         if (o && o->profile) {
             anc::TensorGeometry geo;
@@ -618,6 +620,11 @@ int anc_last_profile(double* out, int max) {
 }
 const char* anc_version(void) { return "anechoic-b200 0.1 (sm_100a)"; }
 double anc_last_device_ms(void) { return g_dev_ms; }
+int anc_set_wait_ns(uint64_t ns) {
+    g_wait_ns.store(ns);
+    return ANC_OK;
+}
+uint64_t anc_get_wait_ns(void) { return g_wait_ns.load(); }
 int anc_last_kernel(void) { return g_last_kernel; }
 int anc_np(int n) { return pad_np(n); }
 int anc_spin_words(int n) { return pad_np(n) / 64; }

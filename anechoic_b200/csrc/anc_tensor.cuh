@@ -47,6 +47,7 @@ struct TensorRun {
     int32_t* out_h;
     long long* prof;          // device [grid][16] phase cycle totals, or null (profiling off)
     int kind;                 // TENSOR_KIND_*
+    uint64_t wait_ns;         // limit of each device wait of the launch (0: give up at the first unsatisfied poll)
 };
 
 // Launch geometry of a run: CTAs in the grid, CTAs per cluster, and how many clusters can be co-resident.

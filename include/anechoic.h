@@ -262,6 +262,15 @@ ANC_API int anc_mf_check(anc_meanfield* mf, void* stream);
 ANC_API int anc_mf_set_wait_ns(anc_meanfield* mf, uint64_t ns);
 ANC_API void anc_mf_destroy(anc_meanfield* mf);
 
+/* No counterpart in the reference, whose spins on its exchange mbarriers have no bound
+ * (gpu/onsager_v2_20261007/src/sca_gpu.cu:249). Limit (ns, default 2e9) of each device-side wait of the tensor engine's
+ * kernels launched after this call, process-wide. A wait that reaches it makes the kernel record an error, stop
+ * issuing work, wait (with its own fixed bound) for the copies and MMAs it has in flight, and return; the call
+ * returns ANC_ETIMEOUT, the results are not valid, and the context and handles stay usable. 0 gives up at the first
+ * unsatisfied poll (for tests of that path). anc_get_wait_ns returns the current limit. */
+ANC_API int anc_set_wait_ns(uint64_t ns);
+ANC_API uint64_t anc_get_wait_ns(void);
+
 /* Last device time of a synchronous run on this thread (ms, CUDA events around the launch). */
 ANC_API double anc_last_device_ms(void);
 
