@@ -249,3 +249,39 @@ def tune(inst: Instance, S: int = 200, R: int = 64, theta0=(30.0, math.log(6.0),
             log(hist[-1])
     theta = torch.stack([raw[0].exp(), raw[1].exp(), raw[2], raw[3], raw[4]]).detach()
     return theta, hist
+
+
+def judge(inst: Instance, S: int, thetas: dict, nchains: int = 1024, seed: int = 20261004, trial_offset: int = 0,
+          targets: Optional[dict] = None, mode: str = "counted", engine: str = "auto") -> dict:
+    """Judge schedules on the exact integer engine only: for each named theta (T0, rate, q0, q_slope, gain) the
+    integer tables of SoftSchedule(S, mode).table_arrays run nchains anneals (the same trial ids for every schedule)
+    and each named target cut t gives p = P(cut >= t) with its Wilson 95 % interval and the secondary TTS99
+    t_batch ln(0.01) / (B ln(1 - p)) (the reference's estimators, analyze.py:15-47). targets defaults to
+    {"median_first": the median cut of the first schedule}. Returns {name: {...}} plus the targets used."""
+    from . import analyze
+    from .engine import DeviceInstance, Tables, run
+    dev = DeviceInstance(inst)
+    sumw = inst.stats()["sumw"]
+    cuts, times, kernels = {}, {}, {}
+    for name, th in thetas.items():
+        tb = Tables.from_arrays(**SoftSchedule(S=S, mode=mode).table_arrays(th))
+        run(dev, tb, seed, 0xB0000000, min(nchains, 128), engine=engine)          # warm-up (untimed, other trials)
+        r = run(dev, tb, seed, trial_offset, nchains, engine=engine)
+        cuts[name], times[name], kernels[name] = r.cuts(sumw), r.device_ms, r.kernel
+    first = next(iter(thetas))
+    if targets is None:
+        targets = {"median_first": int(np.median(cuts[first]))}
+    out = {"targets": dict(targets), "S": S, "anneals": nchains, "engine_kernels": kernels}
+    for name in thetas:
+        c = cuts[name]
+        th = thetas[name]
+        rec = {"theta": [float(x) for x in (th.tolist() if isinstance(th, torch.Tensor) else th)],
+               "mean_cut": float(c.mean()), "best_cut": int(c.max()), "ms_per_batch": times[name]}
+        for tn, tv in targets.items():
+            k = int((c >= tv).sum())
+            p = k / nchains
+            lo, hi = analyze.wilson(k, nchains)
+            rec[tn] = {"p": p, "p_wilson95": [lo, hi], "successes": k,
+                       "tts99_ms_secondary": analyze.tts99_secondary(p, nchains, times[name])}
+        out[name] = rec
+    return out

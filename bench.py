@@ -475,7 +475,7 @@ def bench_ours(args, ws, rank, local):
         line["single_anneal"] = single_anneal(A, dev, tb, timed, p, sumw, target)
         extra = {}
         for name in ("sparse51", "dense16k", "meanfield"):
-            extra[name] = run_extra(name, args)
+            extra[name] = run_extra(name, args, target=target)
         line["configs"] = extra
     print(json.dumps(finite(line)))
     if dist:
@@ -518,9 +518,11 @@ EXTRA_DESC = {
 }
 
 
-def run_extra(name: str, args, steps: int = 3, warmup: int = 1) -> dict:
+def run_extra(name: str, args, steps: int = 3, warmup: int = 1, target=None) -> dict:
     """One of the other BASELINE workloads, timed on the device (the library's CUDA events around each launch, or
-    events on the stream), outside the headline's timed region, with its own roofline."""
+    events on the stream), outside the headline's timed region, with its own roofline. meanfield also tunes the
+    schedule on the relaxation and judges the tuned and the default schedule on the exact engine (1024 anneals each,
+    same trial ids): p at the default schedule's median cut and, when given, at the headline's target cut."""
     import numpy as np
     import torch
     import anechoic_b200 as A
@@ -555,7 +557,20 @@ def run_extra(name: str, args, steps: int = 3, warmup: int = 1) -> dict:
         fl_f = 2.0 * inst.n * inst.n * R * S           # algorithmic: J m per step
         ach = fl_f / (tf / 1000.0) / 1e12
         ach_b = 2 * fl_f / (tb_ / 1000.0) / 1e12
+        theta0 = (30.0, math.log(6.0), 4.0, 0.0, 1.05)
+        t_tune = time.perf_counter()
+        tuned, hist = M.tune(inst, S=S, R=R, theta0=theta0, iters=40, lr=0.05)
+        t_tune = time.perf_counter() - t_tune
+        thetas = {"default": torch.tensor(theta0, dtype=torch.float64), "tuned": tuned.cpu()}
+        judged = M.judge(inst, S, thetas, nchains=CHAINS, seed=RUN_SEED, trial_offset=0xA0000000)
+        if target is not None:
+            judged = M.judge(inst, S, thetas, nchains=CHAINS, seed=RUN_SEED, trial_offset=0xA0000000,
+                             targets={"median_default": judged["targets"]["median_first"],
+                                      "headline_target": int(target)})
         return {"workload": EXTRA_DESC[name], "forward_ms": tf, "adjoint_ms": tb_, "replicas": R, "S": S,
+                "tuning": {"iters": len(hist), "wall_s": t_tune, "soft_cut_first": hist[0][1],
+                           "soft_cut_last": hist[-1][1]},
+                "exact_engine_judgement": judged,
                 "roofline": {"bound": "tensor", "achieved": ach, "peak": bf16_sus, "unit": "TFLOP/s",
                              "frac": ach / bf16_sus, "peak_kind": f"{peak_kind} bf16 sustained",
                              "algorithmic_per_launch": fl_f, "kernel": "mf_gemm_kernel (+ mf_fwd_kernel)",

@@ -178,3 +178,21 @@ def test_wait_limit_expiry_is_reported_and_the_context_recovers(pm1):
     out = relax(mf, beta, q, u, w, m0)
     ref = relax(MeanField(pm1), beta, q, u, w, m0)
     assert torch.equal(out, ref)
+
+
+def test_tuned_schedule_judged_on_the_exact_engine(pm1):
+    """The relaxation tunes; only the exact engine judges: tuned and default schedules run the same 256 trial ids,
+    and each gets p at the default's median cut with a Wilson 95 % interval and the secondary TTS99."""
+    from anechoic_b200.meanfield import judge, tune
+    S = 100
+    theta0 = (30.0, math.log(6.0), 4.0, 0.0, 1.05)
+    tuned, hist = tune(pm1, S=S, R=64, theta0=theta0, iters=6)
+    assert hist[-1][1] >= hist[0][1] - 1.0          # the soft cut does not fall
+    res = judge(pm1, S, {"default": torch.tensor(theta0, dtype=torch.float64), "tuned": tuned.cpu()}, nchains=256)
+    t = res["targets"]["median_first"]
+    for name in ("default", "tuned"):
+        rec = res[name]["median_first"]
+        lo, hi = rec["p_wilson95"]
+        assert 0.0 <= lo <= rec["p"] <= hi <= 1.0 and rec["successes"] == round(rec["p"] * 256)
+        assert res[name]["best_cut"] >= t or rec["p"] == 0.0
+    assert res["default"]["median_first"]["p"] >= 0.5      # at least half reach their own median
