@@ -549,21 +549,27 @@ __global__ void __launch_bounds__(T, 1) plain_kernel(const __grid_constant__ Pla
 
 // ------------------------------------------------------------------------------------------------ cluster variant
 // One anneal spread over a cluster of kCR = 8 CTAs (dense K = 1, NP = 2048), for the lowest latency per anneal.
-// CTA r owns RNG lanes 32r .. 32r+31, i.e. spin word k*8 + r of every round k. Per step:
-//   1. warp 0 decides its 32 lanes x 8 rounds exactly as plain_kernel (fields in registers), building per round the
-//      flip word and the new-sign word (flipped from +1) with two ballots, and the n_lin partial;
-//   2. lanes 0..16 store the 8 flip words, 8 new-sign words and the partial into every CTA's receive slot for this
-//      pass's parity (st.shared::cluster), and one cluster barrier (release / acquire) makes them visible;
-//   3. every CTA turns the 64 flip words into the step's flip list (the same list in every CTA) and counts, for its
-//      8 owned words, the flipped rows x with s'_x J_xy = +1 in bit-sliced carry-save counters. Its 8 words of every
-//      J row (64 KB) stay in shared memory, so no row is read from L2 during the anneal;
-//   4. the deciders add the counts into their fields at the start of the next step (dense_delta, as plain_kernel).
-// The receive slots alternate by pass parity: a slot is rewritten two passes later, after every CTA has passed the
-// cluster barrier of the pass in between, so one barrier per step suffices. No CTA waits on anything but cluster
-// and CTA barriers, which every thread of every CTA reaches the same number of times.
-constexpr int kCT = 256;                  // threads per CTA
+// CTA r owns the 256 slots i = k*256 + 32r + l (round k, RNG lane 32r + l), one per thread: thread t = 32k + l keeps
+// its slot's field, spin and last-flip bit in registers and a copy of lane 32r + l's xoshiro128** state, which it
+// advances 8 draws per step and uses the k-th (every lane's stream is consumed in round order, as the golden model
+// does). The J rows of the owned slots (by symmetry their columns, 256 x 2048 bits = 64 KB) stay in shared memory.
+// Per step:
+//   1. every thread decides its slot; warp k's ballots give flip word k*8 + r (bit l = slot k*256 + 32r + l), the
+//      matching word of new spins +1 among the flipped, and its popcount of the linear band (n_lin partial); lane 0
+//      stores the three into this CTA's send slot for the step's parity and the CTA arrives on the cluster barrier
+//      (release); the next step's draws are made before the wait (acquire);
+//   2. 128 threads load the 64 flip words and 64 new-spin words from the 8 CTAs' send slots (ld.shared::cluster), 64
+//      threads load and reduce the n_lin partials, and a CTA barrier makes them visible;
+//   3. every thread updates its field from all 2048 slots at once: for its row y of J (bit = [J_xy = +1]),
+//        D = sum_w popc(F_w & (U_w ^ J_yw)),   h_y += 2 (|F| - 2 D)   (2 s'_x J_xy summed over the flipped x),
+//      less the diagonal term when y itself flipped (J_yy = 0 is stored as a 0 bit). The initial pass uses the same
+//      formula with F = the active slots, U = s0 and factor 1 (h = b + J s0).
+// No step reads J from L2, no flip list is built and no counter is extracted: the update costs the same whatever
+// the flip count. A send slot is rewritten two steps later, after every CTA has passed the cluster barrier of the step
+// in between, which it arrives at only after its reads of the slot; so one cluster barrier per step suffices. Every
+// thread of every CTA reaches the cluster and CTA barriers the same number of times (no other wait exists).
+constexpr int kCT = 256;                  // threads per CTA (one slot each)
 constexpr int kCR = 8;                    // CTAs per anneal
-constexpr int kCW = 20;                   // receive words per source CTA: 8 flip, 8 new-sign, n_lin partial, spare
 constexpr size_t kClusterSmem = 116 * 1024;   // above half an SM's shared memory: one CTA per SM
 
 __device__ __forceinline__ uint32_t sm_addr(const void* p) { return uint32_t(__cvta_generic_to_shared(p)); }
@@ -582,202 +588,159 @@ __device__ __forceinline__ uint32_t cl_map(uint32_t local, uint32_t rank) {
     asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(a) : "r"(local), "r"(rank));
     return a;
 }
-__device__ __forceinline__ void cl_store(uint32_t addr, uint32_t v) {
-    asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
+__device__ __forceinline__ uint32_t cl_load(uint32_t addr) {
+    uint32_t v;
+    asm volatile("ld.shared::cluster.u32 %0, [%1];" : "=r"(v) : "r"(addr) : "memory");
+    return v;
 }
+__device__ __forceinline__ void cl_arrive() { asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory"); }
+__device__ __forceinline__ void cl_wait() { asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory"); }
 __device__ __forceinline__ void cl_sync() {
-    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+    cl_arrive();
+    cl_wait();
+}
+
+// The draw of round k from this lane's stream: 8 draws per step, the k-th kept.
+__device__ __forceinline__ uint32_t lane_draw(Xoshiro& rng, int k) {
+    uint32_t u = 0u;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const uint32_t v = rng_next(rng);
+        if (j == k) u = v;
+    }
+    return u;
 }
 
 template <int P>
 __global__ void __cluster_dims__(kCR, 1, 1) __launch_bounds__(kCT, 1)
     plain_cluster_kernel(const __grid_constant__ PlainJob job) {
-    constexpr int R = 8, NWJ = 64;
+    constexpr int NWJ = 64;
+    (void)P;
     extern __shared__ __align__(16) uint8_t smem_raw[];
-    uint32_t* Jl = reinterpret_cast<uint32_t*>(smem_raw);   // [2048][8]: owned words of every J row
-    uint32_t* flist = Jl + 2048 * 8;                        // [2048]: flipped slot | new spin -1 << 31
-    uint32_t* recv = flist + 2048;                          // [2][kCR][kCW]
-    uint32_t* comb = recv + 2 * kCR * kCW;                  // [8 warps][8 words][P]
-    uint32_t* res = comb + 8 * 8 * P;                       // [8 words][P]
-    __shared__ int s_cnt[kCT / 32];
-    __shared__ long long s_part[kCR][2];                    // rank 0: every rank's sum of s*h and of b*s
+    // J row of owned slot t: 16 chunks of 16 bytes, chunk c at position c ^ (t & 7) (conflict-free 16-byte loads)
+    uint4* Jr = reinterpret_cast<uint4*>(smem_raw);                     // [256][16]
+    uint32_t* send = reinterpret_cast<uint32_t*>(Jr + kCT * 16);         // [2 parities][8 warps][4]: F, U, n_lin
+    uint4* recv = reinterpret_cast<uint4*>(send + 2 * 8 * 4);            // [2 parities][F, U][16]: 64 words each
+    __shared__ int32_t s_nl[2];
+    __shared__ long long s_red[2][kCT / 32];
+    __shared__ long long s_part[kCR][3];                    // rank 0: every rank's sum of s*h, of b*s and flips
 
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x, lane = tid & 31, k = tid >> 5;
     const uint32_t rank = cl_rank();
     const int c = int(cl_id());                             // anneal index within the launch
     const int n = job.n, nw = job.nw, S = job.tab.S;
     const int32_t hclamp = job.hclamp;
     const int32_t* __restrict__ bias = job.bias;
+    const int slot = k * kLanes + 32 * int(rank) + lane;
+    const bool valid = slot < n;
 
-    for (int e = tid; e < 2048 * 8; e += kCT) Jl[e] = __ldg(job.planes + size_t(e >> 3) * NWJ + (e & 7) * 8 + rank);
-    cl_sync();                                              // every CTA's shared memory is set up before any store
-
-    // decider state (warp 0): lane l of this CTA owns slots i_k = k*256 + 32 rank + lane
-    Xoshiro rng;
-    int32_t hv[R];
-    uint32_t sup = 0u, dif = 0u, vm = 0u;                   // bit k: spin +1 / flipped last pass / active slot
-    uint32_t Fw[R], Nw[R];
-    int32_t nlin_prev = 0, nl = 0;
-    long long flips = 0;
-    if (warp == 0) {
-        rng_seed(rng, job.seed, job.trial_offset + uint32_t(c), 32u * rank + uint32_t(lane));
-#pragma unroll
-        for (int k = 0; k < R; ++k) {
-            const uint32_t rv = rng_next(rng);
-            const int i = k * kLanes + 32 * int(rank) + lane;
-            const bool valid = i < n;
-            const uint32_t sbit = valid ? (rv >> 31) : 1u;
-            sup |= sbit << k;
-            if (valid) vm |= 1u << k;
-            if (valid && !sbit) dif |= 1u << k;             // s_prev = +1 initially
-            hv[k] = (valid && bias) ? bias[i] : 0;
-            Fw[k] = __ballot_sync(FULL, valid);             // initial pass: F = active slots, new spin = s0
-            Nw[k] = __ballot_sync(FULL, valid && !sbit);
-        }
+    {
+        const uint4* row = reinterpret_cast<const uint4*>(job.planes + size_t(slot) * NWJ);
+        for (int ch = 0; ch < 16; ++ch) Jr[tid * 16 + (ch ^ (tid & 7))] = __ldg(row + ch);
     }
-    int pass_nf = 0, pass_mult = 1;
-    bool pass_init = true;
+
+    Xoshiro rng;
+    rng_seed(rng, job.seed, job.trial_offset + uint32_t(c), 32u * rank + uint32_t(lane));
+    const uint32_t r0 = lane_draw(rng, k);
+    bool s_up = valid ? (r0 >> 31) != 0u : true;            // padding slots: +1
+    bool df = valid && !s_up;                               // s != s_prev (s_prev = +1 initially)
+    int32_t h = (valid && bias) ? bias[slot] : 0;
+    uint32_t u = lane_draw(rng, k);                         // step 0's draw
+    int32_t nlin_prev = 0;
+    long long flips = 0;
+    // the initial pass publishes F = active slots and U = s0
+    bool fl = valid, up_new = s_up, ln = false;
+    cl_sync();                                              // every CTA's shared memory is set up before any load
+
     for (int t = -1; t < S; ++t) {
         const int par = (t + 1) & 1;
-        if (t >= 0 && warp == 0) {
+        if (t >= 0) {
             const int32_t fourT = __ldg(job.tab.fourT + t), twoT = fourT >> 1, qv = __ldg(job.tab.q + t);
             const int32_t corr = step_corr(nlin_prev, __ldg(job.tab.kcorr + t), __ldg(job.tab.kconst + t));
             const uint32_t lw = uint32_t(2 * twoT - 1);
-            nl = 0;
-#pragma unroll
-            for (int k = 0; k < R; ++k) {
-                const uint32_t u = rng_next(rng);
-                const bool valid = (vm >> k) & 1u, s_up = (sup >> k) & 1u, df = (dif >> k) & 1u;
-                hv[k] += pass_mult * dense_delta<1, P>(res + k * P, 8, 0, lane, pass_nf, pass_init || df, s_up);
-                int32_t hs = s_up ? hv[k] : -hv[k];
-                if (hclamp > 0) hs = max(-hclamp, min(hs, hclamp));
-                const int32_t x = qv + (df ? corr : -corr);
-                const int32_t zt = hs * 65536 + x;
-                const bool fl = valid && (zt - threshold16(u, fourT) < 0);
-                const bool ln = valid && (uint32_t(zt + twoT - 1) < lw);
-                const uint32_t fb = __ballot_sync(FULL, fl);
-                Fw[k] = fb;
-                Nw[k] = fb & __ballot_sync(FULL, s_up);     // flipped from +1: new spin -1
-                nl += __popc(__ballot_sync(FULL, ln));
-                if (fl) sup ^= 1u << k;
-                dif = (dif & ~(1u << k)) | (uint32_t(fl) << k);
-            }
+            int32_t hs = s_up ? h : -h;
+            if (hclamp > 0) hs = max(-hclamp, min(hs, hclamp));
+            const int32_t zt = hs * 65536 + (qv + (df ? corr : -corr));
+            fl = valid && (zt - threshold16(u, fourT) < 0);
+            ln = valid && (uint32_t(zt + twoT - 1) < lw);
+            up_new = s_up != fl;
         }
-        if (warp == 0 && lane <= 16) {
-            uint32_t v = uint32_t(nl);
-#pragma unroll
-            for (int k = 0; k < R; ++k) {
-                if (lane == k) v = Fw[k];
-                if (lane == 8 + k) v = Nw[k];
-            }
-            const uint32_t local = sm_addr(recv + (par * kCR + rank) * kCW + lane);
-#pragma unroll
-            for (int r = 0; r < kCR; ++r) cl_store(cl_map(local, uint32_t(r)), v);
+        const uint32_t fw = __ballot_sync(FULL, fl), uw = __ballot_sync(FULL, fl && up_new);
+        const uint32_t nlw = __ballot_sync(FULL, ln);
+        if (lane == 0) {
+            uint32_t* sd = send + (par * 8 + k) * 4;
+            sd[0] = fw;
+            sd[1] = uw;
+            sd[2] = uint32_t(__popc(nlw));
         }
-        cl_sync();
-        // the pass's flip list, the same in every CTA: word wi = k*8 + r (round k, source CTA r) holds slots 32 wi + b;
-        // thread tid places the flips of byte tid % 4 of word tid / 4, after a block-wide scan of the byte counts
-        int nf = 0;
-        {
-            const int wd = tid >> 2, sh = 8 * (tid & 3);
-            const uint32_t* src = recv + (par * kCR + (wd & 7)) * kCW;
-            const uint32_t F = (src[wd >> 3] >> sh) & 0xFFu, N = src[8 + (wd >> 3)] >> sh;
-            const int cnt = __popc(F);
-            int incl = cnt;
+        cl_arrive();
+        if (t >= 0) {
+            if (fl) s_up = up_new;
+            df = fl;
+            if (t + 1 < S) u = lane_draw(rng, k);            // next step's draw, while the barrier completes
+        }
+        cl_wait();
+        // flip word wi = kk*8 + rr (round kk, source CTA rr) and its new-spin word; then the n_lin partials
+        if (tid < 128) {
+            const int wi = tid & 63, kk = wi >> 3, rr = wi & 7;
+            const uint32_t v = cl_load(cl_map(sm_addr(send + (par * 8 + kk) * 4 + (tid >> 6)), uint32_t(rr)));
+            reinterpret_cast<uint32_t*>(recv + (par * 2 + (tid >> 6)) * 16)[wi] = v;
+        } else if (tid < 192) {
+            const int e = tid - 128;                        // (source CTA e / 8, warp e % 8)
+            int32_t v = int32_t(cl_load(cl_map(sm_addr(send + (par * 8 + (e & 7)) * 4 + 2), uint32_t(e >> 3))));
 #pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int y = __shfl_up_sync(FULL, incl, o);
-                if (lane >= o) incl += y;
-            }
-            if (lane == 31) s_cnt[warp] = incl;
-            __syncthreads();
-            int pos = incl - cnt;
-#pragma unroll
-            for (int w2 = 0; w2 < kCT / 32; ++w2) {
-                const int v = s_cnt[w2];
-                pos += w2 < warp ? v : 0;
-                nf += v;
-            }
-            uint32_t m = F;
-            while (m) {
-                const int b = __ffs(m) - 1;
-                m &= m - 1;
-                flist[pos++] = uint32_t(32 * wd + sh + b) | (((N >> b) & 1u) << 31);
-            }
+            for (int o = 16; o >= 1; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+            if (lane == 0) s_nl[(tid >> 5) - 4] = v;
         }
         __syncthreads();
         if (t >= 0) {
-            int32_t nlin = 0;
-#pragma unroll
-            for (int r = 0; r < kCR; ++r) nlin += int32_t(recv[(par * kCR + r) * kCW + 16]);
-            nlin_prev = nlin;
-            flips += nf;
-            if (rank == 0 && tid == 0 && job.trace && job.out_trace) job.out_trace[size_t(c) * S + t] = nlin;
+            nlin_prev = s_nl[0] + s_nl[1];
+            if (rank == 0 && tid == 0 && job.trace && job.out_trace) job.out_trace[size_t(c) * S + t] = nlin_prev;
         }
-        // counts of the owned words: warp w, lane (sub = lane / 8, word = lane % 8) takes rows f0 + sub + 4j
-        {
-            const int sub = lane >> 3, w = lane & 7;
-            BitCounter<P> cnt;
-            cnt.clear();
-            for (int f0 = warp * 32; f0 < nf; f0 += 8 * 32) {
-                uint32_t a[8];
+        // D = sum over the 64 words of popc(F & (U ^ J_y)); |F| from the same words
+        const uint4* Fv = recv + par * 2 * 16;
+        const uint4* Uv = Fv + 16;
+        const uint4* Jv = Jr + tid * 16;
+        int32_t D = 0, nf = 0;
 #pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                    const int f = f0 + sub + 4 * j;
-                    if (f < nf) {
-                        const uint32_t e = flist[f];
-                        a[j] = Jl[(e & 0x7fffffffu) * 8 + w] ^ ((e >> 31) ? FULL : 0u);
-                    } else {
-                        a[j] = 0u;
-                    }
-                }
-                cnt.add8(a);
-            }
-#pragma unroll
-            for (int o = 8; o <= 16; o <<= 1) {
-                uint32_t other[P];
-#pragma unroll
-                for (int p = 0; p < P; ++p) other[p] = __shfl_xor_sync(FULL, cnt.c[p], o);
-                cnt.add_planes(other);
-            }
-            if (sub == 0) cnt.store(comb + (warp * 8 + w) * P);
-            __syncthreads();
-            if (tid < 8) {
-                BitCounter<P> acc;
-                acc.clear();
-                for (int v = 0; v < 8; ++v) acc.add_planes(comb + (v * 8 + tid) * P);
-                acc.store(res + tid * P);
-            }
-            __syncthreads();
+        for (int ch = 0; ch < 16; ++ch) {
+            const uint4 J4 = Jv[ch ^ (tid & 7)], F4 = Fv[ch], U4 = Uv[ch];
+            D += __popc(F4.x & (U4.x ^ J4.x)) + __popc(F4.y & (U4.y ^ J4.y)) + __popc(F4.z & (U4.z ^ J4.z)) +
+                 __popc(F4.w & (U4.w ^ J4.w));
+            nf += __popc(F4.x) + __popc(F4.y) + __popc(F4.z) + __popc(F4.w);
         }
-        pass_nf = nf;
-        pass_mult = t >= 0 ? 2 : 1;
-        pass_init = t < 0;
+        if (t >= 0 && tid == 0) flips += nf;
+        // the diagonal: if y itself is in F, its term (J_yy = 0, stored as a 0 bit) was counted as -s'_y
+        if (fl) {
+            nf -= 1;
+            D -= up_new ? 1 : 0;
+        }
+        h += (t >= 0 ? 2 : 1) * (nf - 2 * D);
     }
-    // the last pass's counts, then the outputs
+    // outputs: spins, sum s*h, sum b*s (active slots), flips
     long long sh = 0, bs = 0;
-    if (warp == 0) {
-#pragma unroll
-        for (int k = 0; k < R; ++k) {
-            const bool valid = (vm >> k) & 1u, s_up = (sup >> k) & 1u, df = (dif >> k) & 1u;
-            hv[k] += pass_mult * dense_delta<1, P>(res + k * P, 8, 0, lane, pass_nf, pass_init || df, s_up);
-            const int i = k * kLanes + 32 * int(rank) + lane;
-            const uint32_t sword = __ballot_sync(FULL, s_up);
-            if (valid) {
-                sh += s_up ? hv[k] : -hv[k];
-                if (bias) bs += s_up ? bias[i] : -bias[i];
-                if (job.out_h) job.out_h[size_t(c) * n + i] = hv[k];
-            }
-            const int wi = k * 8 + int(rank);
-            if (lane == 0 && wi < nw) job.out_spins[size_t(c) * nw + wi] = sword & valid_mask(wi, n);
-        }
-        sh = warp_sum64(sh);
-        bs = warp_sum64(bs);
-        if (lane == 0) {
-            const uint32_t a = cl_map(sm_addr(&s_part[rank][0]), 0u);
-            asm volatile("st.shared::cluster.u64 [%0], %1;" ::"r"(a), "l"(sh) : "memory");
-            asm volatile("st.shared::cluster.u64 [%0], %1;" ::"r"(a + 8u), "l"(bs) : "memory");
-        }
+    if (valid) {
+        sh = s_up ? h : -h;
+        if (bias) bs = s_up ? bias[slot] : -bias[slot];
+        if (job.out_h) job.out_h[size_t(c) * n + slot] = h;
+    }
+    const uint32_t sword = __ballot_sync(FULL, s_up);
+    const int wi = k * 8 + int(rank);
+    if (lane == 0 && wi < nw) job.out_spins[size_t(c) * nw + wi] = sword & valid_mask(wi, n);
+    sh = warp_sum64(sh);
+    bs = warp_sum64(bs);
+    if (lane == 0) {
+        s_red[0][k] = sh;
+        s_red[1][k] = bs;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        long long a = 0, b = 0;
+        for (int w = 0; w < kCT / 32; ++w) { a += s_red[0][w]; b += s_red[1][w]; }
+        const uint32_t ad = cl_map(sm_addr(&s_part[rank][0]), 0u);
+        asm volatile("st.shared::cluster.u64 [%0], %1;" ::"r"(ad), "l"(a) : "memory");
+        asm volatile("st.shared::cluster.u64 [%0], %1;" ::"r"(ad + 8u), "l"(b) : "memory");
+        asm volatile("st.shared::cluster.u64 [%0], %1;" ::"r"(ad + 16u), "l"(flips) : "memory");
     }
     cl_sync();
     if (rank == 0 && tid == 0) {
@@ -785,7 +748,7 @@ __global__ void __cluster_dims__(kCR, 1, 1) __launch_bounds__(kCT, 1)
         for (int r = 0; r < kCR; ++r) { a += s_part[r][0]; b += s_part[r][1]; }
         job.out_sum_sh[c] = a;
         if (job.out_sum_bs) job.out_sum_bs[c] = b;
-        job.out_flips[c] = flips;
+        job.out_flips[c] = s_part[0][2];
     }
 }
 
