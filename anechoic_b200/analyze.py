@@ -93,7 +93,8 @@ def estimate(prefix: str) -> dict:
     Pb_ci, p_ci = wilson(kb, nb), wilson(kt, nt)
     out = {k: s.get(k) for k in ("cs", "groups", "steps", "t0", "t1", "q", "ramp", "tec_jv", "trial_offset",
                                   "engine", "kernel", "n", "gpu_before", "gpu_after")}
-    out.update(lam=s.get("lambda"), kappa=s.get("tecT_kappa"))
+    out.update(lam=s.get("lambda"), kappa=s.get("tecT_kappa"))      # the reference's estimate() names
+    out.update({"lambda": s.get("lambda"), "tecT_kappa": s.get("tecT_kappa")})   # the run files' names
     out.update(prefix=os.path.basename(prefix), B=B, batches=nb, successes=kt, trials=nt, p=p, p_wilson95=list(p_ci),
                batches_with_success=kb, P_batch=Pb, P_batch_wilson95=list(Pb_ci), t_batch_ms=t,
                t_batch_min_ms=min(b["device_ms"] for b in bat), t_batch_max_ms=max(b["device_ms"] for b in bat),

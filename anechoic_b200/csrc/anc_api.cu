@@ -134,6 +134,9 @@ struct anc_instance {
     DevBuf<int32_t> w_trace, w_h;
     DevBuf<long long> w_prof;                     // tensor-engine phase counters (opt-in)
     int prof_ctas = 0, prof_S = 0;
+    // CSR pass variant chosen by the tuner (-1: not tuned yet) and its probe's device time per step of each variant
+    int sparse_variant = -1;
+    double sparse_probe_us[anc::kSparseVariants] = {};
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     int device = 0, sms = 0;
@@ -337,9 +340,10 @@ int plan_kind(int K, int np_max, int nwj_max, int sms, KindPlan* out) {
     return ANC_OK;
 }
 
-int launch_plain_single(anc_instance* I, const anc::PlainJob& job, cudaStream_t st) {
+int launch_plain_single(anc_instance* I, const anc::PlainJob& job, cudaStream_t st, int variant = -1) {
     anc::PlainLaunch L{};
     L.job0 = job;
+    L.sparse_variant = variant >= 0 ? variant : std::max(0, I->sparse_variant);
     L.jobs = nullptr;
     L.items = nullptr;
     L.nitems = job.ntrials;
@@ -477,9 +481,55 @@ int run_device_impl(anc_instance* I, anc_tables* tb, uint64_t seed, uint32_t off
         g_last_kernel = ANC_KERNEL_PLAIN_CLUSTER;
         return ANC_OK;
     }
-    rc = launch_plain_single(I, job, st);
+    const int forced = o ? o->sparse_variant : 0;
+    rc = launch_plain_single(I, job, st, forced > 0 ? forced - 1 : -1);
     if (rc == ANC_OK) g_last_kernel = ANC_KERNEL_PLAIN;
     return rc;
+}
+
+// Run-time tuner of the CSR pass (the plain engine on sparse instances): on the first synchronous run of an
+// instance, each compiled variant (kSparseVariantShape: rows in flight per lane group x edges per lane) runs the
+// first min(S, 64) steps of min(nchains, one wave) anneals of that run -- twice, the second launch timed with CUDA
+// events -- and the fastest is kept for every later launch of the instance (device, batch and graph-captured
+// launches included). Every variant computes the same fields; only the time differs. The probes write into the
+// handle's own workspaces, never into the caller's outputs.
+int tune_sparse(anc_instance* I, anc_tables* tb, uint64_t seed, uint32_t off, int nchains, const anc_run_opts* o) {
+    if (I->K != 0 || I->sparse_variant >= 0) return ANC_OK;
+    int32_t hclamp = 0;
+    int rc = resolve_clamp(I, tb, o, &hclamp);
+    if (rc) return rc;
+    const int P = plain_P(I->np);
+    bool stream = false;
+    size_t smem = 0;
+    int per_sm = 0;
+    rc = plain_residency(I, P, &smem, &stream, &per_sm);
+    if (rc) return rc;
+    const int np = std::max(1, std::min(nchains, per_sm * I->sms));
+    const int Sp = std::min(tb->S, 64);
+    CK(I->w_spins.ensure(size_t(I->nw) * np));
+    CK(I->w_sh.ensure(np));
+    CK(I->w_bs.ensure(np));
+    CK(I->w_fl.ensure(np));
+    OutPtrs out{I->w_spins.p, I->w_sh.p, I->w_bs.p, I->w_fl.p, nullptr, nullptr};
+    anc::PlainJob job = make_job(I, tb, seed, off, np, hclamp, out);
+    job.tab.S = Sp;
+    cudaStream_t st = I->stream;
+    int best = 0;
+    for (int v = 0; v < anc::kSparseVariants; ++v) {
+        float ms = 0.f;
+        for (int rep = 0; rep < 2; ++rep) {
+            CK(cudaEventRecord(I->ev0, st));
+            rc = launch_plain_single(I, job, st, v);
+            if (rc) return rc;
+            CK(cudaEventRecord(I->ev1, st));
+            CK(cudaEventSynchronize(I->ev1));
+            CK(cudaEventElapsedTime(&ms, I->ev0, I->ev1));
+        }
+        I->sparse_probe_us[v] = 1000.0 * double(ms) / Sp;
+        if (I->sparse_probe_us[v] < I->sparse_probe_us[best]) best = v;
+    }
+    I->sparse_variant = best;
+    return ANC_OK;
 }
 
 int run_host_impl(anc_instance* I, anc_tables* tb, uint64_t seed, uint32_t off, int nchains, const anc_run_opts* o,
@@ -498,6 +548,10 @@ int run_host_impl(anc_instance* I, anc_tables* tb, uint64_t seed, uint32_t off, 
     OutPtrs out{I->w_spins.p, I->w_sh.p, I->w_bs.p, I->w_fl.p, trace ? I->w_trace.p : nullptr,
                 fields ? I->w_h.p : nullptr};
     cudaStream_t st = I->stream;
+    if (I->K == 0 && !(o && o->sparse_variant > 0)) {
+        const int trc = tune_sparse(I, tb, seed, off, nchains, o);
+        if (trc) return trc;
+    }
     CK(cudaEventRecord(I->ev0, st));
     int rc = run_device_impl(I, tb, seed, off, nchains, o, out, st);
     if (rc) return rc;
@@ -620,6 +674,13 @@ int anc_last_profile(double* out, int max) {
 }
 const char* anc_version(void) { return "anechoic-b200 0.1 (sm_100a)"; }
 double anc_last_device_ms(void) { return g_dev_ms; }
+int anc_sparse_tuning(const anc_instance* I, int* variant, double* probe_us) {
+    if (!I) return fail(ANC_EINVAL, "null handle");
+    if (variant) *variant = I->K == 0 ? I->sparse_variant : -1;
+    if (probe_us)
+        for (int v = 0; v < anc::kSparseVariants; ++v) probe_us[v] = I->sparse_probe_us[v];
+    return ANC_OK;
+}
 int anc_set_wait_ns(uint64_t ns) {
     g_wait_ns.store(ns);
     return ANC_OK;
@@ -936,6 +997,24 @@ int anc_run_batch(int njobs, const anc_job* jobs, const anc_run_opts* o) {
             if (rc) return rc;
         }
     }
+    // the CSR pass variant of the batch's sparse launch: forced by the options, else the tuned variant of its costliest
+    // sparse job (tuned now, on that job, if it has not been)
+    int sparse_variant = (o && o->sparse_variant > 0) ? o->sparse_variant - 1 : -1;
+    if (sparse_variant < 0) {
+        int big = -1;
+        double cost = -1.0;
+        for (int k = 0; k < njobs; ++k)
+            if (jobs[k].inst->K == 0) {
+                const double c = double(jobs[k].inst->np) * jobs[k].tb->S * jobs[k].nchains;
+                if (c > cost) { cost = c; big = k; }
+            }
+        if (big >= 0) {
+            const anc_job& j = jobs[big];
+            const int rc = tune_sparse(j.inst, j.tb, j.seed, j.trial_offset, j.nchains, o);
+            if (rc) return rc;
+            sparse_variant = j.inst->sparse_variant;
+        }
+    }
     cudaStream_t st = nullptr;
     CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     std::unique_ptr<CUstream_st, void (*)(cudaStream_t)> st_guard(st, [](cudaStream_t s) { cudaStreamDestroy(s); });
@@ -998,6 +1077,7 @@ int anc_run_batch(int njobs, const anc_job* jobs, const anc_run_opts* o) {
         if (e != cudaSuccess) return drain(cuda_fail(e, "work items"));
         const KindPlan& kp = plans[ki];
         anc::PlainLaunch L{};
+        if (K == 0) L.sparse_variant = sparse_variant >= 0 ? sparse_variant : 0;
         L.jobs = d_jobs.p;
         L.items = d_items[ki].p;
         L.nitems = int(it.size());

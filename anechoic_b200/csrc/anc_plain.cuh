@@ -58,7 +58,13 @@ struct PlainLaunch {
     int* next_item;                    // queue head (zeroed before launch)
     int np_max, nwj_max;               // shared-memory layout
     int stream;                        // 1: dense counts go into the fields set by set (one result buffer)
+    int sparse_variant;                // CSR pass variant (kSparseVariants index; 0 = rows 1 x edges 8 per lane)
 };
+
+// CSR pass variants the host's tuner chooses among: {lane groups' rows in flight, edges per lane fetched before any
+// is applied}. Every variant computes the same fields (integer atomics into shared memory), only the time differs.
+constexpr int kSparseVariants = 4;
+constexpr int kSparseVariantShape[kSparseVariants][2] = {{1, 8}, {1, 4}, {2, 4}, {1, 16}};
 
 // Shared-memory bytes for a launch (P = counter planes).
 inline size_t plain_smem_bytes(int np_max, int nwj_max, int K, int P, bool stream = false) {

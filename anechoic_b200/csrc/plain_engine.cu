@@ -317,15 +317,10 @@ __device__ __forceinline__ void dense_pass(const uint32_t* __restrict__ planes, 
 // Integer adds in any order: bit-exact. On a B200, over the 51-instance sparse batch (degrees 4 ... 48), one row per
 // group with 8 edges per lane took 134 ms per launch and 4 rows x 2 edges 208 ms; a warp per row, one row at a time,
 // took 684 ms.
-#ifndef ANC_SPARSE_BATCH
-#define ANC_SPARSE_BATCH 1
-#endif
-#ifndef ANC_SPARSE_EDGES
-#define ANC_SPARSE_EDGES 8
-#endif
-constexpr int kSparseBatch = ANC_SPARSE_BATCH, kSparseEdges = ANC_SPARSE_EDGES;
-
+// Sparse pass variants (rows per lane group in flight, edges fetched per lane before any is applied), chosen per
+// instance at run time by the host's tuner (anc_api.cu): kSparseVariants[v] = {batch, edges}.
 // log2 of the lanes per row: the power of two at or above mean degree / kSparseEdges, at most 32.
+template <int kSparseEdges>
 __device__ __forceinline__ int sparse_lanes_log2(int nnz, int n) {
     const int deg = (nnz + kSparseEdges * n - 1) / (kSparseEdges * max(n, 1));
     int lg = 0;
@@ -333,6 +328,7 @@ __device__ __forceinline__ int sparse_lanes_log2(int nnz, int n) {
     return lg;
 }
 
+template <int kSparseBatch, int kSparseEdges>
 __device__ __forceinline__ void sparse_pass(const int32_t* __restrict__ row_ptr, const uint32_t* __restrict__ adj,
                                             const uint32_t* flist, int nf, int lg, int32_t* h, int mult) {
     const int G = 1 << lg, sub = threadIdx.x & (G - 1), NG = T >> lg;
@@ -404,7 +400,7 @@ __device__ __forceinline__ void apply_dense(const uint32_t* res, int nwj, const 
     }
 }
 
-template <int K, int P, bool SPARSE, bool STREAM>
+template <int K, int P, bool SPARSE, bool STREAM, int SB = 1, int SE = 8>
 __global__ void __launch_bounds__(T, 1) plain_kernel(const __grid_constant__ PlainLaunch L) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
     __shared__ int s_item, s_nf, s_lin[8], s_wsum[T / 32];
@@ -460,9 +456,9 @@ __global__ void __launch_bounds__(T, 1) plain_kernel(const __grid_constant__ Pla
         }
         __syncthreads();
         const int nf0 = s_nf;
-        const int sparse_lg = SPARSE ? sparse_lanes_log2(__ldg(job.row_ptr + n), n) : 0;
+        const int sparse_lg = SPARSE ? sparse_lanes_log2<SE>(__ldg(job.row_ptr + n), n) : 0;
         if (SPARSE) {
-            sparse_pass(job.row_ptr, job.adj, flist, nf0, sparse_lg, h, 1);
+            sparse_pass<SB, SE>(job.row_ptr, job.adj, flist, nf0, sparse_lg, h, 1);
         } else {
             dense_pass<K, P, STREAM>(planes, plane_stride, nwj, nf0, flist, comb, res, h, n, 1);
             if (!STREAM) {
@@ -512,7 +508,7 @@ __global__ void __launch_bounds__(T, 1) plain_kernel(const __grid_constant__ Pla
             nlin_prev = nlin;
             if (nf > 0) {
                 if (SPARSE) {
-                    sparse_pass(job.row_ptr, job.adj, flist, nf, sparse_lg, h, 2);
+                    sparse_pass<SB, SE>(job.row_ptr, job.adj, flist, nf, sparse_lg, h, 2);
                 } else {
                     dense_pass<K, P, STREAM>(planes, plane_stride, nwj, nf, flist, comb, res, h, n, 2);
                     if (!STREAM) {
@@ -752,9 +748,9 @@ __global__ void __cluster_dims__(kCR, 1, 1) __launch_bounds__(kCT, 1)
     }
 }
 
-template <int K, int P, bool SPARSE, bool STREAM = false>
+template <int K, int P, bool SPARSE, bool STREAM = false, int SB = 1, int SE = 8>
 int launch_t(const PlainLaunch& L, int grid, size_t smem, cudaStream_t st) {
-    auto fn = plain_kernel<K, P, SPARSE, STREAM>;
+    auto fn = plain_kernel<K, P, SPARSE, STREAM, SB, SE>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return int(e);
     fn<<<grid, T, smem, st>>>(L);
@@ -774,7 +770,14 @@ int occ_t(size_t smem, int* out) {
 // K: 0 = sparse, 1/2/4 dense planes. P: 12 or 16 counter planes (dense only). L.stream selects the streaming layout
 // (K = 2 / 4, P = 16 only: it is needed only for NP > 8192).
 int plain_launch(const PlainLaunch& L, int K, int P, int grid, size_t smem, cudaStream_t st) {
-    if (K == 0) return launch_t<1, 12, true>(L, grid, smem, st);
+    if (K == 0) {
+        switch (L.sparse_variant) {
+            case 1: return launch_t<1, 12, true, false, 1, 4>(L, grid, smem, st);
+            case 2: return launch_t<1, 12, true, false, 2, 4>(L, grid, smem, st);
+            case 3: return launch_t<1, 12, true, false, 1, 16>(L, grid, smem, st);
+            default: return launch_t<1, 12, true, false, 1, 8>(L, grid, smem, st);
+        }
+    }
     if (L.stream) {
         if (P == 16 && K == 2) return launch_t<2, 16, false, true>(L, grid, smem, st);
         if (P == 16 && K == 4) return launch_t<4, 16, false, true>(L, grid, smem, st);

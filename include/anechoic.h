@@ -115,8 +115,19 @@ typedef struct {
     int tensor_kind; /* ANC_TENSOR_*: operand format of the tensor engine's field update */
     int flip_permille; /* AUTO's flip fraction (flips per spin per step) x 1000; 0 = the fraction the last anc_run /
                           anc_run_fields of these tables on this instance saw, else 0.25 */
-    int reserved[2];
+    int sparse_variant; /* CSR instances on the plain engine: 0 = the variant the run-time tuner chose for the instance
+                           (anc_sparse_tuning), v + 1 = force variant v (0 .. 3) */
+    int reserved;
 } anc_run_opts;
+
+/* No counterpart in the reference (its kernel geometry is fixed per build by flags, sca_gpu_bias.cu:637-644). The
+ * run-time tuner of the plain engine's CSR pass: on an instance's first synchronous run (anc_run / anc_run_fields /
+ * anc_run_batch) each compiled variant -- lane groups x edges fetched per lane before any is applied: {1, 8},
+ * {1, 4}, {2, 4}, {1, 16} -- runs the first min(S, 64) steps of up to one wave of that run's anneals into the handle's
+ * own workspaces (twice; the second launch is timed), and the fastest is used for every later launch of the
+ * instance. Writes the chosen variant (-1 = not tuned yet, or not a CSR instance) and probe_us[4], each variant's
+ * probe time per step in microseconds (may be NULL). */
+ANC_API int anc_sparse_tuning(const anc_instance* inst, int* variant, double* probe_us);
 
 /* No counterpart in the reference (its CLI has one engine). The cost model behind ANC_ENGINE_AUTO, host-only: the
  * estimated device time in microseconds of nchains anneals of S steps on each engine, for n spins with kbits-bit dense

@@ -74,3 +74,38 @@ def test_refused_batch_enqueues_nothing(cuda):
     # the valid job alone runs
     outs = A.run_batch([dict(dev=devs[0], tb=tb, seed=1, trial_offset=0, nchains=2)])
     assert int(outs[0].flips.sum()) > 0
+
+
+def test_sparse_tuner_variants_agree_and_pick_is_recorded(cuda, oracle):
+    """The run-time tuner of the CSR pass: every compiled variant gives the same bits (forced through the options),
+    the first synchronous run records each variant's probe time and keeps the fastest for later launches."""
+    import ctypes as C
+    import numpy as np
+    from anechoic_b200 import _lib
+    L = _lib.load()
+    inst = I.torus(60, 80, 11, True, bmax=2)
+    dev = A.DeviceInstance(inst)
+    tb = A.Tables.from_schedule(A.Schedule(**SCHED))
+    v = C.c_int(7)
+    us = (C.c_double * 4)()
+    L.anc_sparse_tuning(dev._h, C.byref(v), us)
+    assert v.value == -1                                   # not tuned before the first synchronous run
+    ref = oracle.run_batch(inst.n, oracle.tables(**SCHED), 3, 40, 20, csr=inst.to_csr(), bias=inst.bias)
+    outs = []
+    for forced in range(1, 5):
+        o = _lib.opts("plain")
+        o.sparse_variant = forced
+        r = A.RunResult(n=inst.n, trial_offset=40, spins=np.zeros((20, A.spin_words(inst.n)), np.uint64),
+                        sum_sh=np.zeros(20, np.int64), sum_bs=np.zeros(20, np.int64), flips=np.zeros(20, np.int64),
+                        trace=np.zeros((20, SCHED["S"]), np.int32))
+        _lib.check(L.anc_run(dev._h, tb._h, 3, 40, 20, C.byref(o), r.spins.ctypes.data, r.sum_sh.ctypes.data,
+                             r.sum_bs.ctypes.data, r.flips.ctypes.data, r.trace.ctypes.data))
+        for c in range(20):
+            assert_same(r, {k: val[c] for k, val in ref.items()}, c, f"variant {forced - 1} chain {c}")
+        outs.append(r)
+    L.anc_sparse_tuning(dev._h, C.byref(v), us)
+    assert v.value == -1                                   # forced runs do not tune
+    A.run(dev, tb, 3, 40, 20, engine="plain")              # the first unforced synchronous run tunes
+    L.anc_sparse_tuning(dev._h, C.byref(v), us)
+    assert 0 <= v.value < 4 and all(us[k] > 0 for k in range(4))
+    assert us[v.value] == min(us[k] for k in range(4))
