@@ -834,33 +834,31 @@ __global__ void __launch_bounds__(kResThreads, 1)
 // (128 rows x 2048 fp4 = 128 KB) resident, and runs one group of 128 replicas at a time. Per step:
 //   8 decision warps: thread (replica r, half hf) owns quarters qq = 2hf, 2hf+1; quarter qq is lanes
 //     16cs + 4qq + j (j < 4) x 8 rounds = 32 slots = TMEM columns qq*32 + j*8 + k. The step's draws were made while
-//     the previous step's MMAs ran (the lane states live in TMEM); the thread reads its 64 fields, decides, and
-//     publishes its 64 D nibbles (32 bytes) and its two n_lin partial counts to the group's exchange buffer in
-//     L2 as tagged words: each 64-bit word holds 4 payload bytes and the 32-bit tag m + 2 of the step that wrote it,
-//     stored with one naturally aligned 64-bit access (single-copy atomic), so a reader that sees the tag sees the
-//     payload. No fence, no flag and no CTA barrier stand between a decision and its publication.
-//   The same warps then fetch the step's D: tile t (128 replicas x 256 K, the slices of CTAs 2t and 2t+1) is read
-//     as 32 KB of tagged words (each warp load instruction reads 512 contiguous bytes), re-read where a tag is not
-//     yet this step's, and its payload stored into a stage of a 6-deep shared-memory ring in the 128-byte-swizzled
-//     K-major layout the MMA reads; one tile's loads are in flight while the previous tile is checked and stored.
-//     Each thread fences the async proxy and one lane per warp arrives on the stage's barrier. Each thread also
-//     sums its replica's 32 n_lin partials for the next step's correction.
+//     the previous step's MMAs ran (the lane states live in TMEM); the thread reads its 64 fields, decides,
+//     writes its 64 D nibbles (32 bytes) and two n_lin partial bytes to the group's exchange buffers, and after a
+//     named barrier one thread publishes flag[g][cs] = m + 2 with a release store (the barrier orders every
+//     writer's stores before it, and release is cumulative over them).
+//   The same warps then fetch the step's D: tile t (128 replicas x 256 K, the slices of CTAs 2t and 2t+1) is
+//     loaded once both slice flags are seen, with 16-byte asynchronous L2 copies (four per thread, up to 6 tiles in flight),
+//     into a stage of a 6-deep shared-memory ring in the 128-byte-swizzled K-major layout the MMA reads; each
+//     thread fences the async proxy and one lane per warp arrives on the stage's barrier. Each thread also sums
+//     its replica's 64 n_lin partial bytes for the next step's correction.
 //   The MMA thread: 4 mxf4 MMAs per tile into the fp32 fields in TMEM, a commit per stage to free it, and a commit
 //     of "fields ready" after the 8th tile.
-// A slice's exchange buffer is double-buffered by step parity and is rewritten two steps later only by a CTA that
-// has received every slice of the step in between, which no CTA publishes before it has read the previous step's
-// slices: a reader never sees a buffer overwritten under it. The buffers are zeroed per launch (tag 0 is never a
-// step's). The exchange crosses L2 through the generic proxy only; the async proxy reads shared memory alone, after
-// the loaders' proxy fence. Every wait is bounded (%globaltimer).
+//   The poller warp: watches the 16 slice flags of the group in L2 and mirrors what it sees into shared memory
+//     (acquire at gpu scope, release at cta scope), so the decision warps wait on shared memory.
+// The exchange crosses L2 through the generic proxy only; the async proxy reads shared memory alone, after the
+// loaders' proxy fence. 10 warps leave 168 registers per thread (a fifth warp on an SM sub-partition would cap
+// them at 96).
 constexpr int kF4Slices = 16;
 constexpr int kF4YS = 128;
 constexpr int kF4DW = 8;                  // decision warps (two quarters of 32 columns per thread)
 constexpr int kF4Stages = 6;
 constexpr int kF4Tiles = 8;               // D tiles per step (2048 fp4 = 1024 bytes per row, 128 bytes per tile)
 constexpr int kF4MmaWarp = kF4DW;
-constexpr int kF4Threads = (kF4DW + 1) * 32;
-constexpr int kF4Cluster = 1;            // CTAs per cluster (1: the scheduler spreads a group's slices)
-constexpr int kF4LLRow = 16;             // tagged words per (slice, replica row): 64 payload bytes
+constexpr int kF4PollWarp = kF4DW + 1;   // watches the group's 16 slice flags for the whole CTA
+constexpr int kF4Threads = (kF4DW + 2) * 32;
+constexpr int kF4Cluster = 1;            // CTAs per cluster (1: the scheduler spreads a group's slices; 4 GPC-local measured slower)
 constexpr int kF4SfCol = 160;             // TMEM columns 144..255 hold scale factors 0x7F (1.0)
 constexpr int kF4RngCol = 256;            // TMEM columns 256..319: RNG lane states, 32 per half hf
 constexpr int kF4TmemCols = 512;
@@ -877,8 +875,9 @@ struct F4Params {
     uint64_t seed;
     uint32_t trial_offset;
     int nchains;
-    uint64_t* ll;                       // [ngroups][2][16 slices][128 rows][16] tagged words of packed e2m1 D (zeroed)
-    uint64_t* nll;                      // [ngroups][2][128 rows][16 slices][2 halves] tagged n_lin partials (zeroed)
+    uint32_t* flags;                    // [ngroups][16] (zeroed)
+    uint8_t* dbuf;                      // [ngroups][2][128][1024] packed e2m1
+    int8_t* nlx;                        // [ngroups][2][128][128]: byte 4 cs + qq = partial n_lin
     uint64_t wait_ns;                   // limit of each wait of the exchange (the drain at exit keeps its own)
     uint32_t* out_spins;                // [nchains][64] (zeroed)
     unsigned long long* out_sum_sh;
@@ -968,82 +967,74 @@ struct F4ExMarks {
     long long flags0, flags7, stored0, stored7;
 };
 
-// Tagged exchange words: payload in the low 32 bits, the writer's step tag in the high 32 bits. Two words per access,
-// each a naturally aligned 64-bit element (single-copy atomic); relaxed at gpu scope, so the loads are served by L2.
-__device__ __forceinline__ void ll_store2(uint64_t* p, uint32_t d0, uint32_t d1, uint32_t tag) {
-    const uint64_t w0 = uint64_t(d0) | (uint64_t(tag) << 32), w1 = uint64_t(d1) | (uint64_t(tag) << 32);
-    asm volatile("st.relaxed.gpu.global.v2.u64 [%0], {%1, %2};" ::"l"(p), "l"(w0), "l"(w1) : "memory");
+// 16-byte global -> shared copy through L2 only (cp.async.cg), and its commit-group bookkeeping.
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
 }
-__device__ __forceinline__ void ll_load2(const uint64_t* p, uint64_t& a, uint64_t& b) {
-    asm volatile("ld.relaxed.gpu.global.v2.u64 {%0, %1}, [%2];" : "=l"(a), "=l"(b) : "l"(p) : "memory");
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// Wait until at most n of this thread's commit groups are pending (n folds to a constant once the caller's loop is
+// unrolled; larger n waits for all).
+__device__ __forceinline__ void cp_async_wait(int n) {
+    switch (n) {
+        case 1: asm volatile("cp.async.wait_group 1;" ::: "memory"); break;
+        case 2: asm volatile("cp.async.wait_group 2;" ::: "memory"); break;
+        case 3: asm volatile("cp.async.wait_group 3;" ::: "memory"); break;
+        case 4: asm volatile("cp.async.wait_group 4;" ::: "memory"); break;
+        case 5: asm volatile("cp.async.wait_group 5;" ::: "memory"); break;
+        case 6: asm volatile("cp.async.wait_group 6;" ::: "memory"); break;
+        default: asm volatile("cp.async.wait_group 0;" ::: "memory"); break;
+    }
 }
-__device__ __forceinline__ bool ll_tagged(uint64_t a, uint64_t b, uint32_t tag) {
-    return uint32_t(a >> 32) == tag && uint32_t(b >> 32) == tag;
-}
-
-// One tile of one step in flight: the 8 tagged-word pairs (16 bytes of payload) this thread moves.
-struct F4Piece {
-    uint64_t w[16];
-};
 
 // Fetch one step's D (step m, parity m & 1; m = -1 is the initial state) into the ring: 8 tiles at ring positions
-// q .. q+7, by the 256 decision threads. Ring position t holds K chunk tk = (t + rot) mod 8 (a CTA starts with the
-// tile holding its own slice): the slices 2tk (tile bytes 0..63 of each row) and 2tk+1 (64..127). Warp w moves tile
-// rows 16w .. 16w+15: its load instruction i reads 512 contiguous bytes of tagged words, rows 16w + 4(i mod 4) ..
-// +3 of slice 2tk + i/4, lane -> row + lane/8, 16-byte piece lane mod 8 (two words = 8 payload bytes = the half
-// lane mod 2 of 16-byte chunk (lane mod 8)/2 of that slice's row). Tile t + 1's loads are issued before tile t is
-// checked: pieces whose tags are not yet m + 2 are re-read (bounded), then every payload is stored at its
-// 128-byte-swizzled position, the thread fences the async proxy and its warp arrives on the stage's barrier. Tiles
-// 6 and 7 wait for the MMAs of tiles 0 and 1 to free their stages. Returns the replica's n_lin (the sum of its 32
-// tagged partials) when want_nlin, else 0. ok (warp-uniform) is false once this warp saw an error; after an error
-// the warp stops storing and arriving.
+// q .. q+7, by the 256 decision threads: warp w copies tile rows 16w .. 16w+15, its copy instruction c covering the
+// four whole 128-byte rows 16w + 4c .. 16w + 4c + 3 (lane: row + lane / 8, 16-byte chunk lane % 8), so each
+// instruction touches four cache lines. Copies are asynchronous,
+// one commit group per tile. Ring position t holds K chunk (t + rot) mod 8, so a CTA starts with the tile holding its
+// own slice. Tile t goes out as soon as its two slices are published, and tile t - 1 is marked full right after, so
+// the MMAs start on the first tile while later slices are still being published (marking tiles 0-3 full only after
+// tiles 0-5 had gone out cost 6 % of the step). Tile 6 and 7 wait for the MMAs of tiles 0 and 1 to free their
+// stages; those tiles were marked full before. A tile is marked full once its group has landed: the thread fences the
+// async proxy and its warp arrives on the stage's barrier. Returns the replica's n_lin (the sum of its 64 partial
+// bytes) when want_nlin, else 0. ok (warp-uniform) is false once this warp saw an error; every wait is bounded, and
+// after an error the warp stops copying and arriving but still waits for the copies it has in flight.
 __device__ __forceinline__ int32_t f4_exchange(const F4Params& P, int g, int m, uint32_t stages_u32, uint32_t bar_full,
-                                               uint32_t bar_empty, uint32_t q, int tid, int r, bool want_nlin, int rot,
-                                               bool& ok, bool prof, F4ExMarks& mk) {
+                                               uint32_t bar_empty, uint32_t q, int tid, int r, bool want_nlin,
+                                               const uint32_t* s_flag, uint32_t tbase, int rot, bool& ok, bool prof,
+                                               F4ExMarks& mk) {
     constexpr uint32_t TILE = kM * kKChunk;
     static_assert(kF4Stages >= 2 && kF4Tiles == 8, "rotation by a 3-bit mask, and two stages in flight");
-    const int lane = tid & 31, warp = tid >> 5;
+    const int lane = tid & 31;
     int* err = P.err;
     const int par = m & 1;
-    const uint32_t tag = uint32_t(m + 2);
-    const uint64_t* llg = P.ll + size_t(g * 2 + par) * kF4Slices * kM * kF4LLRow;
-    const int prow = warp * 16 + (lane >> 3);               // first row of this lane's pieces (+4 per instruction)
-    const int piece = lane & 7, chunk = piece >> 1, half = piece & 1;
-    auto load = [&](int t, F4Piece& v) {
-        const int tk = (t + rot) & (kF4Tiles - 1);
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const int slice = 2 * tk + (i >> 2), row = prow + 4 * (i & 3);
-            ll_load2(llg + (size_t(slice) * kM + row) * kF4LLRow + piece * 2, v.w[2 * i], v.w[2 * i + 1]);
-        }
-    };
-    auto finish = [&](int t, F4Piece& v) {
+    const uint32_t target = tbase + uint32_t(m + 2);    // the slice flags' value for step m, in the mirror's count
+    const int row0 = (tid >> 5) * 16 + (lane >> 3), ch = lane & 7;    // first tile row, 16-byte chunk of this thread
+    const uint8_t* src = P.dbuf + (size_t(g * 2 + par) * kM + row0) * 1024 + ch * 16;
+    // 128-byte swizzle: chunk ch of row x at ch ^ (x mod 8); rows row0 + 4c have x mod 8 = (row0 mod 8) ^ 4 (c & 1)
+    const uint32_t dst0 = uint32_t(row0 * 128 + ((ch ^ (row0 & 7)) << 4));
+    const uint32_t dst1 = uint32_t(row0 * 128 + ((ch ^ ((row0 + 4) & 7)) << 4));
+    // copy tile t into its stage once its slices are published (and, for t >= 6, its stage is free)
+    auto issue = [&](int t) {
         const uint32_t qt = q + uint32_t(t), s = qt % kF4Stages, u = qt / kF4Stages;
-        const int tk = (t + rot) & (kF4Tiles - 1);
+        const int tk = (t + rot) & (kF4Tiles - 1);     // K chunk of ring position t (the CTA's own tile first)
         if (ok && u >= 1) ok = __all_sync(0xffffffffu, mbar_wait_for(bar_empty + 8 * s, (u - 1) & 1u, err, kErrEmpty, P.wait_ns));
         if (ok) {
-            uint32_t pending = 0u;
-#pragma unroll
-            for (int i = 0; i < 8; ++i)
-                if (!ll_tagged(v.w[2 * i], v.w[2 * i + 1], tag)) pending |= 1u << i;
-            uint64_t t0 = 0;
-            for (uint32_t k = 1; pending; ++k) {
-#pragma unroll
-                for (int i = 0; i < 8; ++i)
-                    if ((pending >> i) & 1u) {
-                        const int slice = 2 * tk + (i >> 2), row = prow + 4 * (i & 3);
-                        ll_load2(llg + (size_t(slice) * kM + row) * kF4LLRow + piece * 2, v.w[2 * i], v.w[2 * i + 1]);
-                    }
-#pragma unroll
-                for (int i = 0; i < 8; ++i)
-                    if (((pending >> i) & 1u) && ll_tagged(v.w[2 * i], v.w[2 * i + 1], tag)) pending &= ~(1u << i);
-                if (k == 1) t0 = globaltimer();
-                else if ((k & 63u) == 0 && pending && globaltimer() - t0 > P.wait_ns) {
+            // both slices published: every lane acquires the poller's mirror of their flags (cta scope; the poller
+            // acquired them at gpu scope)
+            const uint32_t fa = smem_u32(s_flag + 2 * tk), fb = smem_u32(s_flag + 2 * tk + 1);
+            const uint64_t t0 = globaltimer();
+            bool seen = false;
+            for (uint32_t k = 1;; ++k) {
+                uint32_t va, vb;
+                asm volatile("ld.acquire.cta.shared::cta.u32 %0, [%1];" : "=r"(va) : "r"(fa) : "memory");
+                asm volatile("ld.acquire.cta.shared::cta.u32 %0, [%1];" : "=r"(vb) : "r"(fb) : "memory");
+                if (va >= target && vb >= target) { seen = true; break; }
+                if ((k & 255u) == 0 && globaltimer() - t0 > P.wait_ns) {
                     atomicCAS(err, 0, kErrFlag);
                     break;
                 }
             }
-            ok = __all_sync(0xffffffffu, pending == 0u);
+            ok = __all_sync(0xffffffffu, seen);
         }
         if (prof && lane == 0) {
             if (t == 0) mk.flags0 = clock64();
@@ -1052,59 +1043,45 @@ __device__ __forceinline__ int32_t f4_exchange(const F4Params& P, int g, int m, 
         if (ok) {
             const uint32_t st = stages_u32 + s * TILE;
 #pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                const int row = prow + 4 * (i & 3), ch = 4 * (i >> 2) + chunk;
-                const uint32_t dst = st + uint32_t(row * 128 + ((ch ^ (row & 7)) << 4) + half * 8);
-                asm volatile("st.shared.v2.u32 [%0], {%1, %2};" ::"r"(dst), "r"(uint32_t(v.w[2 * i])),
-                             "r"(uint32_t(v.w[2 * i + 1]))
-                             : "memory");
-            }
+            for (int c = 0; c < 4; ++c)
+                cp_async16(st + uint32_t(c * 512) + ((c & 1) ? dst1 : dst0), src + size_t(c) * 4096 + tk * 128);
+        }
+        cp_async_commit();          // one group per tile, empty when the copies were skipped
+    };
+    // mark tile t full once its group has landed; `later` groups were committed after it
+    auto arrive = [&](int t, int later) {
+        cp_async_wait(later);
+        if (ok) {
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncwarp();
-            if (lane == 0) mbar_arrive(bar_full + 8 * s);
+            if (lane == 0) mbar_arrive(bar_full + 8 * ((q + uint32_t(t)) % kF4Stages));
         }
         if (prof && lane == 0) {
             if (t == 0) mk.stored0 = clock64();
             if (t == kF4Tiles - 1) mk.stored7 = clock64();
         }
     };
-    F4Piece va, vb;
-    load(0, va);
+    issue(0);
 #pragma unroll
-    for (int t = 0; t < kF4Tiles; t += 2) {
-        load(t + 1, vb);
-        finish(t, va);
-        if (t + 2 < kF4Tiles) load(t + 2, va);
-        finish(t + 1, vb);
+    for (int t = 1; t < kF4Tiles; ++t) {
+        issue(t);
+        arrive(t - 1, 1);
     }
+    arrive(kF4Tiles - 1, 0);
     int32_t nl = 0;
     if (ok && want_nlin) {
-        // the replica's 16 slices x 2 halves of partial counts (bytes 0 and 1 of each payload)
-        const uint64_t* np = P.nll + (size_t(g * 2 + par) * kM + r) * (2 * kF4Slices);
-        uint64_t w[32];
+        // every warp saw all 16 flags before its last tile
+        const uint4* np = reinterpret_cast<const uint4*>(P.nlx + (size_t(g * 2 + par) * kM + r) * 128);
+        uint4 nv[4];
 #pragma unroll
-        for (int i = 0; i < 16; ++i) ll_load2(np + 2 * i, w[2 * i], w[2 * i + 1]);
-        uint32_t pending = 0u;
+        for (int i = 0; i < 4; ++i) nv[i] = __ldcg(np + i);
 #pragma unroll
-        for (int i = 0; i < 16; ++i)
-            if (!ll_tagged(w[2 * i], w[2 * i + 1], tag)) pending |= 1u << i;
-        uint64_t t0 = 0;
-        for (uint32_t k = 1; pending; ++k) {
-#pragma unroll
-            for (int i = 0; i < 16; ++i)
-                if ((pending >> i) & 1u) ll_load2(np + 2 * i, w[2 * i], w[2 * i + 1]);
-#pragma unroll
-            for (int i = 0; i < 16; ++i)
-                if (((pending >> i) & 1u) && ll_tagged(w[2 * i], w[2 * i + 1], tag)) pending &= ~(1u << i);
-            if (k == 1) t0 = globaltimer();
-            else if ((k & 63u) == 0 && pending && globaltimer() - t0 > P.wait_ns) {
-                atomicCAS(err, 0, kErrFlag);
-                break;
-            }
+        for (int i = 0; i < 4; ++i) {
+            nl = __dp4a(int(nv[i].x), 0x01010101, nl);
+            nl = __dp4a(int(nv[i].y), 0x01010101, nl);
+            nl = __dp4a(int(nv[i].z), 0x01010101, nl);
+            nl = __dp4a(int(nv[i].w), 0x01010101, nl);
         }
-        ok = __all_sync(0xffffffffu, pending == 0u) && ok;
-#pragma unroll
-        for (int i = 0; i < 32; ++i) nl = __dp4a(int(uint32_t(w[i])), 0x01010101, nl);
     }
     return nl;
 }
@@ -1121,7 +1098,8 @@ __global__ void __launch_bounds__(kF4Threads, 1)
     uint8_t* stages = smem + 8 * TILE;                      // kF4Stages x 16 KB
     uint64_t* bars = reinterpret_cast<uint64_t*>(stages + kF4Stages * TILE);
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + kF4Bars);
-    __shared__ volatile long long s_pub[2];      // profiling: clock64 of this CTA's publication, by step parity
+    __shared__ volatile long long s_pub[2];      // profiling: clock64 of this CTA's flag publish, by step parity
+    __shared__ uint32_t s_flag[kF4Slices];       // the poller's mirror of the slice flags: gi * (S + 2) + flag
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int cs = int(blockIdx.x % kF4Slices);
@@ -1132,6 +1110,7 @@ __global__ void __launch_bounds__(kF4Threads, 1)
     const uint32_t bar_h = smem_u32(bars + 2 * kF4Stages), bar_j = smem_u32(bars + 2 * kF4Stages + 1);
     const uint32_t bar_fin = smem_u32(bars + 2 * kF4Stages + 2);    // MMA thread: drain before TMEM is freed
 
+    if (tid < kF4Slices) s_flag[tid] = 0u;
     if (tid == 0) {
         for (int s = 0; s < kF4Stages; ++s) {
             mbar_init(bar_full + 8 * s, kF4DW);
@@ -1177,7 +1156,8 @@ __global__ void __launch_bounds__(kF4Threads, 1)
     long long p_f0 = 0, p_f7 = 0, p_s0 = 0, p_s7 = 0;   // decision thread 0: marks after its own publish
     const long long t_loop0 = clock64();
 
-    for (int g = gs0; g < P.ngroups; g += gstride) {
+    for (int g = gs0, gi = 0; g < P.ngroups; g += gstride, ++gi) {
+        const uint32_t tbase = uint32_t(gi) * uint32_t(S + 2);   // this group's offset in the flag mirror
         if (warp < kF4DW) {
             // ---------------- decision warps ----------------
             const int chain = g * kM + r;
@@ -1210,9 +1190,8 @@ __global__ void __launch_bounds__(kF4Threads, 1)
                     }
                 if (e == 0) { sw[0] = swq; dw[0] = dwq; vmask[0] = vmq; }
                 else { sw[1] = swq; dw[1] = dwq; vmask[1] = vmq; }
-                uint64_t* lrow = P.ll + ((size_t(g) * 2 + 1) * kF4Slices + cs) * kM * kF4LLRow + size_t(r) * kF4LLRow + qq * 4;
-                ll_store2(lrow, db[0], db[1], 1u);         // the initial state carries the tag of step -1
-                ll_store2(lrow + 2, db[2], db[3], 1u);
+                uint8_t* drow = P.dbuf + ((size_t(g) * 2 + 1) * kM + r) * 1024 + cs * 64 + qq * 16;
+                *reinterpret_cast<uint4*>(drow) = make_uint4(db[0], db[1], db[2], db[3]);
                 uint32_t st[16];
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
@@ -1231,16 +1210,17 @@ __global__ void __launch_bounds__(kF4Threads, 1)
                 }
                 tmem_wait_st();
             }
-            // the fields are set before this warp marks any tile of this group full, so before the MMA thread
-            // accumulates (it waits for all eight decision warps)
+            // the fields are set before any tile of this group is marked full, so before the MMA thread accumulates
             tc_fence_before();
+            asm volatile("bar.sync 1, %0;" ::"r"(kF4DW * 32) : "memory");
+            if (tid == 0) flag_release(P.flags + g * kF4Slices + cs, 1u);
             uint32_t pk[32];
             // the run's error word is read once per step, off the critical path (its load overlaps the draws);
             // a wait of this warp that gives up clears ok at once
             const bool eok = !err_set(err);
             f4_draw(trng, pk);
             bool ok = __all_sync(0xffffffffu, eok);
-            int32_t nlin_next = f4_exchange(P, g, -1, smem_u32(stages), bar_full, bar_empty, q, tid, r, false, cs >> 1,
+            int32_t nlin_next = f4_exchange(P, g, -1, smem_u32(stages), bar_full, bar_empty, q, tid, r, false, s_flag, tbase, cs >> 1,
                                             ok, false, mk);
             q += kF4Tiles;
             const float hclf = float(P.hclamp);
@@ -1325,18 +1305,14 @@ __global__ void __launch_bounds__(kF4Threads, 1)
                     sw[e] ^= fm;
                     dw[e] = fm;
                 }
-                // publish: chunks 2hf, 2hf+1 of this slice's row r (8 tagged words) and the two partial counts
-                const uint32_t tag = uint32_t(m + 2);
-                uint64_t* lrow = P.ll + ((size_t(g) * 2 + par) * kF4Slices + cs) * kM * kF4LLRow + size_t(r) * kF4LLRow + hf * 8;
-                ll_store2(lrow, dq[0].x, dq[0].y, tag);
-                ll_store2(lrow + 2, dq[0].z, dq[0].w, tag);
-                ll_store2(lrow + 4, dq[1].x, dq[1].y, tag);
-                ll_store2(lrow + 6, dq[1].z, dq[1].w, tag);
-                uint64_t* nrow = P.nll + ((size_t(g) * 2 + par) * kM + r) * (2 * kF4Slices) + cs * 2 + hf;
-                asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(nrow), "l"(uint64_t(nlb) | (uint64_t(tag) << 32))
-                             : "memory");
+                uint8_t* drow = P.dbuf + ((size_t(g) * 2 + par) * kM + r) * 1024 + cs * 64 + hf * 32;
+                reinterpret_cast<uint4*>(drow)[0] = dq[0];
+                reinterpret_cast<uint4*>(drow)[1] = dq[1];
+                *reinterpret_cast<uint16_t*>(P.nlx + ((size_t(g) * 2 + par) * kM + r) * 128 + cs * 4 + hf * 2) = uint16_t(nlb);
                 tc_fence_before();
                 if (prof) { const long long t1 = clock64(); pb += t1 - t0; t0 = t1; }
+                asm volatile("bar.sync 1, %0;" ::"r"(kF4DW * 32) : "memory");
+                if (tid == 0) flag_release(P.flags + g * kF4Slices + cs, uint32_t(m + 2));
                 long long tpub = 0;
                 if (prof) {
                     tpub = clock64();
@@ -1349,7 +1325,7 @@ __global__ void __launch_bounds__(kF4Threads, 1)
                 if (m + 1 < S) f4_draw(trng, pk);
                 ok = ok && __all_sync(0xffffffffu, eok2);
                 if (prof) { const long long t1 = clock64(); pd += t1 - t0; t0 = t1; }
-                nlin_next = f4_exchange(P, g, m, smem_u32(stages), bar_full, bar_empty, q, tid, r, true, cs >> 1,
+                nlin_next = f4_exchange(P, g, m, smem_u32(stages), bar_full, bar_empty, q, tid, r, true, s_flag, tbase, cs >> 1,
                                         ok, prof, mk);
                 q += kF4Tiles;
                 if (prof) {
@@ -1435,6 +1411,41 @@ __global__ void __launch_bounds__(kF4Threads, 1)
                 q += uint32_t(S + 1) * kF4Tiles;
             }
             __syncwarp();
+        } else if (warp == kF4PollWarp) {
+            // ---------------- flag poller ----------------
+            // lane j < 16 watches slice j's flag (values 1 .. S + 1 for steps -1 .. S - 1) with relaxed gpu-scope
+            // loads; whatever the warp newly sees it acquires (fence) and releases to the CTA through s_flag, so
+            // the decision warps wait on shared memory, not L2
+            const uint32_t* fl = P.flags + g * kF4Slices;
+            uint32_t seen = 0u;
+            bool pok = !err_set(err);
+            for (uint32_t target = 1; pok && target <= uint32_t(S + 1); ++target) {
+                const uint64_t t0 = globaltimer();
+                for (uint32_t k = 1;; ++k) {
+                    uint32_t v = 0u;
+                    if (lane < kF4Slices)
+                        asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(fl + lane) : "memory");
+                    const bool fresh = lane < kF4Slices && v > seen;
+                    if (__any_sync(0xffffffffu, fresh)) {
+                        asm volatile("fence.acq_rel.gpu;" ::: "memory");
+                        if (fresh) {
+                            asm volatile("st.release.cta.shared::cta.u32 [%0], %1;" ::"r"(smem_u32(s_flag + lane)),
+                                         "r"(tbase + v)
+                                         : "memory");
+                            seen = v;
+                        }
+                    }
+                    if (__all_sync(0xffffffffu, lane >= kF4Slices || seen >= target)) break;
+                    if ((k & 63u) == 0) {
+                        const bool late = lane == 0 && globaltimer() - t0 > P.wait_ns;
+                        if (late) atomicCAS(err, 0, kErrFlag);
+                        if (__shfl_sync(0xffffffffu, (late || (lane == 0 && err_set(err))) ? 1 : 0, 0)) {
+                            pok = false;
+                            break;
+                        }
+                    }
+                }
+            }
         }
     }
     if (warp == kF4MmaWarp && lane == 0) {
@@ -1463,6 +1474,7 @@ __global__ void __launch_bounds__(kF4Threads, 1)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kF4TmemCols) : "memory");
     }
 }
+
 // ------------------------------------------------------------------------------------------------ host side
 // 2-D uint8 tensor [rows][cols] (cols contiguous), box = box_rows x 128 bytes, 128-byte swizzle.
 bool make_map(CUtensorMap* map, void* base, uint64_t cols, uint64_t rows, uint32_t box_rows) {
@@ -1709,10 +1721,10 @@ int f4_run(TensorInstance* ti, const TensorRun& r, cudaStream_t st, std::string*
         if (why) *why = "the fp4 tensor kernel cannot be co-resident on this device";
         return -2;
     }
-    // error word, then the tagged exchange words of every group (D: 512 KB, n_lin partials: 64 KB per group)
-    const size_t lbytes = size_t(ngroups) * 2 * kF4Slices * kM * kF4LLRow * 8;
-    const size_t nbytes = size_t(ngroups) * 2 * kM * 2 * kF4Slices * 8;
-    const size_t need = 256 + lbytes + nbytes;
+    const size_t fbytes = ((size_t(ngroups) * kF4Slices * 4 + 255) / 256) * 256;
+    const size_t dbytes = size_t(ngroups) * 2 * kM * 1024;
+    const size_t nbytes = size_t(ngroups) * 2 * kM * 128;
+    const size_t need = 256 + fbytes + dbytes + nbytes;
     cudaError_t e = cudaSuccess;
     if (ti->ws_bytes < need) {
         if (ti->d_ws) cudaFree(ti->d_ws);
@@ -1727,8 +1739,9 @@ int f4_run(TensorInstance* ti, const TensorRun& r, cudaStream_t st, std::string*
     }
     uint8_t* base = static_cast<uint8_t*>(ti->d_ws);
     int* err = reinterpret_cast<int*>(base);
-    uint64_t* ll = reinterpret_cast<uint64_t*>(base + 256);
-    uint64_t* nll = reinterpret_cast<uint64_t*>(base + 256 + lbytes);
+    uint32_t* flags = reinterpret_cast<uint32_t*>(base + 256);
+    uint8_t* dbuf = base + 256 + fbytes;
+    int8_t* nlx = reinterpret_cast<int8_t*>(dbuf + dbytes);
     CUtensorMap mapJ;
     if (!make_map(&mapJ, ti->d_J4, 1024, 2048, kF4YS)) {
         if (why) *why = "cuTensorMapEncodeTiled failed";
@@ -1738,7 +1751,7 @@ int f4_run(TensorInstance* ti, const TensorRun& r, cudaStream_t st, std::string*
     if (e == cudaSuccess) e = cudaMemsetAsync(r.out_sum_sh, 0, size_t(r.nchains) * 8, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(r.out_sum_bs, 0, size_t(r.nchains) * 8, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(r.out_flips, 0, size_t(r.nchains) * 8, st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(base, 0, need, st);     // error word + exchange words (tag 0)
+    if (e == cudaSuccess) e = cudaMemsetAsync(base, 0, 256 + fbytes, st);     // error word + flags
     if (e != cudaSuccess) {
         if (why) *why = std::string("memset: ") + cudaGetErrorString(e);
         return -2;
@@ -1756,8 +1769,9 @@ int f4_run(TensorInstance* ti, const TensorRun& r, cudaStream_t st, std::string*
     P.seed = r.seed;
     P.trial_offset = r.trial_offset;
     P.nchains = r.nchains;
-    P.ll = ll;
-    P.nll = nll;
+    P.flags = flags;
+    P.dbuf = dbuf;
+    P.nlx = nlx;
     P.out_spins = r.out_spins;
     P.out_sum_sh = reinterpret_cast<unsigned long long*>(r.out_sum_sh);
     P.out_sum_bs = reinterpret_cast<unsigned long long*>(r.out_sum_bs);

@@ -226,7 +226,8 @@ def initial_magnetisations(n: int, R: int, seed: int) -> torch.Tensor:
 def tune(inst: Instance, S: int = 200, R: int = 64, theta0=(30.0, math.log(6.0), 4.0, 0.0, 1.05), mode="counted",
          iters: int = 30, lr: float = 0.05, seed: int = 1, log=None):
     """Gradient ascent of the mean soft cut over theta = (T0, rate, q0, q_slope, gain) with Adam, the positive
-    parameters (T0, rate) in log space. Returns (theta, history of (iteration, soft cut, theta))."""
+    parameters (T0, rate) in log space. Returns (theta with the highest soft cut seen, history of (iteration, soft
+    cut, theta)); Adam's steps are not monotone, so the last iterate need not be the best."""
     mf = MeanField(inst)
     sch = SoftSchedule(S=S, mode=mode)
     m0 = mf.pad(initial_magnetisations(inst.n, R, seed))
@@ -247,8 +248,8 @@ def tune(inst: Instance, S: int = 200, R: int = 64, theta0=(30.0, math.log(6.0),
         hist.append((it, cut.item(), [float(x) for x in theta.detach().tolist()]))
         if log:
             log(hist[-1])
-    theta = torch.stack([raw[0].exp(), raw[1].exp(), raw[2], raw[3], raw[4]]).detach()
-    return theta, hist
+    best = max(hist, key=lambda h: h[1])
+    return torch.tensor(best[2], dtype=torch.float64, device="cuda"), hist
 
 
 def judge(inst: Instance, S: int, thetas: dict, nchains: int = 1024, seed: int = 20261004, trial_offset: int = 0,
