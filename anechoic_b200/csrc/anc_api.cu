@@ -7,6 +7,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -23,7 +24,9 @@ thread_local std::string g_err;
 thread_local double g_dev_ms = 0.0;
 thread_local std::vector<double> g_prof;
 thread_local int g_last_kernel = 0;
-std::atomic<uint64_t> g_wait_ns{2000000000ull};   // limit of each device wait of the engines' kernels (anc_set_wait_ns)
+std::atomic<uint64_t> g_wait_ns{2000000000ull};
+std::mutex g_batch_tune_mu;                      // guards g_batch_tune
+std::map<std::string, int> g_batch_tune;         // CSR pass variant per batch composition (anc_run_batch)   // limit of each device wait of the engines' kernels (anc_set_wait_ns)
 
 int fail(int code, const char* fmt, ...) {
     char buf[512];
@@ -997,24 +1000,6 @@ int anc_run_batch(int njobs, const anc_job* jobs, const anc_run_opts* o) {
             if (rc) return rc;
         }
     }
-    // the CSR pass variant of the batch's sparse launch: forced by the options, else the tuned variant of its costliest
-    // sparse job (tuned now, on that job, if it has not been)
-    int sparse_variant = (o && o->sparse_variant > 0) ? o->sparse_variant - 1 : -1;
-    if (sparse_variant < 0) {
-        int big = -1;
-        double cost = -1.0;
-        for (int k = 0; k < njobs; ++k)
-            if (jobs[k].inst->K == 0) {
-                const double c = double(jobs[k].inst->np) * jobs[k].tb->S * jobs[k].nchains;
-                if (c > cost) { cost = c; big = k; }
-            }
-        if (big >= 0) {
-            const anc_job& j = jobs[big];
-            const int rc = tune_sparse(j.inst, j.tb, j.seed, j.trial_offset, j.nchains, o);
-            if (rc) return rc;
-            sparse_variant = j.inst->sparse_variant;
-        }
-    }
     cudaStream_t st = nullptr;
     CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     std::unique_ptr<CUstream_st, void (*)(cudaStream_t)> st_guard(st, [](cudaStream_t s) { cudaStreamDestroy(s); });
@@ -1054,20 +1039,17 @@ int anc_run_batch(int njobs, const anc_job* jobs, const anc_run_opts* o) {
         cudaStreamSynchronize(st);
         return rc;
     };
-    if (cudaMemsetAsync(counters.p, 0, 4 * sizeof(int), st) != cudaSuccess) return drain(cuda_fail(cudaGetLastError(), "memset"));
-    if (cudaEventRecord(e0, st) != cudaSuccess) return drain(cuda_fail(cudaGetLastError(), "event"));
+    // work items per kind: a longest-processing-time-first queue, cost ~ np * S per anneal (dense np^2 * S)
+    int nitems[4] = {0, 0, 0, 0};
     for (int ki = 0; ki < 4; ++ki) {
         const int K = kKinds[ki];
-        std::vector<int> sel;
-        for (int k = 0; k < njobs; ++k)
-            if (jobs[k].inst->K == K) sel.push_back(k);
-        if (sel.empty()) continue;
-        // longest-processing-time-first queue: cost ~ np * S per anneal (dense np^2 * S)
         std::vector<std::pair<double, int2>> items;
-        for (int k : sel) {
+        for (int k = 0; k < njobs; ++k) {
+            if (jobs[k].inst->K != K) continue;
             const double cost = double(jobs[k].inst->np) * jobs[k].tb->S * (K == 0 ? 1.0 : double(jobs[k].inst->np));
             for (int c = 0; c < jobs[k].nchains; ++c) items.push_back({cost, make_int2(k, c)});
         }
+        if (items.empty()) continue;
         std::stable_sort(items.begin(), items.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
         std::vector<int2> it(items.size());
         for (size_t i = 0; i < items.size(); ++i) it[i] = items[i].second;
@@ -1075,19 +1057,68 @@ int anc_run_batch(int njobs, const anc_job* jobs, const anc_run_opts* o) {
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(d_items[ki].p, it.data(), it.size() * sizeof(int2), cudaMemcpyHostToDevice, st);
         if (e != cudaSuccess) return drain(cuda_fail(e, "work items"));
+        nitems[ki] = int(it.size());
+    }
+    auto launch_kind = [&](int ki, const anc::PlainJob* djobs, int variant) -> int {
         const KindPlan& kp = plans[ki];
         anc::PlainLaunch L{};
-        if (K == 0) L.sparse_variant = sparse_variant >= 0 ? sparse_variant : 0;
-        L.jobs = d_jobs.p;
+        L.sparse_variant = variant;
+        L.jobs = djobs;
         L.items = d_items[ki].p;
-        L.nitems = int(it.size());
+        L.nitems = nitems[ki];
         L.next_item = counters.p + ki;
         L.np_max = kp.np_max;
         L.nwj_max = kp.nwj_max;
         L.stream = kp.stream ? 1 : 0;
         const int grid = std::max(1, std::min(L.nitems, kp.per_sm * sms));
-        const int rc = anc::plain_launch(L, K, kp.P, grid, kp.smem, st);
-        if (rc) return drain(cuda_fail(cudaError_t(rc), "plain engine launch"));
+        cudaError_t e = cudaMemsetAsync(counters.p + ki, 0, sizeof(int), st);
+        if (e != cudaSuccess) return cuda_fail(e, "memset");
+        const int rc = anc::plain_launch(L, kKinds[ki], kp.P, grid, kp.smem, st);
+        return rc ? cuda_fail(cudaError_t(rc), "plain engine launch") : ANC_OK;
+    };
+    // the CSR pass variant of the sparse launch: forced by the options, else tuned on this batch as a whole (each
+    // variant runs the first min(S, 64) steps of every sparse job, twice, the second timed) and kept for batches of
+    // the same instances and anneal counts
+    int sparse_variant = (o && o->sparse_variant > 0) ? o->sparse_variant - 1 : -1;
+    if (nitems[0] > 0 && sparse_variant < 0) {
+        std::string key = std::to_string(dev);
+        for (int k = 0; k < njobs; ++k)
+            if (jobs[k].inst->K == 0)
+                key += ":" + std::to_string(jobs[k].inst->uid) + "x" + std::to_string(jobs[k].nchains) + "s" +
+                       std::to_string(std::min(jobs[k].tb->S, 64));
+        {
+            std::lock_guard<std::mutex> lock(g_batch_tune_mu);
+            auto it = g_batch_tune.find(key);
+            if (it != g_batch_tune.end()) sparse_variant = it->second;
+        }
+        if (sparse_variant < 0) {
+            std::vector<anc::PlainJob> probe = pj;
+            for (int k = 0; k < njobs; ++k) probe[k].tab.S = std::min(probe[k].tab.S, 64);
+            DevBuf<anc::PlainJob> d_probe;
+            CK(d_probe.ensure(njobs));
+            CK(cudaMemcpy(d_probe.p, probe.data(), sizeof(anc::PlainJob) * njobs, cudaMemcpyHostToDevice));
+            float best = 0.f;
+            for (int v = 0; v < anc::kSparseVariants; ++v) {
+                float ms = 0.f;
+                for (int rep = 0; rep < 2; ++rep) {
+                    CK(cudaEventRecord(e0, st));
+                    const int rc = launch_kind(0, d_probe.p, v);
+                    if (rc) return drain(rc);
+                    CK(cudaEventRecord(e1, st));
+                    CK(cudaEventSynchronize(e1));
+                    CK(cudaEventElapsedTime(&ms, e0, e1));
+                }
+                if (sparse_variant < 0 || ms < best) { best = ms; sparse_variant = v; }
+            }
+            std::lock_guard<std::mutex> lock(g_batch_tune_mu);
+            g_batch_tune[key] = sparse_variant;
+        }
+    }
+    if (cudaEventRecord(e0, st) != cudaSuccess) return drain(cuda_fail(cudaGetLastError(), "event"));
+    for (int ki = 0; ki < 4; ++ki) {
+        if (!nitems[ki]) continue;
+        const int rc = launch_kind(ki, d_jobs.p, ki == 0 ? std::max(0, sparse_variant) : 0);
+        if (rc) return drain(rc);
     }
     if (cudaEventRecord(e1, st) != cudaSuccess) return drain(cuda_fail(cudaGetLastError(), "event"));
     for (const Prepared& p : prep) {

@@ -286,3 +286,57 @@ def judge(inst: Instance, S: int, thetas: dict, nchains: int = 1024, seed: int =
                        "tts99_ms_secondary": analyze.tts99_secondary(p, nchains, times[name])}
         out[name] = rec
     return out
+
+
+def main(argv=None) -> int:
+    """Tune a schedule on the relaxation, then judge it against the starting schedule on the exact engine:
+
+        python -m anechoic_b200.meanfield (--graph F | --gset F | --jint8 F) [--bias F] [--steps 200] [--iters 40]
+                                          [--lr 0.05] [--mode counted|tecT|none] [--anneals 1024] [--seed S]
+                                          [--t0 30 --rate 1.792 --q0 4 --q-slope 0 --gain 1.05]
+
+    Prints one JSON line: the tuning history's first and best soft cut, the tuned theta (T0, rate, q0, q slope,
+    gain) and its integer tables' judgement (anc engine, p at the starting schedule's median cut). --iters 1 runs a
+    single forward and adjoint pass (as a profiler capture needs)."""
+    import argparse
+    import json
+    from .instances import load, read_bias
+    ap = argparse.ArgumentParser(prog="python -m anechoic_b200.meanfield")
+    for k in ("--graph", "--gset", "--jint8"):
+        ap.add_argument(k)
+    ap.add_argument("--bias")
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--iters", type=int, default=40)
+    ap.add_argument("--lr", type=float, default=0.01)
+    ap.add_argument("--mode", default="counted", choices=["counted", "tecT", "none"])
+    ap.add_argument("--anneals", type=int, default=1024)
+    ap.add_argument("--seed", type=int, default=20261004)
+    ap.add_argument("--t0", type=float, default=30.0)
+    ap.add_argument("--rate", type=float, default=math.log(6.0))
+    ap.add_argument("--q0", type=float, default=4.0)
+    ap.add_argument("--q-slope", type=float, default=0.0)
+    ap.add_argument("--gain", type=float, default=1.05)
+    ap.add_argument("--no-judge", action="store_true")
+    a = ap.parse_args(argv)
+    kind = next((k for k in ("graph", "gset", "jint8") if getattr(a, k)), None)
+    if kind is None:
+        ap.error("one of --graph, --gset, --jint8 is required")
+    inst = load(kind, getattr(a, kind))
+    if a.bias:
+        inst.bias = read_bias(a.bias, inst.n)
+    theta0 = (a.t0, a.rate, a.q0, a.q_slope, a.gain)
+    tuned, hist = tune(inst, S=a.steps, theta0=theta0, mode=a.mode, iters=a.iters, lr=a.lr)
+    best = max(hist, key=lambda h: h[1])
+    line = {"n": inst.n, "steps": a.steps, "iters": len(hist), "soft_cut_first": hist[0][1], "soft_cut_best": best[1],
+            "theta0": list(theta0), "theta_tuned": best[2]}
+    if not a.no_judge:
+        line["judgement"] = judge(inst, a.steps, {"start": torch.tensor(theta0, dtype=torch.float64),
+                                                  "tuned": tuned.cpu()}, nchains=a.anneals, seed=a.seed,
+                                  mode=a.mode)
+    print(json.dumps(line))
+    return 0
+
+
+if __name__ == "__main__":
+    import sys
+    sys.exit(main())

@@ -559,7 +559,7 @@ def run_extra(name: str, args, steps: int = 3, warmup: int = 1, target=None) -> 
         ach_b = 2 * fl_f / (tb_ / 1000.0) / 1e12
         theta0 = (30.0, math.log(6.0), 4.0, 0.0, 1.05)
         t_tune = time.perf_counter()
-        tuned, hist = M.tune(inst, S=S, R=R, theta0=theta0, iters=40, lr=0.05)
+        tuned, hist = M.tune(inst, S=S, R=R, theta0=theta0, iters=40, lr=0.01)
         t_tune = time.perf_counter() - t_tune
         thetas = {"default": torch.tensor(theta0, dtype=torch.float64), "tuned": tuned.cpu()}
         judged = M.judge(inst, S, thetas, nchains=CHAINS, seed=RUN_SEED, trial_offset=0xA0000000)
