@@ -590,6 +590,11 @@ __device__ __forceinline__ uint32_t cl_load(uint32_t addr) {
     return v;
 }
 __device__ __forceinline__ void cl_arrive() { asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory"); }
+// Arrival without release semantics: the lanes that wrote the send slot fence (cluster scope) before it, which is the
+// release; the other threads have nothing to publish.
+__device__ __forceinline__ void cl_arrive_relaxed() {
+    asm volatile("barrier.cluster.arrive.relaxed.aligned;" ::: "memory");
+}
 __device__ __forceinline__ void cl_wait() { asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory"); }
 __device__ __forceinline__ void cl_sync() {
     cl_arrive();
@@ -617,7 +622,7 @@ __global__ void __cluster_dims__(kCR, 1, 1) __launch_bounds__(kCT, 1)
     uint4* Jr = reinterpret_cast<uint4*>(smem_raw);                     // [256][16]
     uint32_t* send = reinterpret_cast<uint32_t*>(Jr + kCT * 16);         // [2 parities][8 warps][4]: F, U, n_lin
     uint4* recv = reinterpret_cast<uint4*>(send + 2 * 8 * 4);            // [2 parities][F, U][16]: 64 words each
-    __shared__ int32_t s_nl[2];
+    __shared__ int32_t s_nl[2], s_nf[2];
     __shared__ long long s_red[2][kCT / 32];
     __shared__ long long s_part[kCR][3];                    // rank 0: every rank's sum of s*h, of b*s and flips
 
@@ -646,14 +651,23 @@ __global__ void __cluster_dims__(kCR, 1, 1) __launch_bounds__(kCT, 1)
     long long flips = 0;
     // the initial pass publishes F = active slots and U = s0
     bool fl = valid, up_new = s_up, ln = false;
+    // this step's table entries, loaded one step ahead (off the decision's critical path)
+    int32_t fourT_n = __ldg(job.tab.fourT), q_n = __ldg(job.tab.q), kconst_n = __ldg(job.tab.kconst);
+    int64_t kcorr_n = __ldg(job.tab.kcorr);
     cl_sync();                                              // every CTA's shared memory is set up before any load
 
     for (int t = -1; t < S; ++t) {
         const int par = (t + 1) & 1;
         if (t >= 0) {
-            const int32_t fourT = __ldg(job.tab.fourT + t), twoT = fourT >> 1, qv = __ldg(job.tab.q + t);
-            const int32_t corr = step_corr(nlin_prev, __ldg(job.tab.kcorr + t), __ldg(job.tab.kconst + t));
+            const int32_t fourT = fourT_n, twoT = fourT >> 1, qv = q_n;
+            const int32_t corr = step_corr(nlin_prev, kcorr_n, kconst_n);
             const uint32_t lw = uint32_t(2 * twoT - 1);
+            if (t + 1 < S) {
+                fourT_n = __ldg(job.tab.fourT + t + 1);
+                q_n = __ldg(job.tab.q + t + 1);
+                kconst_n = __ldg(job.tab.kconst + t + 1);
+                kcorr_n = __ldg(job.tab.kcorr + t + 1);
+            }
             int32_t hs = s_up ? h : -h;
             if (hclamp > 0) hs = max(-hclamp, min(hs, hclamp));
             const int32_t zt = hs * 65536 + (qv + (df ? corr : -corr));
@@ -668,8 +682,9 @@ __global__ void __cluster_dims__(kCR, 1, 1) __launch_bounds__(kCT, 1)
             sd[0] = fw;
             sd[1] = uw;
             sd[2] = uint32_t(__popc(nlw));
+            asm volatile("fence.acq_rel.cluster;" ::: "memory");   // release of the slot, before the arrival
         }
-        cl_arrive();
+        cl_arrive_relaxed();
         if (t >= 0) {
             if (fl) s_up = up_new;
             df = fl;
@@ -681,6 +696,12 @@ __global__ void __cluster_dims__(kCR, 1, 1) __launch_bounds__(kCT, 1)
             const int wi = tid & 63, kk = wi >> 3, rr = wi & 7;
             const uint32_t v = cl_load(cl_map(sm_addr(send + (par * 8 + kk) * 4 + (tid >> 6)), uint32_t(rr)));
             reinterpret_cast<uint32_t*>(recv + (par * 2 + (tid >> 6)) * 16)[wi] = v;
+            if (tid < 64) {                                 // |F|: popcounts of the 64 flip words, two warp sums
+                int32_t c = __popc(v);
+#pragma unroll
+                for (int o = 16; o >= 1; o >>= 1) c += __shfl_xor_sync(FULL, c, o);
+                if (lane == 0) s_nf[tid >> 5] = c;
+            }
         } else if (tid < 192) {
             const int e = tid - 128;                        // (source CTA e / 8, warp e % 8)
             int32_t v = int32_t(cl_load(cl_map(sm_addr(send + (par * 8 + (e & 7)) * 4 + 2), uint32_t(e >> 3))));
@@ -697,13 +718,12 @@ __global__ void __cluster_dims__(kCR, 1, 1) __launch_bounds__(kCT, 1)
         const uint4* Fv = recv + par * 2 * 16;
         const uint4* Uv = Fv + 16;
         const uint4* Jv = Jr + tid * 16;
-        int32_t D = 0, nf = 0;
+        int32_t D = 0, nf = s_nf[0] + s_nf[1];
 #pragma unroll
         for (int ch = 0; ch < 16; ++ch) {
             const uint4 J4 = Jv[ch ^ (tid & 7)], F4 = Fv[ch], U4 = Uv[ch];
             D += __popc(F4.x & (U4.x ^ J4.x)) + __popc(F4.y & (U4.y ^ J4.y)) + __popc(F4.z & (U4.z ^ J4.z)) +
                  __popc(F4.w & (U4.w ^ J4.w));
-            nf += __popc(F4.x) + __popc(F4.y) + __popc(F4.z) + __popc(F4.w);
         }
         if (t >= 0 && tid == 0) flips += nf;
         // the diagonal: if y itself is in F, its term (J_yy = 0, stored as a 0 bit) was counted as -s'_y
