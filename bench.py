@@ -127,6 +127,13 @@ def profile_traffic(kernel: str):
     return e.get("bytes_per_launch") if e else None
 
 
+def stream_traffic(S: int):
+    """DRAM bytes per launch of the streaming kernel at S steps: the committed capture (S = 20) scaled by the field
+    updates, since J is read once per update (profiles/traffic.json)."""
+    b = profile_traffic("tensor_stream_kernel")
+    return None if b is None else b * (S + 1) / 21.0
+
+
 def finite(obj):
     """The JSON line holds no inf or nan (strict JSON): a non-finite number (e.g. TTS99 with no success) becomes null."""
     if isinstance(obj, float):
@@ -623,6 +630,7 @@ def run_extra(name: str, args, steps: int = 3, warmup: int = 1, target=None) -> 
                            "frac": a_ops / (2 * bf16_sus), "peak_kind": f"{peak_kind} bf16 sustained x 2",
                            "algorithmic_per_launch": ops, "kernel": "tensor_stream_kernel",
                            "hbm_j_stream": {"achieved": a_j, "peak": hbm, "unit": "GB/s", "frac": a_j / hbm},
+                           "traffic": stream_traffic(S),
                            "note": "int8 dense ops (tera-ops/s), every column of dS counted"}
     else:
         # algorithmic bytes: coupling rows of flipped spins (CSR entries of 4 B) + fields (8 B) and spin bits
@@ -631,6 +639,7 @@ def run_extra(name: str, args, steps: int = 3, warmup: int = 1, target=None) -> 
         alg = mean_flips * row_bytes + sum(i.n for i in insts) * per * S * 8.25
         ach = alg / (t / 1000.0) / 1e9
         out["roofline"] = {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                           "traffic": profile_traffic("plain_kernel_csr"),
                            "peak_kind": peak_kind, "algorithmic_per_launch": alg, "kernel": "plain_kernel",
                            "note": "CSR rows of flipped spins + fields + spin bits; rows are L2-resident, so the HBM "
                                    "copy peak is a lower bound of the roof"}
