@@ -1413,9 +1413,10 @@ __global__ void __launch_bounds__(kF4Threads, 1)
             __syncwarp();
         } else if (warp == kF4PollWarp) {
             // ---------------- flag poller ----------------
-            // lane j < 16 watches slice j's flag (values 1 .. S + 1 for steps -1 .. S - 1) with relaxed gpu-scope
-            // loads; whatever the warp newly sees it acquires (fence) and releases to the CTA through s_flag, so
-            // the decision warps wait on shared memory, not L2
+            // lane j < 16 watches slice j's flag (values 1 .. S + 1 for steps -1 .. S - 1) with acquire loads at gpu
+            // scope and releases what it newly sees to the CTA through s_flag, so the decision warps wait on shared
+            // memory, not L2 (relaxed loads with a fence per new observation measured 1.4 % slower: the fence delayed
+            // the next poll)
             const uint32_t* fl = P.flags + g * kF4Slices;
             uint32_t seen = 0u;
             bool pok = !err_set(err);
@@ -1424,10 +1425,9 @@ __global__ void __launch_bounds__(kF4Threads, 1)
                 for (uint32_t k = 1;; ++k) {
                     uint32_t v = 0u;
                     if (lane < kF4Slices)
-                        asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(fl + lane) : "memory");
+                        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(fl + lane) : "memory");
                     const bool fresh = lane < kF4Slices && v > seen;
                     if (__any_sync(0xffffffffu, fresh)) {
-                        asm volatile("fence.acq_rel.gpu;" ::: "memory");
                         if (fresh) {
                             asm volatile("st.release.cta.shared::cta.u32 [%0], %1;" ::"r"(smem_u32(s_flag + lane)),
                                          "r"(tbase + v)
