@@ -72,10 +72,12 @@ int pad_np(int n) { return std::max(2048, ((n + 255) / 256) * 256); }
 //                                               flip rewrites n fields from one row of bit planes (K planes);
 //                                               a_1 = 3.4, a_2 = 5.1, a_4 = 10.2, c_1 = 5.4e-6, c_2 = 1.6e-5,
 //                                               c_4 = 3.3e-5 (least squares in log time over the one-wave launches)
-//   cluster  2.2 + 2.1 phi n / 2048              (1-bit couplings, NP = 2048: the rows split over 8 CTAs)
-//   tensor   a constant per kernel: the MMA chain and the decisions cost the same whatever flips: fp4 8.6 (9.2 with
-//            more than one replica group per wave), int8 22.7 at NP = 2048, 21.6 and 27.5 at NP = 3072 and 4096,
-//            streaming 98.5 (measured 98.6 at NP = 10240 and 98 at NP = 16384: bound by its step latency, not by
+//   cluster  1.96                                (1-bit couplings, NP = 2048: every thread sums popcounts over all 64
+//                                               flip words whatever flipped, so the step costs the same at any phi;
+//                                               measured 1.93 ... 2.05)
+//   tensor   a constant per kernel: the MMA chain and the decisions cost the same whatever flips: fp4 8.1 (8.3 with
+//            more than one replica group per wave), int8 23.3 at NP = 2048, 21.7 and 28.3 at NP = 3072 and 4096,
+//            streaming 99.5 (measured 99.5 at NP = 10240 and 98 at NP = 16384: bound by its step latency, not by
 //            reading J)
 // Each engine advances a fixed number of anneals at once (per_wave); a launch of more takes further waves.
 constexpr double kPhiPrior = 0.25;   // flip fraction assumed before any run of these tables on this instance
@@ -88,9 +90,9 @@ double plain_step_us(int n, int K, double phi) {
 
 double tensor_step_us(int n, bool fp4, int groups_per_wave) {
     const int R = pad_np(n) / 256;
-    if (anc::stream_supported(n)) return 98.5;
-    if (R == 8) return fp4 ? (groups_per_wave > 1 ? 9.2 : 8.6) : 22.7;
-    return R == 12 ? 21.6 : 27.5;
+    if (anc::stream_supported(n)) return 99.5;
+    if (R == 8) return fp4 ? (groups_per_wave > 1 ? 8.3 : 8.1) : 23.3;
+    return R == 12 ? 21.7 : 28.3;
 }
 
 // us[ANC_ENGINE_*] for nchains anneals of S steps (-1: engine unavailable, per_wave[e] == 0); returns the engine with
@@ -106,7 +108,7 @@ int estimate_engines(int n, int K, int nchains, int S, double phi, bool fp4, con
         us[ANC_ENGINE_TENSOR] = waves(ANC_ENGINE_TENSOR) * S * tensor_step_us(n, fp4, (groups + 127) / 128);
     }
     if (per_wave[ANC_ENGINE_CLUSTER] > 0)
-        us[ANC_ENGINE_CLUSTER] = waves(ANC_ENGINE_CLUSTER) * S * (2.2 + 2.1 * phi * double(n) / 2048.0);
+        us[ANC_ENGINE_CLUSTER] = waves(ANC_ENGINE_CLUSTER) * S * 1.96;
     int best = ANC_ENGINE_PLAIN;
     for (int e : {ANC_ENGINE_PLAIN, ANC_ENGINE_TENSOR, ANC_ENGINE_CLUSTER})
         if (us[e] >= 0 && (us[best] < 0 || us[e] < us[best])) best = e;
