@@ -292,7 +292,7 @@ def main(argv=None) -> int:
     """Tune a schedule on the relaxation, then judge it against the starting schedule on the exact engine:
 
         python -m anechoic_b200.meanfield (--graph F | --gset F | --jint8 F) [--bias F] [--steps 200] [--iters 40]
-                                          [--lr 0.05] [--mode counted|tecT|none] [--anneals 1024] [--seed S]
+                                          [--lr 0.01] [--mode counted|tecT|none] [--anneals 1024] [--seed S]
                                           [--t0 30 --rate 1.792 --q0 4 --q-slope 0 --gain 1.05]
 
     Prints one JSON line: the tuning history's first and best soft cut, the tuned theta (T0, rate, q0, q slope,
