@@ -24,7 +24,7 @@ EXPORTS = ("anc_instance_create", "anc_instance_create_csr", "anc_instance_get_i
            "anc_run_batch", "anc_last_device_ms", "anc_last_kernel", "anc_last_error", "anc_last_profile", "anc_version",
            "anc_run_batch_noalloc", "anc_mf_create", "anc_mf_npad", "anc_mf_forward", "anc_mf_backward",
            "anc_mf_check", "anc_mf_set_wait_ns", "anc_mf_destroy", "anc_set_wait_ns", "anc_get_wait_ns",
-           "anc_sparse_tuning")
+           "anc_sparse_tuning", "anc_kernel_tuning")
 
 
 class AncError(RuntimeError):
@@ -44,7 +44,7 @@ class InstanceInfo(C.Structure):
 class RunOpts(C.Structure):
     _fields_ = [("engine", C.c_int), ("wide", C.c_int), ("threads", C.c_int), ("profile", C.c_int),
                 ("tensor_kind", C.c_int), ("flip_permille", C.c_int), ("sparse_variant", C.c_int),
-                ("reserved", C.c_int)]
+                ("kernel_variant", C.c_int)]
 
 
 class Job(C.Structure):
@@ -104,6 +104,7 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         L.anc_get_wait_ns.argtypes = []
         L.anc_get_wait_ns.restype = _u64
         L.anc_sparse_tuning.argtypes = [_vp, C.POINTER(_i), _vp]
+        L.anc_kernel_tuning.argtypes = [_vp, _i, _i, C.POINTER(_i), C.POINTER(_i), _vp]
         _lib = L
         return L
 

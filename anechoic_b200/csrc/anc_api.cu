@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <cmath>
 #include <cstdarg>
@@ -24,9 +25,17 @@ thread_local std::string g_err;
 thread_local double g_dev_ms = 0.0;
 thread_local std::vector<double> g_prof;
 thread_local int g_last_kernel = 0;
-std::atomic<uint64_t> g_wait_ns{2000000000ull};
+std::atomic<uint64_t> g_wait_ns{2000000000ull};   // limit of each device wait of the engines' kernels (anc_set_wait_ns)
 std::mutex g_batch_tune_mu;                      // guards g_batch_tune
-std::map<std::string, int> g_batch_tune;         // CSR pass variant per batch composition (anc_run_batch)   // limit of each device wait of the engines' kernels (anc_set_wait_ns)
+std::map<std::string, int> g_batch_tune;         // CSR pass variant per batch composition (anc_run_batch)
+// Run-time choice among the dense kernels' compiled variants (anc_kernel_tuning), per tuning key (device, kernel,
+// NP, K, replica groups): the chosen variant and each variant's probe time per step.
+struct KernelTune {
+    int variant = -1, nvariants = 0;
+    double probe_us[4] = {0.0, 0.0, 0.0, 0.0};
+};
+std::mutex g_kernel_tune_mu;                     // guards g_kernel_tune
+std::map<std::array<int, 5>, KernelTune> g_kernel_tune;
 
 int fail(int code, const char* fmt, ...) {
     char buf[512];
@@ -345,10 +354,13 @@ int plan_kind(int K, int np_max, int nwj_max, int sms, KindPlan* out) {
     return ANC_OK;
 }
 
+int tuned_variant(anc_instance* I, int kernel, int nchains);
+
+// One launch of the one-CTA plain engine; variant >= 0 forces the CSR pass variant (sparse instances) or the dense
+// pass variant (dense instances), else the tuned one.
 int launch_plain_single(anc_instance* I, const anc::PlainJob& job, cudaStream_t st, int variant = -1) {
     anc::PlainLaunch L{};
     L.job0 = job;
-    L.sparse_variant = variant >= 0 ? variant : std::max(0, I->sparse_variant);
     L.jobs = nullptr;
     L.items = nullptr;
     L.nitems = job.ntrials;
@@ -361,6 +373,15 @@ int launch_plain_single(anc_instance* I, const anc::PlainJob& job, cudaStream_t 
     int per_sm = 0;
     int rc = plain_residency(I, P, &smem, &stream, &per_sm);
     if (rc) return rc;
+    if (I->K == 0) {
+        L.sparse_variant = variant >= 0 ? variant : std::max(0, I->sparse_variant);
+    } else {
+        const int nv = anc::dense_variants(I->K, stream);
+        if (variant >= nv)
+            return fail(ANC_EINVAL, "kernel_variant %d out of range: the plain engine has %d dense variant(s) here",
+                        variant + 1, nv);
+        L.dense_variant = variant >= 0 ? variant : std::min(nv - 1, tuned_variant(I, ANC_KERNEL_PLAIN, job.ntrials));
+    }
     L.stream = stream ? 1 : 0;
     const int grid = std::max(1, std::min(job.ntrials, per_sm * I->sms));
     CK(cudaMemsetAsync(I->counter.p, 0, sizeof(int), st));
@@ -397,6 +418,25 @@ const int* engine_waves(anc_instance* I) {
     return I->per_wave;
 }
 
+// Tuning key of a run of nchains anneals of this instance on `kernel` (ANC_KERNEL_PLAIN for dense instances,
+// ANC_KERNEL_TENSOR_FP4): device, kernel, NP, K and, for the fp4 kernel, the replica groups one wave runs at once.
+std::array<int, 5> tune_key(anc_instance* I, int kernel, int nchains) {
+    int groups = 0;
+    if (kernel == ANC_KERNEL_TENSOR_FP4) {
+        const int slots = std::max(1, engine_waves(I)[ANC_ENGINE_TENSOR] / 128);
+        groups = std::max(1, std::min((nchains + 127) / 128, slots));
+    }
+    return {I->device, kernel, I->np, I->K, groups};
+}
+
+// The tuned variant for this key, 0 before any tuning.
+int tuned_variant(anc_instance* I, int kernel, int nchains) {
+    const auto key = tune_key(I, kernel, nchains);
+    std::lock_guard<std::mutex> lock(g_kernel_tune_mu);
+    const auto it = g_kernel_tune.find(key);
+    return it == g_kernel_tune.end() ? 0 : std::max(0, it->second.variant);
+}
+
 // Flip fraction AUTO assumes: the caller's hint, else what the last host-output run of these tables on this instance
 // saw, else the prior.
 double flip_fraction(const anc_instance* I, const anc_tables* tb, const anc_run_opts* o) {
@@ -427,9 +467,10 @@ int ensure_tensor(anc_instance* I) {
     return ANC_OK;
 }
 
-// Launch on device outputs; no synchronisation.
+// Launch on device outputs; no synchronisation. S_probe > 0 runs only the first S_probe steps of the schedule (the
+// run-time tuners' probes).
 int run_device_impl(anc_instance* I, anc_tables* tb, uint64_t seed, uint32_t off, int nchains, const anc_run_opts* o,
-                    const OutPtrs& out, cudaStream_t st) {
+                    const OutPtrs& out, cudaStream_t st, int S_probe = 0) {
     if (!I || !tb) return fail(ANC_EINVAL, "null handle");
     if (nchains < 1) return fail(ANC_EINVAL, "nchains must be >= 1");
     if (!out.spins || !out.sh || !out.fl) return fail(ANC_EINVAL, "spins, sum_sh and flips outputs are required");
@@ -442,8 +483,14 @@ int run_device_impl(anc_instance* I, anc_tables* tb, uint64_t seed, uint32_t off
             return fail(ANC_EINVAL, "tensor engine does not support n=%d K=%d", I->n, I->K);
         rc = ensure_tensor(I);
         if (rc) return rc;
+        const int forced = o ? o->kernel_variant : 0;
+        if (forced > anc::kF4Variants)
+            return fail(ANC_EINVAL, "kernel_variant %d out of range: the fp4 kernel has %d variants", forced,
+                        anc::kF4Variants);
         anc::TensorRun r{};
         r.tab = dev_tables(tb);
+        if (S_probe > 0) r.tab.S = std::min(r.tab.S, S_probe);
+        r.variant = forced > 0 ? forced - 1 : tuned_variant(I, ANC_KERNEL_TENSOR_FP4, nchains);
         r.seed = seed;
         r.trial_offset = off;
         r.nchains = nchains;
@@ -476,7 +523,8 @@ int run_device_impl(anc_instance* I, anc_tables* tb, uint64_t seed, uint32_t off
         g_last_kernel = I->tensor.last_kind == anc::TENSOR_KIND_FP4 ? ANC_KERNEL_TENSOR_FP4 : ANC_KERNEL_TENSOR_INT8;
         return ANC_OK;
     }
-    const anc::PlainJob job = make_job(I, tb, seed, off, nchains, hclamp, out);
+    anc::PlainJob job = make_job(I, tb, seed, off, nchains, hclamp, out);
+    if (S_probe > 0) job.tab.S = std::min(job.tab.S, S_probe);
     if (engine == ANC_ENGINE_CLUSTER) {
         if (!anc::plain_cluster_supported(I->K, I->np))
             return fail(ANC_EINVAL, "the cluster engine needs dense 1-bit couplings with n <= 2048 (n=%d K=%d)", I->n,
@@ -486,7 +534,7 @@ int run_device_impl(anc_instance* I, anc_tables* tb, uint64_t seed, uint32_t off
         g_last_kernel = ANC_KERNEL_PLAIN_CLUSTER;
         return ANC_OK;
     }
-    const int forced = o ? o->sparse_variant : 0;
+    const int forced = o ? (I->K == 0 ? o->sparse_variant : o->kernel_variant) : 0;
     rc = launch_plain_single(I, job, st, forced > 0 ? forced - 1 : -1);
     if (rc == ANC_OK) g_last_kernel = ANC_KERNEL_PLAIN;
     return rc;
@@ -537,6 +585,82 @@ int tune_sparse(anc_instance* I, anc_tables* tb, uint64_t seed, uint32_t off, in
     return ANC_OK;
 }
 
+// Run-time tuner of the dense kernels' compiled variants (anc_kernel_tuning): when a run would use the plain engine
+// on a dense instance or the fp4 kernel, and that run's tuning key (tune_key) has not been tuned in this process, each
+// variant runs the first min(S, 256) steps of the run's anneals (one wave of the plain engine; every replica group of
+// one fp4 wave) three times; its probe time is the least of the last two launches (CUDA events). Variant 0, the one
+// measured fastest on a B200 when the variants were compiled, is kept unless another probes more than 1 % faster:
+// the variants differ by a few percent, and a 64-step probe of one launch picked the wrong one in a third of the
+// recorded fp4 cases. The probes write into the handle's workspaces `out`, never into the caller's outputs; every
+// variant computes the same bits.
+int tune_kernel(anc_instance* I, anc_tables* tb, uint64_t seed, uint32_t off, int nchains, const anc_run_opts* o,
+                const OutPtrs& out) {
+    if (o && o->kernel_variant > 0) return ANC_OK;
+    const int engine = pick_engine(I, tb, nchains, o);
+    int kernel = 0, nv = 1, nprobe = nchains;
+    if (engine == ANC_ENGINE_PLAIN && I->K != 0) {
+        size_t smem = 0;
+        bool stream = false;
+        int per_sm = 0;
+        const int rc = plain_residency(I, plain_P(I->np), &smem, &stream, &per_sm);
+        if (rc) return rc;
+        kernel = ANC_KERNEL_PLAIN;
+        nv = anc::dense_variants(I->K, stream);
+        nprobe = std::min(nchains, per_sm * I->sms);
+    } else if (engine == ANC_ENGINE_TENSOR && fp4_candidate(I) && anc::tensor_supported(I->n, I->K, nchains) &&
+               !(o && o->tensor_kind == ANC_TENSOR_INT8)) {
+        kernel = ANC_KERNEL_TENSOR_FP4;
+        nv = anc::kF4Variants;
+        nprobe = std::min(nchains, std::max(128, engine_waves(I)[ANC_ENGINE_TENSOR]));
+    }
+    if (nv < 2) return ANC_OK;
+    const auto key = tune_key(I, kernel, nchains);
+    {
+        std::lock_guard<std::mutex> lock(g_kernel_tune_mu);
+        if (g_kernel_tune.count(key)) return ANC_OK;
+    }
+    anc_run_opts po{};
+    if (o) po = *o;
+    else po.wide = -1;     // the defaults of a call without options: clamp only where the range plan needs it
+    po.engine = engine;
+    po.profile = 0;
+    if (kernel == ANC_KERNEL_TENSOR_FP4) po.tensor_kind = ANC_TENSOR_FP4;
+    const int Sp = std::min(tb->S, 256);
+    OutPtrs pout = out;
+    pout.trace = nullptr;
+    pout.h = nullptr;
+    cudaStream_t st = I->stream;
+    KernelTune rec;
+    rec.nvariants = nv;
+    for (int v = 0; v < nv; ++v) {
+        po.kernel_variant = v + 1;
+        float ms = 0.f, best_ms = 0.f;
+        for (int rep = 0; rep < 3; ++rep) {
+            CK(cudaEventRecord(I->ev0, st));
+            int rc = run_device_impl(I, tb, seed, off, nprobe, &po, pout, st, Sp);
+            if (rc) return rc;
+            CK(cudaEventRecord(I->ev1, st));
+            CK(cudaEventSynchronize(I->ev1));
+            CK(cudaEventElapsedTime(&ms, I->ev0, I->ev1));
+            if (I->tensor_ready && I->tensor.last_err) {
+                std::string why;
+                rc = anc::tensor_check_error(&I->tensor, st, &why);
+                I->tensor.last_err = nullptr;
+                if (rc == -3) return fail(ANC_ETIMEOUT, "tensor engine (tuning probe): %s", why.c_str());
+                if (rc) return fail(ANC_ECUDA, "tensor engine (tuning probe): %s", why.c_str());
+            }
+            if (rep == 1 || (rep > 1 && ms < best_ms)) best_ms = ms;
+        }
+        rec.probe_us[v] = 1000.0 * double(best_ms) / Sp;
+    }
+    rec.variant = 0;
+    for (int v = 1; v < nv; ++v)
+        if (rec.probe_us[v] < 0.99 * rec.probe_us[0] && rec.probe_us[v] < rec.probe_us[rec.variant]) rec.variant = v;
+    std::lock_guard<std::mutex> lock(g_kernel_tune_mu);
+    g_kernel_tune.emplace(key, rec);
+    return ANC_OK;
+}
+
 int run_host_impl(anc_instance* I, anc_tables* tb, uint64_t seed, uint32_t off, int nchains, const anc_run_opts* o,
                   uint64_t* spins, int64_t* sum_sh, int64_t* sum_bs, int64_t* flips, int32_t* trace,
                   int32_t* fields) {
@@ -555,6 +679,10 @@ int run_host_impl(anc_instance* I, anc_tables* tb, uint64_t seed, uint32_t off, 
     cudaStream_t st = I->stream;
     if (I->K == 0 && !(o && o->sparse_variant > 0)) {
         const int trc = tune_sparse(I, tb, seed, off, nchains, o);
+        if (trc) return trc;
+    }
+    if (I->K != 0) {
+        const int trc = tune_kernel(I, tb, seed, off, nchains, o, out);
         if (trc) return trc;
     }
     CK(cudaEventRecord(I->ev0, st));
@@ -684,6 +812,38 @@ int anc_sparse_tuning(const anc_instance* I, int* variant, double* probe_us) {
     if (variant) *variant = I->K == 0 ? I->sparse_variant : -1;
     if (probe_us)
         for (int v = 0; v < anc::kSparseVariants; ++v) probe_us[v] = I->sparse_probe_us[v];
+    return ANC_OK;
+}
+int anc_kernel_tuning(const anc_instance* Ic, int kernel, int nchains, int* variant, int* nvariants,
+                      double* probe_us) {
+    if (!Ic) return fail(ANC_EINVAL, "null handle");
+    anc_instance* I = const_cast<anc_instance*>(Ic);    // the key may query (and cache) the engines' wave sizes
+    int nv = 1;
+    if (kernel == ANC_KERNEL_PLAIN) {
+        if (I->K == 0) return fail(ANC_EINVAL, "CSR instances are tuned by the CSR-pass tuner (anc_sparse_tuning)");
+        size_t smem = 0;
+        bool stream = false;
+        int per_sm = 0;
+        const int rc = plain_residency(I, plain_P(I->np), &smem, &stream, &per_sm);
+        if (rc) return rc;
+        nv = anc::dense_variants(I->K, stream);
+    } else if (kernel == ANC_KERNEL_TENSOR_FP4) {
+        nv = anc::kF4Variants;
+    } else {
+        return fail(ANC_EINVAL, "kernel %d has no compiled variants to tune", kernel);
+    }
+    if (nchains < 1) return fail(ANC_EINVAL, "nchains must be >= 1");
+    const auto key = tune_key(I, kernel, nchains);
+    KernelTune rec;
+    {
+        std::lock_guard<std::mutex> lock(g_kernel_tune_mu);
+        const auto it = g_kernel_tune.find(key);
+        if (it != g_kernel_tune.end()) rec = it->second;
+    }
+    if (variant) *variant = rec.variant;
+    if (nvariants) *nvariants = nv;
+    if (probe_us)
+        for (int v = 0; v < 4; ++v) probe_us[v] = rec.probe_us[v];
     return ANC_OK;
 }
 int anc_set_wait_ns(uint64_t ns) {

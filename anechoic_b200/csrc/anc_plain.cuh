@@ -59,12 +59,20 @@ struct PlainLaunch {
     int np_max, nwj_max;               // shared-memory layout
     int stream;                        // 1: dense counts go into the fields set by set (one result buffer)
     int sparse_variant;                // CSR pass variant (kSparseVariants index; 0 = rows 1 x edges 8 per lane)
+    int dense_variant;                 // dense pass variant (dense_variants(K) of them; 0 = the default)
 };
 
 // CSR pass variants the host's tuner chooses among: {lane groups' rows in flight, edges per lane fetched before any
 // is applied}. Every variant computes the same fields (integer atomics into shared memory), only the time differs.
 constexpr int kSparseVariants = 4;
 constexpr int kSparseVariantShape[kSparseVariants][2] = {{1, 8}, {1, 4}, {2, 4}, {1, 16}};
+
+// Compiled variants of the dense pass (rows of bit planes each thread counts per batch):
+//   K = 1: 0 = 8 rows with the next 8 fetched ahead, 1 = 8 rows, 2 = 16 rows;
+//   K = 2: 0 = 8 rows, 1 = 16 rows;
+//   K = 4 and the streaming layout: 8 rows only (16 rows of 6 counter sets exceed the 128 registers a thread has).
+constexpr int kDenseVariantsMax = 3;
+inline int dense_variants(int K, bool stream) { return stream ? 1 : K == 1 ? 3 : K == 2 ? 2 : 1; }
 
 // Shared-memory bytes for a launch (P = counter planes).
 inline size_t plain_smem_bytes(int np_max, int nwj_max, int K, int P, bool stream = false) {

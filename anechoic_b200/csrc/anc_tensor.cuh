@@ -48,7 +48,12 @@ struct TensorRun {
     long long* prof;          // device [grid][16] phase cycle totals, or null (profiling off)
     int kind;                 // TENSOR_KIND_*
     uint64_t wait_ns;         // limit of each device wait of the launch (0: give up at the first unsatisfied poll)
+    int variant;              // compiled variant of the fp4 kernel (kF4Variants; 0 = the 4-stage ring)
 };
+
+// Compiled variants of the fp4 kernel: the depth of its shared-memory ring of dS tiles (variant 0 .. 3: 4, 6, 5 or 3
+// stages of 16 KB; 4 measured fastest on a B200 at 1 and 8 replica groups, so it is the default before tuning).
+constexpr int kF4Variants = 4;
 
 // Launch geometry of a run: CTAs in the grid, CTAs per cluster, and how many clusters can be co-resident.
 struct TensorGeometry {

@@ -156,11 +156,15 @@ __device__ __forceinline__ void stream_apply(const uint32_t* res, int cc, int32_
 
 // Dense field pass: bit-sliced counts of the flipped rows, combined across groups into res[cc][w][P]; with STREAM
 // (K >= 2, nwj <= T) each set cc is instead combined into res[w][P] and added into h (factor mult) right away.
-template <int K, int P, bool STREAM>
+// DV is the compiled variant (dense_variants): whether the next 8 rows are fetched ahead (K = 1, DV = 0) and how many
+// rows a batch counts (8, or 16 for K = 1, DV = 2 and K = 2, DV = 1).
+template <int K, int P, bool STREAM, int DV = 0>
 __device__ __forceinline__ void dense_pass(const uint32_t* __restrict__ planes, size_t plane_stride, int nwj, int nf,
                                            const uint32_t* flist, uint32_t* comb, uint32_t* res, int32_t* h, int n,
                                            int mult) {
     constexpr int NC = K <= 1 ? 1 : 2 * (K - 1);
+    constexpr bool PREFETCH = K <= 1 && DV == 0;
+    constexpr int RB = (K <= 1 && DV == 2) || (K == 2 && DV == 1) ? 2 : 1;
     const int tid = threadIdx.x;
     if (nwj <= T) {
         const int G = T / nwj, g = tid / nwj, w = tid - g * nwj;
@@ -168,7 +172,7 @@ __device__ __forceinline__ void dense_pass(const uint32_t* __restrict__ planes, 
         BitCounter<P> cnt[NC];
 #pragma unroll
         for (int cc = 0; cc < NC; ++cc) cnt[cc].clear();
-        if (active && K <= 1) {
+        if (active && PREFETCH) {
             // one plane: the next 8 rows are fetched before the current 8 are counted, so the counting overlaps
             // the L2 latency of the fetches
             uint32_t cur[8], nxt[8];
@@ -200,7 +204,7 @@ __device__ __forceinline__ void dense_pass(const uint32_t* __restrict__ planes, 
                 cnt[0].add_w8_pair(w8a, w8b);
             }
         } else if (active) {
-            constexpr int RB = 1;
+            // RB batches of 8 rows fetched together, then counted
             for (int f0 = g; f0 < nf; f0 += 8 * RB * G) {
                 uint32_t a[RB][NC][8];
 #pragma unroll
@@ -400,7 +404,7 @@ __device__ __forceinline__ void apply_dense(const uint32_t* res, int nwj, const 
     }
 }
 
-template <int K, int P, bool SPARSE, bool STREAM, int SB = 1, int SE = 8>
+template <int K, int P, bool SPARSE, bool STREAM, int SB = 1, int SE = 8, int DV = 0>
 __global__ void __launch_bounds__(T, 1) plain_kernel(const __grid_constant__ PlainLaunch L) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
     __shared__ int s_item, s_nf, s_lin[8], s_wsum[T / 32];
@@ -460,7 +464,7 @@ __global__ void __launch_bounds__(T, 1) plain_kernel(const __grid_constant__ Pla
         if (SPARSE) {
             sparse_pass<SB, SE>(job.row_ptr, job.adj, flist, nf0, sparse_lg, h, 1);
         } else {
-            dense_pass<K, P, STREAM>(planes, plane_stride, nwj, nf0, flist, comb, res, h, n, 1);
+            dense_pass<K, P, STREAM, DV>(planes, plane_stride, nwj, nf0, flist, comb, res, h, n, 1);
             if (!STREAM) {
                 __syncthreads();
                 apply_dense<K, P>(res, nwj, Sw, Dw, h, n, nf0, true, 1);
@@ -510,7 +514,7 @@ __global__ void __launch_bounds__(T, 1) plain_kernel(const __grid_constant__ Pla
                 if (SPARSE) {
                     sparse_pass<SB, SE>(job.row_ptr, job.adj, flist, nf, sparse_lg, h, 2);
                 } else {
-                    dense_pass<K, P, STREAM>(planes, plane_stride, nwj, nf, flist, comb, res, h, n, 2);
+                    dense_pass<K, P, STREAM, DV>(planes, plane_stride, nwj, nf, flist, comb, res, h, n, 2);
                     if (!STREAM) {
                         __syncthreads();
                         apply_dense<K, P>(res, nwj, Sw, Dw, h, n, nf, false, 2);
@@ -768,9 +772,9 @@ __global__ void __cluster_dims__(kCR, 1, 1) __launch_bounds__(kCT, 1)
     }
 }
 
-template <int K, int P, bool SPARSE, bool STREAM = false, int SB = 1, int SE = 8>
+template <int K, int P, bool SPARSE, bool STREAM = false, int SB = 1, int SE = 8, int DV = 0>
 int launch_t(const PlainLaunch& L, int grid, size_t smem, cudaStream_t st) {
-    auto fn = plain_kernel<K, P, SPARSE, STREAM, SB, SE>;
+    auto fn = plain_kernel<K, P, SPARSE, STREAM, SB, SE, DV>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return int(e);
     fn<<<grid, T, smem, st>>>(L);
@@ -803,13 +807,28 @@ int plain_launch(const PlainLaunch& L, int K, int P, int grid, size_t smem, cuda
         if (P == 16 && K == 4) return launch_t<4, 16, false, true>(L, grid, smem, st);
         return int(cudaErrorInvalidValue);
     }
+    const int dv = L.dense_variant;
     if (P == 12) {
-        if (K == 1) return launch_t<1, 12, false>(L, grid, smem, st);
-        if (K == 2) return launch_t<2, 12, false>(L, grid, smem, st);
+        if (K == 1) {
+            if (dv == 1) return launch_t<1, 12, false, false, 1, 8, 1>(L, grid, smem, st);
+            if (dv == 2) return launch_t<1, 12, false, false, 1, 8, 2>(L, grid, smem, st);
+            return launch_t<1, 12, false>(L, grid, smem, st);
+        }
+        if (K == 2) {
+            if (dv == 1) return launch_t<2, 12, false, false, 1, 8, 1>(L, grid, smem, st);
+            return launch_t<2, 12, false>(L, grid, smem, st);
+        }
         if (K == 4) return launch_t<4, 12, false>(L, grid, smem, st);
     } else if (P == 16) {
-        if (K == 1) return launch_t<1, 16, false>(L, grid, smem, st);
-        if (K == 2) return launch_t<2, 16, false>(L, grid, smem, st);
+        if (K == 1) {
+            if (dv == 1) return launch_t<1, 16, false, false, 1, 8, 1>(L, grid, smem, st);
+            if (dv == 2) return launch_t<1, 16, false, false, 1, 8, 2>(L, grid, smem, st);
+            return launch_t<1, 16, false>(L, grid, smem, st);
+        }
+        if (K == 2) {
+            if (dv == 1) return launch_t<2, 16, false, false, 1, 8, 1>(L, grid, smem, st);
+            return launch_t<2, 16, false>(L, grid, smem, st);
+        }
         if (K == 4) return launch_t<4, 16, false>(L, grid, smem, st);
     }
     return int(cudaErrorInvalidValue);

@@ -840,7 +840,7 @@ __global__ void __launch_bounds__(kResThreads, 1)
 //     writer's stores before it, and release is cumulative over them).
 //   The same warps then fetch the step's D: tile t (128 replicas x 256 K, the slices of CTAs 2t and 2t+1) is
 //     loaded once both slice flags are seen, with 16-byte asynchronous L2 copies (four per thread, up to 6 tiles in flight),
-//     into a stage of a 6-deep shared-memory ring in the 128-byte-swizzled K-major layout the MMA reads; each
+//     into a stage of an NS-deep shared-memory ring (NS = 6, 5, 4 or 3: compiled variants the host's tuner picks from) in the 128-byte-swizzled K-major layout the MMA reads; each
 //     thread fences the async proxy and one lane per warp arrives on the stage's barrier. Each thread also sums
 //     its replica's 64 n_lin partial bytes for the next step's correction.
 //   The MMA thread: 4 mxf4 MMAs per tile into the fp32 fields in TMEM, a commit per stage to free it, and a commit
@@ -853,7 +853,6 @@ __global__ void __launch_bounds__(kResThreads, 1)
 constexpr int kF4Slices = 16;
 constexpr int kF4YS = 128;
 constexpr int kF4DW = 8;                  // decision warps (two quarters of 32 columns per thread)
-constexpr int kF4Stages = 6;
 constexpr int kF4Tiles = 8;               // D tiles per step (2048 fp4 = 1024 bytes per row, 128 bytes per tile)
 constexpr int kF4MmaWarp = kF4DW;
 constexpr int kF4PollWarp = kF4DW + 1;   // watches the group's 16 slice flags for the whole CTA
@@ -862,7 +861,8 @@ constexpr int kF4Cluster = 1;            // CTAs per cluster (1: the scheduler s
 constexpr int kF4SfCol = 160;             // TMEM columns 144..255 hold scale factors 0x7F (1.0)
 constexpr int kF4RngCol = 256;            // TMEM columns 256..319: RNG lane states, 32 per half hf
 constexpr int kF4TmemCols = 512;
-constexpr int kF4Bars = 2 * kF4Stages + 3;   // full[6], empty[6], fields ready, J loaded, drain
+// mbarriers of an NS-stage ring: full[NS], empty[NS], fields ready, J loaded, drain
+__host__ __device__ constexpr int f4_bars(int ns) { return 2 * ns + 3; }
 
 struct F4Params {
     int n, S, ngroups;
@@ -993,17 +993,18 @@ __device__ __forceinline__ void cp_async_wait(int n) {
 // one commit group per tile. Ring position t holds K chunk (t + rot) mod 8, so a CTA starts with the tile holding its
 // own slice. Tile t goes out as soon as its two slices are published, and tile t - 1 is marked full right after, so
 // the MMAs start on the first tile while later slices are still being published (marking tiles 0-3 full only after
-// tiles 0-5 had gone out cost 6 % of the step). Tile 6 and 7 wait for the MMAs of tiles 0 and 1 to free their
-// stages; those tiles were marked full before. A tile is marked full once its group has landed: the thread fences the
+// tiles 0-5 had gone out cost 6 % of the step). Tiles NS .. 7 wait for the MMAs of tiles 0 .. 7 - NS to free their
+// stages; those tiles were marked full before (tile t - NS <= t - 2 is marked full before tile t is issued). A tile is marked full once its group has landed: the thread fences the
 // async proxy and its warp arrives on the stage's barrier. Returns the replica's n_lin (the sum of its 64 partial
 // bytes) when want_nlin, else 0. ok (warp-uniform) is false once this warp saw an error; every wait is bounded, and
 // after an error the warp stops copying and arriving but still waits for the copies it has in flight.
+template <int NS>
 __device__ __forceinline__ int32_t f4_exchange(const F4Params& P, int g, int m, uint32_t stages_u32, uint32_t bar_full,
                                                uint32_t bar_empty, uint32_t q, int tid, int r, bool want_nlin,
                                                const uint32_t* s_flag, uint32_t tbase, int rot, bool& ok, bool prof,
                                                F4ExMarks& mk) {
     constexpr uint32_t TILE = kM * kKChunk;
-    static_assert(kF4Stages >= 2 && kF4Tiles == 8, "rotation by a 3-bit mask, and two stages in flight");
+    static_assert(NS >= 2 && NS <= kF4Tiles && kF4Tiles == 8, "rotation by a 3-bit mask, and two stages in flight");
     const int lane = tid & 31;
     int* err = P.err;
     const int par = m & 1;
@@ -1015,7 +1016,7 @@ __device__ __forceinline__ int32_t f4_exchange(const F4Params& P, int g, int m, 
     const uint32_t dst1 = uint32_t(row0 * 128 + ((ch ^ ((row0 + 4) & 7)) << 4));
     // copy tile t into its stage once its slices are published (and, for t >= 6, its stage is free)
     auto issue = [&](int t) {
-        const uint32_t qt = q + uint32_t(t), s = qt % kF4Stages, u = qt / kF4Stages;
+        const uint32_t qt = q + uint32_t(t), s = qt % NS, u = qt / NS;
         const int tk = (t + rot) & (kF4Tiles - 1);     // K chunk of ring position t (the CTA's own tile first)
         if (ok && u >= 1) ok = __all_sync(0xffffffffu, mbar_wait_for(bar_empty + 8 * s, (u - 1) & 1u, err, kErrEmpty, P.wait_ns));
         if (ok) {
@@ -1054,7 +1055,7 @@ __device__ __forceinline__ int32_t f4_exchange(const F4Params& P, int g, int m, 
         if (ok) {
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncwarp();
-            if (lane == 0) mbar_arrive(bar_full + 8 * ((q + uint32_t(t)) % kF4Stages));
+            if (lane == 0) mbar_arrive(bar_full + 8 * ((q + uint32_t(t)) % NS));
         }
         if (prof && lane == 0) {
             if (t == 0) mk.stored0 = clock64();
@@ -1086,6 +1087,7 @@ __device__ __forceinline__ int32_t f4_exchange(const F4Params& P, int g, int m, 
     return nl;
 }
 
+template <int NS>
 __global__ void __launch_bounds__(kF4Threads, 1)
     tensor_fp4_kernel(const __grid_constant__ CUtensorMap mapJ, const __grid_constant__ F4Params P) {
     constexpr int R = 8;                                    // rounds
@@ -1095,9 +1097,9 @@ __global__ void __launch_bounds__(kF4Threads, 1)
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t* jres = smem;                                   // 8 x 16 KB
-    uint8_t* stages = smem + 8 * TILE;                      // kF4Stages x 16 KB
-    uint64_t* bars = reinterpret_cast<uint64_t*>(stages + kF4Stages * TILE);
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + kF4Bars);
+    uint8_t* stages = smem + 8 * TILE;                      // NS x 16 KB
+    uint64_t* bars = reinterpret_cast<uint64_t*>(stages + NS * TILE);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + f4_bars(NS));
     __shared__ volatile long long s_pub[2];      // profiling: clock64 of this CTA's flag publish, by step parity
     __shared__ uint32_t s_flag[kF4Slices];       // the poller's mirror of the slice flags: gi * (S + 2) + flag
 
@@ -1106,13 +1108,13 @@ __global__ void __launch_bounds__(kF4Threads, 1)
     const int gs0 = int(blockIdx.x / kF4Slices), gstride = int(gridDim.x / kF4Slices);
     const int n = P.n, S = P.S;
     int* err = P.err;
-    const uint32_t bar_full = smem_u32(bars), bar_empty = smem_u32(bars + kF4Stages);
-    const uint32_t bar_h = smem_u32(bars + 2 * kF4Stages), bar_j = smem_u32(bars + 2 * kF4Stages + 1);
-    const uint32_t bar_fin = smem_u32(bars + 2 * kF4Stages + 2);    // MMA thread: drain before TMEM is freed
+    const uint32_t bar_full = smem_u32(bars), bar_empty = smem_u32(bars + NS);
+    const uint32_t bar_h = smem_u32(bars + 2 * NS), bar_j = smem_u32(bars + 2 * NS + 1);
+    const uint32_t bar_fin = smem_u32(bars + 2 * NS + 2);    // MMA thread: drain before TMEM is freed
 
     if (tid < kF4Slices) s_flag[tid] = 0u;
     if (tid == 0) {
-        for (int s = 0; s < kF4Stages; ++s) {
+        for (int s = 0; s < NS; ++s) {
             mbar_init(bar_full + 8 * s, kF4DW);
             mbar_init(bar_empty + 8 * s, 1);
         }
@@ -1220,7 +1222,7 @@ __global__ void __launch_bounds__(kF4Threads, 1)
             const bool eok = !err_set(err);
             f4_draw(trng, pk);
             bool ok = __all_sync(0xffffffffu, eok);
-            int32_t nlin_next = f4_exchange(P, g, -1, smem_u32(stages), bar_full, bar_empty, q, tid, r, false, s_flag, tbase, cs >> 1,
+            int32_t nlin_next = f4_exchange<NS>(P, g, -1, smem_u32(stages), bar_full, bar_empty, q, tid, r, false, s_flag, tbase, cs >> 1,
                                             ok, false, mk);
             q += kF4Tiles;
             const float hclf = float(P.hclamp);
@@ -1325,7 +1327,7 @@ __global__ void __launch_bounds__(kF4Threads, 1)
                 if (m + 1 < S) f4_draw(trng, pk);
                 ok = ok && __all_sync(0xffffffffu, eok2);
                 if (prof) { const long long t1 = clock64(); pd += t1 - t0; t0 = t1; }
-                nlin_next = f4_exchange(P, g, m, smem_u32(stages), bar_full, bar_empty, q, tid, r, true, s_flag, tbase, cs >> 1,
+                nlin_next = f4_exchange<NS>(P, g, m, smem_u32(stages), bar_full, bar_empty, q, tid, r, true, s_flag, tbase, cs >> 1,
                                         ok, prof, mk);
                 q += kF4Tiles;
                 if (prof) {
@@ -1350,8 +1352,8 @@ __global__ void __launch_bounds__(kF4Threads, 1)
                     const long long t0 = prof ? clock64() : 0;
                     mok = mok && !err_set(err);    // once per step, while the thread waits for the first tile
                     for (int t = 0; t < kF4Tiles; ++t, ++q) {
-                        const int s = int(q % kF4Stages);
-                        const uint32_t u = q / kF4Stages;
+                        const int s = int(q % NS);
+                        const uint32_t u = q / NS;
                         const long long w0 = prof ? clock64() : 0;
                         mok = mok && mbar_wait_for(bar_full + 8 * s, u & 1u, err, kErrFull, P.wait_ns);
                         const bool ok = mok;
@@ -1679,14 +1681,28 @@ int ensure_bias_perm(TensorInstance* ti, const int32_t* bias, std::string* why) 
     return 0;
 }
 
-size_t f4_smem_bytes() {
-    return 1024 + 8 * size_t(kM) * kKChunk + size_t(kF4Stages) * kM * kKChunk + kF4Bars * 8 + 16;
+size_t f4_smem_bytes(int ns) {
+    return 1024 + 8 * size_t(kM) * kKChunk + size_t(ns) * kM * kKChunk + size_t(f4_bars(ns)) * 8 + 16;
 }
 
-// Concurrent group slots of the fp4 kernel (16 co-resident CTAs each).
+// The fp4 kernel's compiled ring depths; TensorRun::variant v runs kF4StageVariants[v].
+constexpr int kF4StageVariants[kF4Variants] = {4, 6, 5, 3};
+
+using F4Kernel = void (*)(const CUtensorMap, const F4Params);
+F4Kernel f4_kernel(int variant) {
+    switch (variant) {
+        case 1: return tensor_fp4_kernel<6>;
+        case 2: return tensor_fp4_kernel<5>;
+        case 3: return tensor_fp4_kernel<3>;
+        default: return tensor_fp4_kernel<4>;
+    }
+}
+
+// Concurrent group slots of the fp4 kernel (16 co-resident CTAs each; queried with the deepest ring, one CTA per SM
+// in every variant).
 int f4_group_slots(int ngroups, int* out) {
-    auto fn = tensor_fp4_kernel;
-    const size_t smem = f4_smem_bytes();
+    auto fn = f4_kernel(1);
+    const size_t smem = f4_smem_bytes(kF4StageVariants[1]);
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     int per_sm = 0, dev = 0, sms = 0;
     if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kF4Threads, smem);
@@ -1781,8 +1797,9 @@ int f4_run(TensorInstance* ti, const TensorRun& r, cudaStream_t st, std::string*
     P.err = err;
     P.prof = r.prof;
     P.wait_ns = r.wait_ns;
-    auto fn = tensor_fp4_kernel;
-    const size_t smem = f4_smem_bytes();
+    const int variant = (r.variant >= 0 && r.variant < kF4Variants) ? r.variant : 0;
+    auto fn = f4_kernel(variant);
+    const size_t smem = f4_smem_bytes(kF4StageVariants[variant]);
     e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute at[2];

@@ -117,7 +117,9 @@ typedef struct {
                           anc_run_fields of these tables on this instance saw, else 0.25 */
     int sparse_variant; /* CSR instances on the plain engine: 0 = the variant the run-time tuner chose for the instance
                            (anc_sparse_tuning), v + 1 = force variant v (0 .. 3) */
-    int reserved;
+    int kernel_variant; /* dense instances on the plain engine and the tensor engine's fp4 kernel: 0 = the variant the
+                           run-time tuner chose (anc_kernel_tuning; the default variant before any tuning), v + 1 =
+                           force variant v */
 } anc_run_opts;
 
 /* No counterpart in the reference (its kernel geometry is fixed per build by flags, sca_gpu_bias.cu:637-644). The
@@ -128,6 +130,22 @@ typedef struct {
  * instance. Writes the chosen variant (-1 = not tuned yet, or not a CSR instance) and probe_us[4], each variant's
  * probe time per step in microseconds (may be NULL). */
 ANC_API int anc_sparse_tuning(const anc_instance* inst, int* variant, double* probe_us);
+
+/* No counterpart in the reference (its tile shapes and depths are fixed per build by flags, sca_gpu_bias.cu:637-644).
+ * The run-time tuner of the dense kernels' compiled variants:
+ *   ANC_KERNEL_PLAIN (dense instances): rows of bit planes a thread counts per batch -- K = 1: 0 = 8 rows with the
+ *     next 8 fetched ahead, 1 = 8 rows, 2 = 16 rows; K = 2: 0 = 8 rows, 1 = 16 rows; K = 4 and NP > 8192: one variant;
+ *   ANC_KERNEL_TENSOR_FP4: the depth of the shared-memory ring of dS tiles -- 0 = 4 stages, 1 = 6, 2 = 5, 3 = 3.
+ * The first synchronous run (anc_run / anc_run_fields) that uses one of these kernels for a (device, kernel, NP, K,
+ * replica groups) key not yet tuned runs each variant on the first min(S, 256) steps of that run's anneals (one wave
+ * of the plain engine, every replica group of the fp4 kernel) into the handle's own workspaces -- three times, the
+ * least of the last two launches timed -- and keeps variant 0 unless another probes more than 1 % faster, in which
+ * case the fastest, for every later launch with that key in the process (device and
+ * graph-captured launches included; anc_run_batch and anc_run_batch_noalloc use variant 0). For the key a run of
+ * nchains anneals of this instance on `kernel` would use, writes the chosen variant (-1 = not tuned yet), the number
+ * of compiled variants and probe_us[4], each variant's probe time per step in microseconds (may be NULL). */
+ANC_API int anc_kernel_tuning(const anc_instance* inst, int kernel, int nchains, int* variant, int* nvariants,
+                              double* probe_us);
 
 /* No counterpart in the reference (its CLI has one engine). The cost model behind ANC_ENGINE_AUTO, host-only: the
  * estimated device time in microseconds of nchains anneals of S steps on each engine, for n spins with kbits-bit dense
