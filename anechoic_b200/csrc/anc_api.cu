@@ -147,6 +147,8 @@ struct anc_instance {
     DevBuf<long long> w_sh, w_bs, w_fl;
     DevBuf<int32_t> w_trace, w_h;
     DevBuf<long long> w_prof;                     // tensor-engine phase counters (opt-in)
+    DevBuf<int> w_err;                            // cluster engine's error word
+    bool cluster_err_pending = false;             // a cluster launch's error word is still to be read
     int prof_ctas = 0, prof_S = 0;
     // CSR pass variant chosen by the tuner (-1: not tuned yet) and its probe's device time per step of each variant
     int sparse_variant = -1;
@@ -529,6 +531,13 @@ int run_device_impl(anc_instance* I, anc_tables* tb, uint64_t seed, uint32_t off
         if (!anc::plain_cluster_supported(I->K, I->np))
             return fail(ANC_EINVAL, "the cluster engine needs dense 1-bit couplings with n <= 2048 (n=%d K=%d)", I->n,
                         I->K);
+        CK(I->w_err.ensure(1));
+        CK(cudaMemsetAsync(I->w_err.p, 0, sizeof(int), st));
+        job.err = I->w_err.p;
+        // the limit, but never below 10 ms: an exchange that gave up can leave pushes in flight toward a CTA, so a
+        // forced expiry (a limit of 0) is kept off this engine (a step takes about 2 us)
+        job.wait_ns = std::max<uint64_t>(10000000ull, g_wait_ns.load());
+        I->cluster_err_pending = true;
         rc = anc::plain_cluster_launch(job, st);
         if (rc) return cuda_fail(cudaError_t(rc), "cluster engine launch");
         g_last_kernel = ANC_KERNEL_PLAIN_CLUSTER;
@@ -696,6 +705,13 @@ int run_host_impl(anc_instance* I, anc_tables* tb, uint64_t seed, uint32_t off, 
     if (trace) CK(cudaMemcpyAsync(trace, I->w_trace.p, size_t(nchains) * tb->S * 4, cudaMemcpyDeviceToHost, st));
     if (fields) CK(cudaMemcpyAsync(fields, I->w_h.p, size_t(nchains) * I->n * 4, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    if (I->cluster_err_pending) {
+        int e = 0;
+        CK(cudaMemcpy(&e, I->w_err.p, sizeof(int), cudaMemcpyDeviceToHost));
+        I->cluster_err_pending = false;
+        if (e) return fail(ANC_ETIMEOUT, "cluster engine: a step's exchange did not arrive within the wait limit (%llu ns)",
+                           static_cast<unsigned long long>(g_wait_ns.load()));
+    }
     if (I->tensor_ready && I->tensor.last_err) {
         std::string why;
         rc = anc::tensor_check_error(&I->tensor, st, &why);

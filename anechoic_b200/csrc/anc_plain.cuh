@@ -48,7 +48,13 @@ struct PlainJob {
     int64_t* out_flips;                // [ntrials]
     int32_t* out_trace;                // [ntrials][S] or null
     int32_t* out_h;                    // [ntrials][n] or null (final fields)
+    // cluster engine only: error word (a bounded wait that gave up sets it; may be null) and the limit of each wait
+    int* err;
+    uint64_t wait_ns;
 };
+
+// Error codes of the cluster engine's error word.
+constexpr int kClusterErrRecv = 1;     // a step's exchange words did not all arrive within the wait limit
 
 struct PlainLaunch {
     PlainJob job0;                     // the job when items == nullptr (item index = trial index)

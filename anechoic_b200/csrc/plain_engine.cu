@@ -553,23 +553,27 @@ __global__ void __launch_bounds__(T, 1) plain_kernel(const __grid_constant__ Pla
 // its slot's field, spin and last-flip bit in registers and a copy of lane 32r + l's xoshiro128** state, which it
 // advances 8 draws per step and uses the k-th (every lane's stream is consumed in round order, as the golden model
 // does). The J rows of the owned slots (by symmetry their columns, 256 x 2048 bits = 64 KB) stay in shared memory.
-// Per step:
-//   1. every thread decides its slot; warp k's ballots give flip word k*8 + r (bit l = slot k*256 + 32r + l), the
-//      matching word of new spins +1 among the flipped, and its popcount of the linear band (n_lin partial); lane 0
-//      stores the three into this CTA's send slot for the step's parity and the CTA arrives on the cluster barrier
-//      (release); the next step's draws are made before the wait (acquire);
-//   2. 128 threads load the 64 flip words and 64 new-spin words from the 8 CTAs' send slots (ld.shared::cluster), 64
-//      threads load and reduce the n_lin partials, and a CTA barrier makes them visible;
-//   3. every thread updates its field from all 2048 slots at once: for its row y of J (bit = [J_xy = +1]),
+// Per step m (m = 0: the initial pass; m = t + 1 for step t), with p = m & 1:
+//   1. every thread decides its slot; warp k's ballots give flip word wi = k*8 + r (bit l = slot k*256 + 32r + l),
+//      the matching word of new spins +1 among the flipped, and the warp's counts of band slots and flips;
+//   2. lanes 0 .. 7 of warp k push the warp's word pair and its packed counts to CTA `lane` with st.async (12 bytes
+//      into that CTA's exchange buffer p, completing on its mbarrier p): every CTA receives 64 x 12 = 768 bytes per
+//      step, and its thread 0 arrives on its own mbarrier p expecting them;
+//   3. every thread makes its next draws, then waits (bounded) for mbarrier p's phase (cluster-scope acquire: the
+//      remote stores are visible after it); each warp sums the 64 packed counts itself (n_lin for the next
+//      correction, |F|), so no CTA barrier is needed;
+//   4. every thread updates its field from all 2048 slots at once: for its row y of J (bit = [J_xy = +1]),
 //        D = sum_w popc(F_w & (U_w ^ J_yw)),   h_y += 2 (|F| - 2 D)   (2 s'_x J_xy summed over the flipped x),
 //      less the diagonal term when y itself flipped (J_yy = 0 is stored as a 0 bit). The initial pass uses the same
 //      formula with F = the active slots, U = s0 and factor 1 (h = b + J s0).
-// No step reads J from L2, no flip list is built and no counter is extracted: the update costs the same whatever
-// the flip count. A send slot is rewritten two steps later, after every CTA has passed the cluster barrier of the step
-// in between, which it arrives at only after its reads of the slot; so one cluster barrier per step suffices. Every
-// thread of every CTA reaches the cluster and CTA barriers the same number of times (no other wait exists).
+// No step reads J from L2, no flip list is built, no counter is extracted and no barrier is crossed: the update costs
+// the same whatever the flip count. Buffer p is written again at step m + 2 only by a CTA that has received every
+// CTA's words of step m + 1, and a CTA sends those only after each of its warps has finished reading buffer p of step
+// m (the words sent depend on the fields those reads updated); so the pushes of step m + 2 cannot overtake the reads
+// of step m, nor count toward mbarrier p's phase of step m.
 constexpr int kCT = 256;                  // threads per CTA (one slot each)
 constexpr int kCR = 8;                    // CTAs per anneal
+constexpr uint32_t kClusterTx = 64 * 12;  // exchange bytes a CTA receives per step
 constexpr size_t kClusterSmem = 116 * 1024;   // above half an SM's shared memory: one CTA per SM
 
 __device__ __forceinline__ uint32_t sm_addr(const void* p) { return uint32_t(__cvta_generic_to_shared(p)); }
@@ -588,21 +592,44 @@ __device__ __forceinline__ uint32_t cl_map(uint32_t local, uint32_t rank) {
     asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(a) : "r"(local), "r"(rank));
     return a;
 }
-__device__ __forceinline__ uint32_t cl_load(uint32_t addr) {
-    uint32_t v;
-    asm volatile("ld.shared::cluster.u32 %0, [%1];" : "=r"(v) : "r"(addr) : "memory");
-    return v;
-}
-__device__ __forceinline__ void cl_arrive() { asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory"); }
-// Arrival without release semantics: the lanes that wrote the send slot fence (cluster scope) before it, which is the
-// release; the other threads have nothing to publish.
-__device__ __forceinline__ void cl_arrive_relaxed() {
-    asm volatile("barrier.cluster.arrive.relaxed.aligned;" ::: "memory");
-}
-__device__ __forceinline__ void cl_wait() { asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory"); }
 __device__ __forceinline__ void cl_sync() {
-    cl_arrive();
-    cl_wait();
+    asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+    asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ uint64_t cl_globaltimer() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// remote store of two words / one word into another CTA's shared memory, completing on its mbarrier
+__device__ __forceinline__ void st_async2(uint32_t addr, uint32_t a, uint32_t b, uint32_t bar) {
+    asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v2.b32 [%0], {%1, %2}, [%3];"
+                 ::"r"(addr), "r"(a), "r"(b), "r"(bar) : "memory");
+}
+__device__ __forceinline__ void st_async1(uint32_t addr, uint32_t a, uint32_t bar) {
+    asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.b32 [%0], %1, [%2];"
+                 ::"r"(addr), "r"(a), "r"(bar) : "memory");
+}
+__device__ __forceinline__ bool cl_try_wait(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait for phase `parity`; false after limit_ns (0: at the first unsatisfied poll). The timer is read every
+// 256 polls.
+__device__ __forceinline__ bool cl_wait_for(uint32_t bar, uint32_t parity, uint64_t limit_ns) {
+    if (cl_try_wait(bar, parity)) return true;
+    if (limit_ns == 0) return false;
+    const uint64_t t0 = cl_globaltimer();
+    for (uint32_t k = 1;; ++k) {
+        if (cl_try_wait(bar, parity)) return true;
+        if ((k & 255u) == 0 && cl_globaltimer() - t0 > limit_ns) return false;
+    }
 }
 
 // The draw of round k from this lane's stream: 8 draws per step, the k-th kept.
@@ -624,9 +651,9 @@ __global__ void __cluster_dims__(kCR, 1, 1) __launch_bounds__(kCT, 1)
     extern __shared__ __align__(16) uint8_t smem_raw[];
     // J row of owned slot t: 16 chunks of 16 bytes, chunk c at position c ^ (t & 7) (conflict-free 16-byte loads)
     uint4* Jr = reinterpret_cast<uint4*>(smem_raw);                     // [256][16]
-    uint32_t* send = reinterpret_cast<uint32_t*>(Jr + kCT * 16);         // [2 parities][8 warps][4]: F, U, n_lin
-    uint4* recv = reinterpret_cast<uint4*>(send + 2 * 8 * 4);            // [2 parities][F, U][16]: 64 words each
-    __shared__ int32_t s_nl[2], s_nf[2];
+    uint2* FU = reinterpret_cast<uint2*>(Jr + kCT * 16);                // [2 parities][64 words]: flip, new spin +1
+    uint32_t* NLc = reinterpret_cast<uint32_t*>(FU + 2 * 64);            // [2][64]: band count | flip count << 16
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(NLc + 2 * 64);          // [2]: exchange of each parity
     __shared__ long long s_red[2][kCT / 32];
     __shared__ long long s_part[kCR][3];                    // rank 0: every rank's sum of s*h, of b*s and flips
 
@@ -639,10 +666,20 @@ __global__ void __cluster_dims__(kCR, 1, 1) __launch_bounds__(kCT, 1)
     const int slot = k * kLanes + 32 * int(rank) + lane;
     const bool valid = slot < n;
 
+    if (tid == 0) {
+        for (int q = 0; q < 2; ++q)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(sm_addr(mbar + q)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
     {
         const uint4* row = reinterpret_cast<const uint4*>(job.planes + size_t(slot) * NWJ);
         for (int ch = 0; ch < 16; ++ch) Jr[tid * 16 + (ch ^ (tid & 7))] = __ldg(row + ch);
     }
+    // remote addresses this thread pushes to (lanes 0 .. 7: CTA `lane`), word wi = k*8 + rank of each buffer
+    const uint32_t dst_rank = uint32_t(lane & 7);
+    const uint32_t dst_fu = cl_map(sm_addr(FU + k * 8 + int(rank)), dst_rank);
+    const uint32_t dst_nl = cl_map(sm_addr(NLc + k * 8 + int(rank)), dst_rank);
+    const uint32_t dst_mb = cl_map(sm_addr(mbar), dst_rank);
 
     Xoshiro rng;
     rng_seed(rng, job.seed, job.trial_offset + uint32_t(c), 32u * rank + uint32_t(lane));
@@ -653,15 +690,16 @@ __global__ void __cluster_dims__(kCR, 1, 1) __launch_bounds__(kCT, 1)
     uint32_t u = lane_draw(rng, k);                         // step 0's draw
     int32_t nlin_prev = 0;
     long long flips = 0;
+    bool ok = true;                                         // false once a wait gave up
     // the initial pass publishes F = active slots and U = s0
     bool fl = valid, up_new = s_up, ln = false;
     // this step's table entries, loaded one step ahead (off the decision's critical path)
     int32_t fourT_n = __ldg(job.tab.fourT), q_n = __ldg(job.tab.q), kconst_n = __ldg(job.tab.kconst);
     int64_t kcorr_n = __ldg(job.tab.kcorr);
-    cl_sync();                                              // every CTA's shared memory is set up before any load
+    cl_sync();                                              // barriers initialised and J loaded in every CTA
 
     for (int t = -1; t < S; ++t) {
-        const int par = (t + 1) & 1;
+        const int m = t + 1, par = m & 1;
         if (t >= 0) {
             const int32_t fourT = fourT_n, twoT = fourT >> 1, qv = q_n;
             const int32_t corr = step_corr(nlin_prev, kcorr_n, kconst_n);
@@ -681,61 +719,83 @@ __global__ void __cluster_dims__(kCR, 1, 1) __launch_bounds__(kCT, 1)
         }
         const uint32_t fw = __ballot_sync(FULL, fl), uw = __ballot_sync(FULL, fl && up_new);
         const uint32_t nlw = __ballot_sync(FULL, ln);
-        if (lane == 0) {
-            uint32_t* sd = send + (par * 8 + k) * 4;
-            sd[0] = fw;
-            sd[1] = uw;
-            sd[2] = uint32_t(__popc(nlw));
-            asm volatile("fence.acq_rel.cluster;" ::: "memory");   // release of the slot, before the arrival
+        if (lane < kCR) {
+            const uint32_t bar = dst_mb + 8u * uint32_t(par);
+            st_async2(dst_fu + 8u * 64u * uint32_t(par), fw, uw, bar);
+            st_async1(dst_nl + 4u * 64u * uint32_t(par), uint32_t(__popc(nlw)) | (uint32_t(__popc(fw)) << 16), bar);
         }
-        cl_arrive_relaxed();
+        const uint32_t my_bar = sm_addr(mbar + par);
+        if (tid == 0)
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(my_bar), "r"(kClusterTx)
+                         : "memory");
         if (t >= 0) {
             if (fl) s_up = up_new;
             df = fl;
-            if (t + 1 < S) u = lane_draw(rng, k);            // next step's draw, while the barrier completes
+            if (t + 1 < S) u = lane_draw(rng, k);            // next step's draw, while the words travel
         }
-        cl_wait();
-        // flip word wi = kk*8 + rr (round kk, source CTA rr) and its new-spin word; then the n_lin partials
-        if (tid < 128) {
-            const int wi = tid & 63, kk = wi >> 3, rr = wi & 7;
-            const uint32_t v = cl_load(cl_map(sm_addr(send + (par * 8 + kk) * 4 + (tid >> 6)), uint32_t(rr)));
-            reinterpret_cast<uint32_t*>(recv + (par * 2 + (tid >> 6)) * 16)[wi] = v;
-            if (tid < 64) {                                 // |F|: popcounts of the 64 flip words, two warp sums
-                int32_t c = __popc(v);
-#pragma unroll
-                for (int o = 16; o >= 1; o >>= 1) c += __shfl_xor_sync(FULL, c, o);
-                if (lane == 0) s_nf[tid >> 5] = c;
-            }
-        } else if (tid < 192) {
-            const int e = tid - 128;                        // (source CTA e / 8, warp e % 8)
-            int32_t v = int32_t(cl_load(cl_map(sm_addr(send + (par * 8 + (e & 7)) * 4 + 2), uint32_t(e >> 3))));
-#pragma unroll
-            for (int o = 16; o >= 1; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
-            if (lane == 0) s_nl[(tid >> 5) - 4] = v;
+        if (ok && !cl_wait_for(my_bar, uint32_t((m >> 1) & 1), job.wait_ns)) {
+            ok = false;
+            if (job.err) atomicCAS(job.err, 0, kClusterErrRecv);
         }
-        __syncthreads();
+        // n_lin and |F| of step t: each warp sums the 64 packed counts (low half: band, high half: flips)
+        uint32_t pc = NLc[par * 64 + 2 * lane] + NLc[par * 64 + 2 * lane + 1];
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) pc += __shfl_xor_sync(FULL, pc, o);
+        int32_t nf = int32_t(pc >> 16);
         if (t >= 0) {
-            nlin_prev = s_nl[0] + s_nl[1];
+            nlin_prev = int32_t(pc & 0xffffu);
             if (rank == 0 && tid == 0 && job.trace && job.out_trace) job.out_trace[size_t(c) * S + t] = nlin_prev;
+            if (tid == 0) flips += nf;
         }
-        // D = sum over the 64 words of popc(F & (U ^ J_y)); |F| from the same words
-        const uint4* Fv = recv + par * 2 * 16;
-        const uint4* Uv = Fv + 16;
+        // D = sum over the 64 words x_w = F_w & (U_w ^ J_yw) of popc(x_w), through a carry-save (Harley-Seal) tree
+        // over blocks of 16 words: 60 three-input adders and 8 popcounts per thread where a popcount per word took 64
+        const uint4* FUv = reinterpret_cast<const uint4*>(FU + par * 64);   // {F_2q, U_2q, F_2q+1, U_2q+1}
         const uint4* Jv = Jr + tid * 16;
-        int32_t D = 0, nf = s_nf[0] + s_nf[1];
+        uint32_t ones = 0u, twos = 0u, fours = 0u, eights = 0u;
+        int32_t sixteens = 0;
 #pragma unroll
-        for (int ch = 0; ch < 16; ++ch) {
-            const uint4 J4 = Jv[ch ^ (tid & 7)], F4 = Fv[ch], U4 = Uv[ch];
-            D += __popc(F4.x & (U4.x ^ J4.x)) + __popc(F4.y & (U4.y ^ J4.y)) + __popc(F4.z & (U4.z ^ J4.z)) +
-                 __popc(F4.w & (U4.w ^ J4.w));
+        for (int b = 0; b < 4; ++b) {
+            uint32_t x[16];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int ch = 4 * b + q;
+                const uint4 J4 = Jv[ch ^ (tid & 7)], A = FUv[2 * ch], B = FUv[2 * ch + 1];
+                x[4 * q + 0] = A.x & (A.y ^ J4.x);
+                x[4 * q + 1] = A.z & (A.w ^ J4.y);
+                x[4 * q + 2] = B.x & (B.y ^ J4.z);
+                x[4 * q + 3] = B.z & (B.w ^ J4.w);
+            }
+            uint32_t tA, tB, fA, fB, eA, eB, s16;
+            csa(ones, tA, ones, x[0], x[1]);
+            csa(ones, tB, ones, x[2], x[3]);
+            csa(twos, fA, twos, tA, tB);
+            csa(ones, tA, ones, x[4], x[5]);
+            csa(ones, tB, ones, x[6], x[7]);
+            csa(twos, fB, twos, tA, tB);
+            csa(fours, eA, fours, fA, fB);
+            csa(ones, tA, ones, x[8], x[9]);
+            csa(ones, tB, ones, x[10], x[11]);
+            csa(twos, fA, twos, tA, tB);
+            csa(ones, tA, ones, x[12], x[13]);
+            csa(ones, tB, ones, x[14], x[15]);
+            csa(twos, fB, twos, tA, tB);
+            csa(fours, eB, fours, fA, fB);
+            csa(eights, s16, eights, eA, eB);
+            sixteens += __popc(s16);
         }
-        if (t >= 0 && tid == 0) flips += nf;
+        int32_t D = 16 * sixteens + 8 * __popc(eights) + 4 * __popc(fours) + 2 * __popc(twos) + __popc(ones);
         // the diagonal: if y itself is in F, its term (J_yy = 0, stored as a 0 bit) was counted as -s'_y
         if (fl) {
             nf -= 1;
             D -= up_new ? 1 : 0;
         }
         h += (t >= 0 ? 2 : 1) * (nf - 2 * D);
+    }
+    if (!ok) {
+        // a wait gave up: let pushes still in flight toward this CTA land before the cluster may exit
+        const uint64_t t0 = cl_globaltimer();
+        while (cl_globaltimer() - t0 < 200000ull) {
+        }
     }
     // outputs: spins, sum s*h, sum b*s (active slots), flips
     long long sh = 0, bs = 0;

@@ -296,7 +296,8 @@ ANC_API void anc_mf_destroy(anc_meanfield* mf);
  * kernels launched after this call, process-wide. A wait that reaches it makes the kernel record an error, stop
  * issuing work, wait (with its own fixed bound) for the copies and MMAs it has in flight, and return; the call
  * returns ANC_ETIMEOUT, the results are not valid, and the context and handles stay usable. 0 gives up at the first
- * unsatisfied poll (for tests of that path). anc_get_wait_ns returns the current limit. */
+ * unsatisfied poll (for tests of that path). The cluster engine's exchange waits use the same limit with a floor of
+ * 10 ms. anc_get_wait_ns returns the current limit. */
 ANC_API int anc_set_wait_ns(uint64_t ns);
 ANC_API uint64_t anc_get_wait_ns(void);
 
