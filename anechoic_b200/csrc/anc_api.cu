@@ -81,9 +81,9 @@ int pad_np(int n) { return std::max(2048, ((n + 255) / 256) * 256); }
 //                                               flip rewrites n fields from one row of bit planes (K planes);
 //                                               a_1 = 3.4, a_2 = 5.1, a_4 = 10.2, c_1 = 5.4e-6, c_2 = 1.6e-5,
 //                                               c_4 = 3.3e-5 (least squares in log time over the one-wave launches)
-//   cluster  1.96                                (1-bit couplings, NP = 2048: every thread sums popcounts over all 64
+//   cluster  1.30                                (1-bit couplings, NP = 2048: every thread sums popcounts over all 64
 //                                               flip words whatever flipped, so the step costs the same at any phi;
-//                                               measured 1.93 ... 2.05)
+//                                               measured 1.28 per step for one anneal, 1.33 for a wave of 15)
 //   tensor   a constant per kernel: the MMA chain and the decisions cost the same whatever flips: fp4 8.1 (8.3 with
 //            more than one replica group per wave), int8 23.3 at NP = 2048, 21.7 and 28.3 at NP = 3072 and 4096,
 //            streaming 99.5 (measured 99.5 at NP = 10240 and 98 at NP = 16384: bound by its step latency, not by
@@ -117,7 +117,7 @@ int estimate_engines(int n, int K, int nchains, int S, double phi, bool fp4, con
         us[ANC_ENGINE_TENSOR] = waves(ANC_ENGINE_TENSOR) * S * tensor_step_us(n, fp4, (groups + 127) / 128);
     }
     if (per_wave[ANC_ENGINE_CLUSTER] > 0)
-        us[ANC_ENGINE_CLUSTER] = waves(ANC_ENGINE_CLUSTER) * S * 1.96;
+        us[ANC_ENGINE_CLUSTER] = waves(ANC_ENGINE_CLUSTER) * S * 1.30;
     int best = ANC_ENGINE_PLAIN;
     for (int e : {ANC_ENGINE_PLAIN, ANC_ENGINE_TENSOR, ANC_ENGINE_CLUSTER})
         if (us[e] >= 0 && (us[best] < 0 || us[e] < us[best])) best = e;

@@ -40,7 +40,7 @@ def main():
                        "ms": {}, "kernel": {}}
                 flips = None
                 for e in ("plain", "cluster", "tensor"):
-                    if e == "cluster" and (c > 32 or dev.info["kbits"] != 1 or inst.n > 2048):
+                    if e == "cluster" and (dev.info["kbits"] != 1 or inst.n > 2048):
                         continue
                     times = []
                     for k in range(4):
