@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <utility>
 #include <vector>
 
 #include "anc_meanfield.cuh"
@@ -48,6 +49,13 @@ namespace {
 
 using namespace ptx;
 
+// Programmatic dependent launch. Every kernel of a step sequence lets the next one in the stream launch right away
+// (pdl_trigger), so that kernel's prologue -- TMEM allocation, barrier set-up, the TMA load of its J tile -- overlaps
+// this kernel; it then waits for this kernel to complete, with its memory visible (pdl_wait), before reading anything
+// this kernel wrote. Both are no-ops in a kernel launched without the programmatic-serialization attribute.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 constexpr int kRows = 128;                 // rows of J per CTA (MMA M)
 constexpr int kRep = kMfReplicas;          // MMA N
 constexpr int kKC = 256;                   // K per CTA: 4 swizzle atoms of 64 BF16
@@ -79,6 +87,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int y0 = blockIdx.x * kRows, k0 = blockIdx.y * kKC;
     const uint32_t bar_full = smem_u32(bars), bar_done = smem_u32(bars + 1);
+    pdl_trigger();
     if (tid == 0) {
         mbar_init(bar_full, 1);
         mbar_init(bar_done, 1);
@@ -96,8 +105,12 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     const uint32_t tmem = *tslot;
     if (tid == 0) {
         mbar_arrive_expect_tx(bar_full, 4 * (kATile + 3 * kBTile));
+        for (int a = 0; a < 4; ++a) tma_load_2d(smem_u32(sa + a * kATile), &mapJ, k0 + 64 * a, y0, bar_full);
+        // the operand terms come from the previous kernel; the partials this CTA writes are read by the previous
+        // step's elementwise kernel: both only after it completed. The other threads write only after bar_done,
+        // which follows this wait.
+        pdl_wait();
         for (int a = 0; a < 4; ++a) {
-            tma_load_2d(smem_u32(sa + a * kATile), &mapJ, k0 + 64 * a, y0, bar_full);
             tma_load_2d(smem_u32(sbh + a * kBTile), &mapXh, k0 + 64 * a, 0, bar_full);
             tma_load_2d(smem_u32(sbm + a * kBTile), &mapXm, k0 + 64 * a, 0, bar_full);
             tma_load_2d(smem_u32(sbl + a * kBTile), &mapXl, k0 + 64 * a, 0, bar_full);
@@ -219,6 +232,8 @@ __device__ __forceinline__ float sum_parts(const float* __restrict__ parts, int 
 __global__ void __launch_bounds__(kElemThreads) mf_prep_kernel(const float* __restrict__ m, int n, int npad,
                                                                float* __restrict__ nout, __nv_bfloat16* __restrict__ x) {
     __shared__ float red[32];
+    pdl_trigger();
+    pdl_wait();
     const int r = blockIdx.x, i = blockIdx.y * kElemThreads + threadIdx.x;
     const size_t idx = size_t(r) * npad + i;
     const float v = m[idx];
@@ -244,6 +259,8 @@ struct FwdArgs {
 
 __global__ void __launch_bounds__(kElemThreads) mf_fwd_kernel(const FwdArgs a) {
     __shared__ float red[32];
+    pdl_trigger();
+    pdl_wait();
     const int r = blockIdx.x, npad = a.npad, nch = gridDim.y, i = blockIdx.y * kElemThreads + threadIdx.x;
     const float beta = a.beta[a.t], q = a.q[a.t];
     const float gamma = a.u[a.t] * sum_parts(a.n_cur, nch, r) + a.w[a.t];
@@ -287,6 +304,8 @@ struct BwdArgs {
 //   dL/dbeta_t += sum abar_t P_t, dL/dq_t += sum pbar_t m_t, dL/du_t += -s_t n_t, dL/dw_t += -s_t
 __global__ void __launch_bounds__(kElemThreads) mf_bwd_kernel(const BwdArgs a) {
     __shared__ float red[3 * 32];
+    pdl_trigger();
+    pdl_wait();
     const int r = blockIdx.x, npad = a.npad, t = a.t, nch = gridDim.y, ch = blockIdx.y;
     const int i = ch * kElemThreads + threadIdx.x;
     const float beta = a.beta[t];
@@ -323,6 +342,8 @@ __global__ void __launch_bounds__(kElemThreads) mf_bwd_kernel(const BwdArgs a) {
 
 // gsched[t][k][r] = sum over chunks of gparts[t][k][ch][r] (chunk order); one thread per (t, k, r).
 __global__ void mf_gsum_kernel(const float* __restrict__ gparts, int S, int nch, float* __restrict__ gsched) {
+    pdl_trigger();
+    pdl_wait();
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= S * 4 * kRep) return;
     const int r = e % kRep, tk = e / kRep;
@@ -337,11 +358,29 @@ bool check(cudaError_t e, const char* what, std::string* why) {
     return false;
 }
 
+// Launch with programmatic stream serialization (see pdl_trigger / pdl_wait): the kernel may start while the previous
+// kernel in the stream still runs, and waits for it where it reads that kernel's outputs.
+template <class... KArgs, class... Args>
+cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                       Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
 int gemm(MfContext* c, const CUtensorMap (&mx)[3], cudaStream_t st, std::string* why) {
-    mf_gemm_kernel<<<dim3(c->npad / kRows, c->npad / kKC), kGemmThreads, gemm_smem(), st>>>(c->mapJ, mx[0], mx[1], mx[2],
-                                                                                           c->partial, c->npad, c->err,
-                                                                                           c->wait_ns);
-    return check(cudaGetLastError(), "mean-field GEMM launch", why) ? 0 : -2;
+    const cudaError_t e = launch_pdl(mf_gemm_kernel, dim3(c->npad / kRows, c->npad / kKC), dim3(kGemmThreads),
+                                     gemm_smem(), st, c->mapJ, mx[0], mx[1], mx[2], c->partial, c->npad, c->err,
+                                     c->wait_ns);
+    return check(e, "mean-field GEMM launch", why) ? 0 : -2;
 }
 
 float* mslot(float* base, int k, int npad) { return base + size_t(k) * kRep * npad; }
@@ -376,8 +415,9 @@ int run_steps(MfContext* c, int t0, int t1, const float* beta, const float* q, c
         a.x = c->xm;
         a.n_next = c->nbuf + size_t(t + 1) * nch(c) * kRep;
         a.P_out = pout(t);
-        mf_fwd_kernel<<<dim3(kRep, nch(c)), kElemThreads, 0, st>>>(a);
-        if (!check(cudaGetLastError(), "mean-field forward step", why)) return -2;
+        if (!check(launch_pdl(mf_fwd_kernel, dim3(kRep, nch(c)), dim3(kElemThreads), 0, st, a), "mean-field forward step",
+                   why))
+            return -2;
     }
     return 0;
 }
@@ -539,8 +579,9 @@ int backward_body(MfContext* c, int S, const float* beta, const float* q, const 
             a.x = c->xp;
             a.s_out = c->svec + size_t(t % 3) * nch(c) * kRep;
             a.gparts = c->gparts;
-            mf_bwd_kernel<<<dim3(kRep, nch(c)), kElemThreads, 0, st>>>(a);
-            if (!check(cudaGetLastError(), "mean-field adjoint step", why)) return -2;
+            if (!check(launch_pdl(mf_bwd_kernel, dim3(kRep, nch(c)), dim3(kElemThreads), 0, st, a),
+                       "mean-field adjoint step", why))
+                return -2;
         }
     }
     const int ne = S * 4 * kRep;
