@@ -81,9 +81,10 @@ int pad_np(int n) { return std::max(2048, ((n + 255) / 256) * 256); }
 //                                               flip rewrites n fields from one row of bit planes (K planes);
 //                                               a_1 = 3.4, a_2 = 5.1, a_4 = 10.2, c_1 = 5.4e-6, c_2 = 1.6e-5,
 //                                               c_4 = 3.3e-5 (least squares in log time over the one-wave launches)
-//   cluster  1.30                                (1-bit couplings, NP = 2048: every thread sums popcounts over all 64
-//                                               flip words whatever flipped, so the step costs the same at any phi;
-//                                               measured 1.28 per step for one anneal, 1.33 for a wave of 15)
+//   cluster  1.15 when the anneals fit one wave of 16-CTA clusters (taken as half the 8-CTA wave: 7 here), else
+//            1.30 per wave of 8-CTA clusters (1-bit couplings, NP = 2048: every thread sums popcounts over all 64
+//            flip words whatever flipped, so the step costs the same at any phi; measured 1.13 - 1.14 for 1 - 7
+//            anneals on 16 CTAs, 1.25 - 1.35 per wave of up to 15 on 8)
 //   tensor   a constant per kernel: the MMA chain and the decisions cost the same whatever flips: fp4 8.1 (8.3 with
 //            more than one replica group per wave), int8 23.3 at NP = 2048, 21.7 and 28.3 at NP = 3072 and 4096,
 //            streaming 99.5 (measured 99.5 at NP = 10240 and 98 at NP = 16384: bound by its step latency, not by
@@ -117,7 +118,8 @@ int estimate_engines(int n, int K, int nchains, int S, double phi, bool fp4, con
         us[ANC_ENGINE_TENSOR] = waves(ANC_ENGINE_TENSOR) * S * tensor_step_us(n, fp4, (groups + 127) / 128);
     }
     if (per_wave[ANC_ENGINE_CLUSTER] > 0)
-        us[ANC_ENGINE_CLUSTER] = waves(ANC_ENGINE_CLUSTER) * S * 1.30;
+        us[ANC_ENGINE_CLUSTER] = nchains <= per_wave[ANC_ENGINE_CLUSTER] / 2 ? S * 1.15
+                                                                             : waves(ANC_ENGINE_CLUSTER) * S * 1.30;
     int best = ANC_ENGINE_PLAIN;
     for (int e : {ANC_ENGINE_PLAIN, ANC_ENGINE_TENSOR, ANC_ENGINE_CLUSTER})
         if (us[e] >= 0 && (us[best] < 0 || us[e] < us[best])) best = e;
@@ -140,6 +142,7 @@ struct anc_instance {
     anc::TensorInstance tensor;                   // tensor-engine operands (built on first use)
     bool tensor_ready = false;
     int per_wave[4] = {-1, -1, -1, -1};           // anneals per wave of each engine (ANC_ENGINE_*; -1: not queried)
+    int cluster16_wave = -1;                      // anneals one wave of 16-CTA clusters runs (-1: not queried)
     uint64_t uid = g_next_uid.fetch_add(1);       // identifies the instance to the tables' flip record
     // per-handle workspace for single-job launches
     DevBuf<int> counter;
@@ -420,6 +423,17 @@ const int* engine_waves(anc_instance* I) {
     return I->per_wave;
 }
 
+// Anneals one wave of 16-CTA clusters runs on this device (0 if none fits); queried once per instance.
+int cluster16_wave(anc_instance* I) {
+    if (I->cluster16_wave < 0) {
+        int c = 0;
+        if (anc::plain_cluster_max_active(&c, 16) != cudaSuccess) c = 0;
+        cudaGetLastError();
+        I->cluster16_wave = std::max(0, c);
+    }
+    return I->cluster16_wave;
+}
+
 // Tuning key of a run of nchains anneals of this instance on `kernel` (ANC_KERNEL_PLAIN for dense instances,
 // ANC_KERNEL_TENSOR_FP4): device, kernel, NP, K and, for the fp4 kernel, the replica groups one wave runs at once.
 std::array<int, 5> tune_key(anc_instance* I, int kernel, int nchains) {
@@ -531,6 +545,11 @@ int run_device_impl(anc_instance* I, anc_tables* tb, uint64_t seed, uint32_t off
         if (!anc::plain_cluster_supported(I->K, I->np))
             return fail(ANC_EINVAL, "the cluster engine needs dense 1-bit couplings with n <= 2048 (n=%d K=%d)", I->n,
                         I->K);
+        const int forced = o ? o->kernel_variant : 0;
+        if (forced > 2)
+            return fail(ANC_EINVAL, "kernel_variant %d out of range: the cluster engine has 2 variants", forced);
+        int ctas = forced == 2 ? 16 : 8;
+        if (forced == 0) ctas = nchains <= cluster16_wave(I) ? 16 : 8;
         CK(I->w_err.ensure(1));
         CK(cudaMemsetAsync(I->w_err.p, 0, sizeof(int), st));
         job.err = I->w_err.p;
@@ -538,7 +557,7 @@ int run_device_impl(anc_instance* I, anc_tables* tb, uint64_t seed, uint32_t off
         // forced expiry (a limit of 0) is kept off this engine (a step takes about 2 us)
         job.wait_ns = std::max<uint64_t>(10000000ull, g_wait_ns.load());
         I->cluster_err_pending = true;
-        rc = anc::plain_cluster_launch(job, st);
+        rc = anc::plain_cluster_launch(job, st, ctas);
         if (rc) return cuda_fail(cudaError_t(rc), "cluster engine launch");
         g_last_kernel = ANC_KERNEL_PLAIN_CLUSTER;
         return ANC_OK;

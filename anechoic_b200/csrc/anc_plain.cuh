@@ -108,7 +108,8 @@ int plain_max_blocks_per_sm(int K, int P, size_t smem, int* out, bool stream = f
 // Cluster variant (plain_engine.cu): one anneal per cluster of 8 CTAs, dense K = 1 couplings with NP = 2048 only.
 // job.ntrials anneals, trial c = job.trial_offset + c; every output is written (no zeroing needed).
 bool plain_cluster_supported(int K, int np);
-int plain_cluster_launch(const PlainJob& job, cudaStream_t stream);
-int plain_cluster_max_active(int* out);      // clusters co-resident on this device
+// One anneal per cluster of `ctas` CTAs (8, or 16: half the slots per SM, a non-portable cluster size)
+int plain_cluster_launch(const PlainJob& job, cudaStream_t stream, int ctas = 8);
+int plain_cluster_max_active(int* out, int ctas = 8);      // clusters of `ctas` co-resident on this device
 
 }  // namespace anc

@@ -548,7 +548,9 @@ __global__ void __launch_bounds__(T, 1) plain_kernel(const __grid_constant__ Pla
 }
 
 // ------------------------------------------------------------------------------------------------ cluster variant
-// One anneal spread over a cluster of kCR = 8 CTAs (dense K = 1, NP = 2048), for the lowest latency per anneal.
+// One anneal spread over a cluster of CR = 8 or 16 CTAs (dense K = 1, NP = 2048), for the lowest latency per anneal.
+// With 16 CTAs each SM holds 128 slots, half the update's work, and a warp's words interleave two rounds (below); the
+// description that follows is for CR = 8.
 // CTA r owns the 256 slots i = k*256 + 32r + l (round k, RNG lane 32r + l), one per thread: thread t = 32k + l keeps
 // its slot's field, spin and last-flip bit in registers and a copy of lane 32r + l's xoshiro128** state, which it
 // advances 8 draws per step and uses the k-th (every lane's stream is consumed in round order, as the golden model
@@ -571,8 +573,6 @@ __global__ void __launch_bounds__(T, 1) plain_kernel(const __grid_constant__ Pla
 // CTA's words of step m + 1, and a CTA sends those only after each of its warps has finished reading buffer p of step
 // m (the words sent depend on the fields those reads updated); so the pushes of step m + 2 cannot overtake the reads
 // of step m, nor count toward mbarrier p's phase of step m.
-constexpr int kCT = 256;                  // threads per CTA (one slot each)
-constexpr int kCR = 8;                    // CTAs per anneal
 constexpr uint32_t kClusterTx = 64 * 12;  // exchange bytes a CTA receives per step
 constexpr size_t kClusterSmem = 116 * 1024;   // above half an SM's shared memory: one CTA per SM
 
@@ -643,46 +643,64 @@ __device__ __forceinline__ uint32_t lane_draw(Xoshiro& rng, int k) {
     return u;
 }
 
-template <int P>
-__global__ void __cluster_dims__(kCR, 1, 1) __launch_bounds__(kCT, 1)
+template <int CR>
+__global__ void __cluster_dims__(CR, 1, 1) __launch_bounds__(2048 / CR, 1)
     plain_cluster_kernel(const __grid_constant__ PlainJob job) {
     constexpr int NWJ = 64;
-    (void)P;
+    constexpr int CT = 2048 / CR;                 // owned slots (threads) per CTA
+    constexpr int LPC = 256 / CR;                 // RNG lanes per CTA
+    static_assert((CR == 8 || CR == 16) && (CT / 32) * CR == 64, "64 exchange words per step");
     extern __shared__ __align__(16) uint8_t smem_raw[];
-    // J row of owned slot t: 16 chunks of 16 bytes, chunk c at position c ^ (t & 7) (conflict-free 16-byte loads)
-    uint4* Jr = reinterpret_cast<uint4*>(smem_raw);                     // [256][16]
-    uint2* FU = reinterpret_cast<uint2*>(Jr + kCT * 16);                // [2 parities][64 words]: flip, new spin +1
+    // J row of owned slot t in exchange-word order: 16 chunks of 16 bytes, chunk c at position c ^ (t & 7)
+    // (conflict-free 16-byte loads)
+    uint4* Jr = reinterpret_cast<uint4*>(smem_raw);                     // [CT][16]
+    uint2* FU = reinterpret_cast<uint2*>(Jr + CT * 16);                 // [2 parities][64 words]: flip, new spin +1
     uint32_t* NLc = reinterpret_cast<uint32_t*>(FU + 2 * 64);            // [2][64]: band count | flip count << 16
     uint64_t* mbar = reinterpret_cast<uint64_t*>(NLc + 2 * 64);          // [2]: exchange of each parity
-    __shared__ long long s_red[2][kCT / 32];
-    __shared__ long long s_part[kCR][3];                    // rank 0: every rank's sum of s*h, of b*s and flips
+    __shared__ long long s_red[2][CT / 32];
+    __shared__ long long s_part[CR][3];                     // rank 0: every rank's sum of s*h, of b*s and flips
 
-    const int tid = threadIdx.x, lane = tid & 31, k = tid >> 5;
+    // warp w covers rounds w * 32 / LPC ..; its lane holds round k of RNG lane l of this CTA's LPC lanes
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int k = w * (32 / LPC) + lane / LPC;
     const uint32_t rank = cl_rank();
     const int c = int(cl_id());                             // anneal index within the launch
     const int n = job.n, nw = job.nw, S = job.tab.S;
     const int32_t hclamp = job.hclamp;
     const int32_t* __restrict__ bias = job.bias;
-    const int slot = k * kLanes + 32 * int(rank) + lane;
+    const int rlane = LPC * int(rank) + lane % LPC;         // RNG lane
+    const int slot = k * kLanes + rlane;
     const bool valid = slot < n;
+    const int wi_own = w * CR + int(rank);                  // this warp's exchange word
 
     if (tid == 0) {
         for (int q = 0; q < 2; ++q)
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(sm_addr(mbar + q)) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    {
+    if (LPC == 32) {
+        // exchange word w * 8 + r is spin word w * 8 + r: the row as stored
         const uint4* row = reinterpret_cast<const uint4*>(job.planes + size_t(slot) * NWJ);
         for (int ch = 0; ch < 16; ++ch) Jr[tid * 16 + (ch ^ (tid & 7))] = __ldg(row + ch);
+    } else {
+        // exchange word w * 16 + r holds the 16 lanes 16 r .. of rounds 2w (low half) and 2w + 1 (high half): halves
+        // of spin words 2w * 8 + r / 2 and (2w + 1) * 8 + r / 2
+        const uint32_t* row = job.planes + size_t(slot) * NWJ;
+        uint32_t* Jw = reinterpret_cast<uint32_t*>(Jr + tid * 16);
+        for (int wi = 0; wi < 64; ++wi) {
+            const int ww = wi / CR, rr = wi % CR;
+            const uint32_t A = __ldg(row + (2 * ww) * 8 + rr / 2), B = __ldg(row + (2 * ww + 1) * 8 + rr / 2);
+            Jw[4 * ((wi >> 2) ^ (tid & 7)) + (wi & 3)] = __byte_perm(A, B, (rr & 1) ? 0x7632 : 0x5410);
+        }
     }
-    // remote addresses this thread pushes to (lanes 0 .. 7: CTA `lane`), word wi = k*8 + rank of each buffer
-    const uint32_t dst_rank = uint32_t(lane & 7);
-    const uint32_t dst_fu = cl_map(sm_addr(FU + k * 8 + int(rank)), dst_rank);
-    const uint32_t dst_nl = cl_map(sm_addr(NLc + k * 8 + int(rank)), dst_rank);
+    // remote addresses this thread pushes to (lanes 0 .. CR - 1: CTA `lane`), word wi_own of each buffer
+    const uint32_t dst_rank = uint32_t(lane % CR);
+    const uint32_t dst_fu = cl_map(sm_addr(FU + wi_own), dst_rank);
+    const uint32_t dst_nl = cl_map(sm_addr(NLc + wi_own), dst_rank);
     const uint32_t dst_mb = cl_map(sm_addr(mbar), dst_rank);
 
     Xoshiro rng;
-    rng_seed(rng, job.seed, job.trial_offset + uint32_t(c), 32u * rank + uint32_t(lane));
+    rng_seed(rng, job.seed, job.trial_offset + uint32_t(c), uint32_t(rlane));
     const uint32_t r0 = lane_draw(rng, k);
     bool s_up = valid ? (r0 >> 31) != 0u : true;            // padding slots: +1
     bool df = valid && !s_up;                               // s != s_prev (s_prev = +1 initially)
@@ -719,7 +737,7 @@ __global__ void __cluster_dims__(kCR, 1, 1) __launch_bounds__(kCT, 1)
         }
         const uint32_t fw = __ballot_sync(FULL, fl), uw = __ballot_sync(FULL, fl && up_new);
         const uint32_t nlw = __ballot_sync(FULL, ln);
-        if (lane < kCR) {
+        if (lane < CR) {
             const uint32_t bar = dst_mb + 8u * uint32_t(par);
             st_async2(dst_fu + 8u * 64u * uint32_t(par), fw, uw, bar);
             st_async1(dst_nl + 4u * 64u * uint32_t(par), uint32_t(__popc(nlw)) | (uint32_t(__popc(fw)) << 16), bar);
@@ -805,18 +823,31 @@ __global__ void __cluster_dims__(kCR, 1, 1) __launch_bounds__(kCT, 1)
         if (job.out_h) job.out_h[size_t(c) * n + slot] = h;
     }
     const uint32_t sword = __ballot_sync(FULL, s_up);
-    const int wi = k * 8 + int(rank);
-    if (lane == 0 && wi < nw) job.out_spins[size_t(c) * nw + wi] = sword & valid_mask(wi, n);
+    if (lane == 0) {
+        if (LPC == 32) {
+            if (wi_own < nw) job.out_spins[size_t(c) * nw + wi_own] = sword & valid_mask(wi_own, n);
+        } else {
+            // the two 16-bit halves of the exchange word are half words of spin words 2w * 8 + r / 2 and
+            // (2w + 1) * 8 + r / 2; every half of every spin word is written by exactly one CTA
+            uint16_t* out16 = reinterpret_cast<uint16_t*>(job.out_spins + size_t(c) * nw);
+            for (int hh = 0; hh < 2; ++hh) {
+                const int sw_i = (2 * w + hh) * 8 + int(rank) / 2, half = int(rank) & 1;
+                if (sw_i < nw)
+                    out16[2 * sw_i + half] = uint16_t(((sword >> (16 * hh)) & 0xffffu) &
+                                                      (valid_mask(sw_i, n) >> (16 * half)));
+            }
+        }
+    }
     sh = warp_sum64(sh);
     bs = warp_sum64(bs);
     if (lane == 0) {
-        s_red[0][k] = sh;
-        s_red[1][k] = bs;
+        s_red[0][w] = sh;
+        s_red[1][w] = bs;
     }
     __syncthreads();
     if (tid == 0) {
         long long a = 0, b = 0;
-        for (int w = 0; w < kCT / 32; ++w) { a += s_red[0][w]; b += s_red[1][w]; }
+        for (int ww = 0; ww < CT / 32; ++ww) { a += s_red[0][ww]; b += s_red[1][ww]; }
         const uint32_t ad = cl_map(sm_addr(&s_part[rank][0]), 0u);
         asm volatile("st.shared::cluster.u64 [%0], %1;" ::"r"(ad), "l"(a) : "memory");
         asm volatile("st.shared::cluster.u64 [%0], %1;" ::"r"(ad + 8u), "l"(b) : "memory");
@@ -825,7 +856,7 @@ __global__ void __cluster_dims__(kCR, 1, 1) __launch_bounds__(kCT, 1)
     cl_sync();
     if (rank == 0 && tid == 0) {
         long long a = 0, b = 0;
-        for (int r = 0; r < kCR; ++r) { a += s_part[r][0]; b += s_part[r][1]; }
+        for (int r = 0; r < CR; ++r) { a += s_part[r][0]; b += s_part[r][1]; }
         job.out_sum_sh[c] = a;
         if (job.out_sum_bs) job.out_sum_bs[c] = b;
         job.out_flips[c] = s_part[0][2];
@@ -896,30 +927,47 @@ int plain_launch(const PlainLaunch& L, int K, int P, int grid, size_t smem, cuda
 
 bool plain_cluster_supported(int K, int np) { return K == 1 && np == 2048; }
 
-int plain_cluster_launch(const PlainJob& job, cudaStream_t st) {
-    auto fn = plain_cluster_kernel<12>;
+namespace {
+// The cluster kernel for `cr` CTAs per anneal with its attributes set (16 is a non-portable cluster size).
+template <int CR>
+cudaError_t cluster_prepare() {
+    auto fn = plain_cluster_kernel<CR>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kClusterSmem));
+    if (e == cudaSuccess && CR > 8) e = cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    return e;
+}
+template <int CR>
+int cluster_launch_t(const PlainJob& job, cudaStream_t st) {
+    cudaError_t e = cluster_prepare<CR>();
     if (e != cudaSuccess) return int(e);
-    fn<<<job.ntrials * kCR, kCT, kClusterSmem, st>>>(job);
+    plain_cluster_kernel<CR><<<job.ntrials * CR, 2048 / CR, kClusterSmem, st>>>(job);
     return int(cudaGetLastError());
 }
-
-int plain_cluster_max_active(int* out) {
-    auto fn = plain_cluster_kernel<12>;
-    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kClusterSmem));
+template <int CR>
+int cluster_max_active_t(int* out) {
+    cudaError_t e = cluster_prepare<CR>();
     if (e != cudaSuccess) return int(e);
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeClusterDimension;
-    at[0].val.clusterDim.x = kCR;
+    at[0].val.clusterDim.x = CR;
     at[0].val.clusterDim.y = 1;
     at[0].val.clusterDim.z = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    cfg.gridDim = dim3(kCR);
-    cfg.blockDim = dim3(kCT);
+    cfg.gridDim = dim3(CR);
+    cfg.blockDim = dim3(2048 / CR);
     cfg.dynamicSmemBytes = kClusterSmem;
-    return int(cudaOccupancyMaxActiveClusters(out, fn, &cfg));
+    return int(cudaOccupancyMaxActiveClusters(out, plain_cluster_kernel<CR>, &cfg));
+}
+}  // namespace
+
+int plain_cluster_launch(const PlainJob& job, cudaStream_t st, int ctas) {
+    return ctas == 16 ? cluster_launch_t<16>(job, st) : cluster_launch_t<8>(job, st);
+}
+
+int plain_cluster_max_active(int* out, int ctas) {
+    return ctas == 16 ? cluster_max_active_t<16>(out) : cluster_max_active_t<8>(out);
 }
 
 int plain_max_blocks_per_sm(int K, int P, size_t smem, int* out, bool stream) {

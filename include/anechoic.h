@@ -119,7 +119,8 @@ typedef struct {
                            (anc_sparse_tuning), v + 1 = force variant v (0 .. 3) */
     int kernel_variant; /* dense instances on the plain engine and the tensor engine's fp4 kernel: 0 = the variant the
                            run-time tuner chose (anc_kernel_tuning; the default variant before any tuning), v + 1 =
-                           force variant v */
+                           force variant v. Cluster engine: 0 = 16 CTAs per anneal when the anneals fit one wave of
+                           16-CTA clusters, else 8; 1 = 8 CTAs; 2 = 16 CTAs */
 } anc_run_opts;
 
 /* No counterpart in the reference (its kernel geometry is fixed per build by flags, sca_gpu_bias.cu:637-644). The

@@ -104,3 +104,33 @@ def test_refuses_other_instances(cuda):
         with pytest.raises(A.AncError) as e:
             A.run(A.DeviceInstance(inst), tb, 1, 0, 1, engine="cluster")
         assert e.value.code == -1 and "cluster" in str(e.value)
+
+
+@pytest.mark.parametrize("variant", [1, 2])
+def test_cluster_sizes_forced_vs_oracle(cuda, oracle, variant):
+    """Both cluster sizes, forced through anc_run_opts.kernel_variant (1: 8 CTAs per anneal, 2: 16 CTAs, the spin and
+    exchange words then interleaving two rounds' half words), with a bias, a ragged n and more anneals than one wave of
+    16-CTA clusters: every spin, n_lin step, flip count and sum against the golden-model restatement."""
+    import ctypes as C
+    from anechoic_b200 import _lib
+    L = _lib.load()
+    n = 1500
+    inst = I.random_kbit(n, 2, 31, pzero=0.0, bmax=5)
+    dev = A.DeviceInstance(inst)
+    sc = dict(S=200, t0=20.0, t1=2.0, q=4.0, lam=1.05, ramp=True)
+    tb = A.Tables.from_schedule(A.Schedule(**sc))
+    nch = 10
+    ref = oracle.run_batch(n, oracle.tables(**sc), 77, 4321, nch, dense=inst.dense, bias=inst.bias)
+    o = _lib.opts("cluster")
+    o.kernel_variant = variant
+    r = A.RunResult(n=n, trial_offset=4321, spins=np.zeros((nch, A.spin_words(n)), np.uint64),
+                    sum_sh=np.zeros(nch, np.int64), sum_bs=np.zeros(nch, np.int64), flips=np.zeros(nch, np.int64),
+                    trace=np.zeros((nch, sc["S"]), np.int32))
+    _lib.check(L.anc_run(dev._h, tb._h, 77, 4321, nch, C.byref(o), r.spins.ctypes.data, r.sum_sh.ctypes.data,
+                         r.sum_bs.ctypes.data, r.flips.ctypes.data, r.trace.ctypes.data))
+    assert L.anc_last_kernel() == 4
+    for c in range(nch):
+        assert_same(r, {k: v[c] for k, v in ref.items()}, c, f"variant {variant} chain {c}")
+    o.kernel_variant = 3
+    assert L.anc_run(dev._h, tb._h, 77, 0, 1, C.byref(o), r.spins.ctypes.data, r.sum_sh.ctypes.data, None, None,
+                     None) == -1
