@@ -643,12 +643,56 @@ __device__ __forceinline__ uint32_t lane_draw(Xoshiro& rng, int k) {
     return u;
 }
 
+// D of one slot over the 16 NB words of blocks B0 .. B0 + NB - 1 (block b: words 16b .. 16b + 15): the sum of
+// popc(x_w), x_w = F_w & (U_w ^ J_yw), through a carry-save (Harley-Seal) tree -- 15 three-input adders and one
+// popcount per block of 16 words, 4 more popcounts at the end, where a popcount per word took 16 per block.
+template <int NB, int B0>
+__device__ __forceinline__ int32_t cluster_words_d(const uint4* Jv, const uint4* FUv, int swz) {
+    uint32_t ones = 0u, twos = 0u, fours = 0u, eights = 0u;
+    int32_t sixteens = 0;
+#pragma unroll
+    for (int b = B0; b < B0 + NB; ++b) {
+        uint32_t x[16];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int ch = 4 * b + q;               // 16-byte chunk of the J row: words 4ch .. 4ch+3
+            const uint4 J4 = Jv[ch ^ swz], A = FUv[2 * ch], B = FUv[2 * ch + 1];
+            x[4 * q + 0] = A.x & (A.y ^ J4.x);
+            x[4 * q + 1] = A.z & (A.w ^ J4.y);
+            x[4 * q + 2] = B.x & (B.y ^ J4.z);
+            x[4 * q + 3] = B.z & (B.w ^ J4.w);
+        }
+        uint32_t tA, tB, fA, fB, eA, eB, s16;
+        csa(ones, tA, ones, x[0], x[1]);
+        csa(ones, tB, ones, x[2], x[3]);
+        csa(twos, fA, twos, tA, tB);
+        csa(ones, tA, ones, x[4], x[5]);
+        csa(ones, tB, ones, x[6], x[7]);
+        csa(twos, fB, twos, tA, tB);
+        csa(fours, eA, fours, fA, fB);
+        csa(ones, tA, ones, x[8], x[9]);
+        csa(ones, tB, ones, x[10], x[11]);
+        csa(twos, fA, twos, tA, tB);
+        csa(ones, tA, ones, x[12], x[13]);
+        csa(ones, tB, ones, x[14], x[15]);
+        csa(twos, fB, twos, tA, tB);
+        csa(fours, eB, fours, fA, fB);
+        csa(eights, s16, eights, eA, eB);
+        sixteens += __popc(s16);
+    }
+    return 16 * sixteens + 8 * __popc(eights) + 4 * __popc(fours) + 2 * __popc(twos) + __popc(ones);
+}
+
+// Threads per CTA of the cluster kernel: one deciding thread per owned slot, and with 16 CTAs an update helper too.
+__host__ __device__ constexpr int cluster_threads(int cr) { return (2048 / cr) * (cr == 16 ? 2 : 1); }
+
 template <int CR>
-__global__ void __cluster_dims__(CR, 1, 1) __launch_bounds__(2048 / CR, 1)
+__global__ void __cluster_dims__(CR, 1, 1) __launch_bounds__(cluster_threads(CR), 1)
     plain_cluster_kernel(const __grid_constant__ PlainJob job) {
     constexpr int NWJ = 64;
-    constexpr int CT = 2048 / CR;                 // owned slots (threads) per CTA
+    constexpr int CT = 2048 / CR;                 // owned slots (deciding threads) per CTA
     constexpr int LPC = 256 / CR;                 // RNG lanes per CTA
+    constexpr bool HELP = CR == 16;               // a helper thread per slot sums half of its update's words
     static_assert((CR == 8 || CR == 16) && (CT / 32) * CR == 64, "64 exchange words per step");
     extern __shared__ __align__(16) uint8_t smem_raw[];
     // J row of owned slot t in exchange-word order: 16 chunks of 16 bytes, chunk c at position c ^ (t & 7)
@@ -656,12 +700,15 @@ __global__ void __cluster_dims__(CR, 1, 1) __launch_bounds__(2048 / CR, 1)
     uint4* Jr = reinterpret_cast<uint4*>(smem_raw);                     // [CT][16]
     uint2* FU = reinterpret_cast<uint2*>(Jr + CT * 16);                 // [2 parities][64 words]: flip, new spin +1
     uint32_t* NLc = reinterpret_cast<uint32_t*>(FU + 2 * 64);            // [2][64]: band count | flip count << 16
-    uint64_t* mbar = reinterpret_cast<uint64_t*>(NLc + 2 * 64);          // [2]: exchange of each parity
+    int32_t* Dh = reinterpret_cast<int32_t*>(NLc + 2 * 64);              // [2][CT]: helpers' partial D (HELP)
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(Dh + 2 * CT);           // [2]: exchange of each parity
     __shared__ long long s_red[2][CT / 32];
     __shared__ long long s_part[CR][3];                     // rank 0: every rank's sum of s*h, of b*s and flips
 
-    // warp w covers rounds w * 32 / LPC ..; its lane holds round k of RNG lane l of this CTA's LPC lanes
-    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    // warp w covers rounds w * 32 / LPC ..; its lane holds round k of RNG lane l of this CTA's LPC lanes. Thread
+    // st + CT (HELP) is the update helper of slot st.
+    const int tid = threadIdx.x, st = tid % CT, lane = st & 31, w = st >> 5;
+    const bool decider = tid < CT;
     const int k = w * (32 / LPC) + lane / LPC;
     const uint32_t rank = cl_rank();
     const int c = int(cl_id());                             // anneal index within the launch
@@ -678,19 +725,21 @@ __global__ void __cluster_dims__(CR, 1, 1) __launch_bounds__(2048 / CR, 1)
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(sm_addr(mbar + q)) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
+    // with a helper, the deciding thread loads words 0 .. 31 of its slot's row and the helper words 32 .. 63
+    const int wlo = HELP ? 32 * (tid / CT) : 0, whi = HELP ? wlo + 32 : 64;
     if (LPC == 32) {
         // exchange word w * 8 + r is spin word w * 8 + r: the row as stored
         const uint4* row = reinterpret_cast<const uint4*>(job.planes + size_t(slot) * NWJ);
-        for (int ch = 0; ch < 16; ++ch) Jr[tid * 16 + (ch ^ (tid & 7))] = __ldg(row + ch);
+        for (int ch = wlo / 4; ch < whi / 4; ++ch) Jr[st * 16 + (ch ^ (st & 7))] = __ldg(row + ch);
     } else {
         // exchange word w * 16 + r holds the 16 lanes 16 r .. of rounds 2w (low half) and 2w + 1 (high half): halves
         // of spin words 2w * 8 + r / 2 and (2w + 1) * 8 + r / 2
         const uint32_t* row = job.planes + size_t(slot) * NWJ;
-        uint32_t* Jw = reinterpret_cast<uint32_t*>(Jr + tid * 16);
-        for (int wi = 0; wi < 64; ++wi) {
+        uint32_t* Jw = reinterpret_cast<uint32_t*>(Jr + st * 16);
+        for (int wi = wlo; wi < whi; ++wi) {
             const int ww = wi / CR, rr = wi % CR;
             const uint32_t A = __ldg(row + (2 * ww) * 8 + rr / 2), B = __ldg(row + (2 * ww + 1) * 8 + rr / 2);
-            Jw[4 * ((wi >> 2) ^ (tid & 7)) + (wi & 3)] = __byte_perm(A, B, (rr & 1) ? 0x7632 : 0x5410);
+            Jw[4 * ((wi >> 2) ^ (st & 7)) + (wi & 3)] = __byte_perm(A, B, (rr & 1) ? 0x7632 : 0x5410);
         }
     }
     // remote addresses this thread pushes to (lanes 0 .. CR - 1: CTA `lane`), word wi_own of each buffer
@@ -716,133 +765,121 @@ __global__ void __cluster_dims__(CR, 1, 1) __launch_bounds__(2048 / CR, 1)
     int64_t kcorr_n = __ldg(job.tab.kcorr);
     cl_sync();                                              // barriers initialised and J loaded in every CTA
 
-    for (int t = -1; t < S; ++t) {
-        const int m = t + 1, par = m & 1;
-        if (t >= 0) {
-            const int32_t fourT = fourT_n, twoT = fourT >> 1, qv = q_n;
-            const int32_t corr = step_corr(nlin_prev, kcorr_n, kconst_n);
-            const uint32_t lw = uint32_t(2 * twoT - 1);
-            if (t + 1 < S) {
-                fourT_n = __ldg(job.tab.fourT + t + 1);
-                q_n = __ldg(job.tab.q + t + 1);
-                kconst_n = __ldg(job.tab.kconst + t + 1);
-                kcorr_n = __ldg(job.tab.kcorr + t + 1);
+    if (HELP && !decider) {
+        // helper: the partial D of slot st over words 32 .. 63 of every step, handed over through Dh
+        for (int m = 0; m <= S; ++m) {
+            const int par = m & 1;
+            if (ok && !cl_wait_for(sm_addr(mbar + par), uint32_t((m >> 1) & 1), job.wait_ns)) {
+                ok = false;
+                if (job.err) atomicCAS(job.err, 0, kClusterErrRecv);
             }
-            int32_t hs = s_up ? h : -h;
-            if (hclamp > 0) hs = max(-hclamp, min(hs, hclamp));
-            const int32_t zt = hs * 65536 + (qv + (df ? corr : -corr));
-            fl = valid && (zt - threshold16(u, fourT) < 0);
-            ln = valid && (uint32_t(zt + twoT - 1) < lw);
-            up_new = s_up != fl;
+            Dh[par * CT + st] = cluster_words_d<2, 2>(Jr + st * 16, reinterpret_cast<const uint4*>(FU + par * 64),
+                                                      st & 7);
+            asm volatile("bar.arrive 1, %0;" ::"r"(2 * CT) : "memory");
         }
-        const uint32_t fw = __ballot_sync(FULL, fl), uw = __ballot_sync(FULL, fl && up_new);
-        const uint32_t nlw = __ballot_sync(FULL, ln);
-        if (lane < CR) {
-            const uint32_t bar = dst_mb + 8u * uint32_t(par);
-            st_async2(dst_fu + 8u * 64u * uint32_t(par), fw, uw, bar);
-            st_async1(dst_nl + 4u * 64u * uint32_t(par), uint32_t(__popc(nlw)) | (uint32_t(__popc(fw)) << 16), bar);
-        }
-        const uint32_t my_bar = sm_addr(mbar + par);
-        if (tid == 0)
-            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(my_bar), "r"(kClusterTx)
-                         : "memory");
-        if (t >= 0) {
-            if (fl) s_up = up_new;
-            df = fl;
-            if (t + 1 < S) u = lane_draw(rng, k);            // next step's draw, while the words travel
-        }
-        if (ok && !cl_wait_for(my_bar, uint32_t((m >> 1) & 1), job.wait_ns)) {
-            ok = false;
-            if (job.err) atomicCAS(job.err, 0, kClusterErrRecv);
-        }
-        // n_lin and |F| of step t: each warp sums the 64 packed counts (low half: band, high half: flips)
-        uint32_t pc = NLc[par * 64 + 2 * lane] + NLc[par * 64 + 2 * lane + 1];
-#pragma unroll
-        for (int o = 16; o >= 1; o >>= 1) pc += __shfl_xor_sync(FULL, pc, o);
-        int32_t nf = int32_t(pc >> 16);
-        if (t >= 0) {
-            nlin_prev = int32_t(pc & 0xffffu);
-            if (rank == 0 && tid == 0 && job.trace && job.out_trace) job.out_trace[size_t(c) * S + t] = nlin_prev;
-            if (tid == 0) flips += nf;
-        }
-        // D = sum over the 64 words x_w = F_w & (U_w ^ J_yw) of popc(x_w), through a carry-save (Harley-Seal) tree
-        // over blocks of 16 words: 60 three-input adders and 8 popcounts per thread where a popcount per word took 64
-        const uint4* FUv = reinterpret_cast<const uint4*>(FU + par * 64);   // {F_2q, U_2q, F_2q+1, U_2q+1}
-        const uint4* Jv = Jr + tid * 16;
-        uint32_t ones = 0u, twos = 0u, fours = 0u, eights = 0u;
-        int32_t sixteens = 0;
-#pragma unroll
-        for (int b = 0; b < 4; ++b) {
-            uint32_t x[16];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int ch = 4 * b + q;
-                const uint4 J4 = Jv[ch ^ (tid & 7)], A = FUv[2 * ch], B = FUv[2 * ch + 1];
-                x[4 * q + 0] = A.x & (A.y ^ J4.x);
-                x[4 * q + 1] = A.z & (A.w ^ J4.y);
-                x[4 * q + 2] = B.x & (B.y ^ J4.z);
-                x[4 * q + 3] = B.z & (B.w ^ J4.w);
+    } else {
+        for (int t = -1; t < S; ++t) {
+            const int m = t + 1, par = m & 1;
+            if (t >= 0) {
+                const int32_t fourT = fourT_n, twoT = fourT >> 1, qv = q_n;
+                const int32_t corr = step_corr(nlin_prev, kcorr_n, kconst_n);
+                const uint32_t lw = uint32_t(2 * twoT - 1);
+                if (t + 1 < S) {
+                    fourT_n = __ldg(job.tab.fourT + t + 1);
+                    q_n = __ldg(job.tab.q + t + 1);
+                    kconst_n = __ldg(job.tab.kconst + t + 1);
+                    kcorr_n = __ldg(job.tab.kcorr + t + 1);
+                }
+                int32_t hs = s_up ? h : -h;
+                if (hclamp > 0) hs = max(-hclamp, min(hs, hclamp));
+                const int32_t zt = hs * 65536 + (qv + (df ? corr : -corr));
+                fl = valid && (zt - threshold16(u, fourT) < 0);
+                ln = valid && (uint32_t(zt + twoT - 1) < lw);
+                up_new = s_up != fl;
             }
-            uint32_t tA, tB, fA, fB, eA, eB, s16;
-            csa(ones, tA, ones, x[0], x[1]);
-            csa(ones, tB, ones, x[2], x[3]);
-            csa(twos, fA, twos, tA, tB);
-            csa(ones, tA, ones, x[4], x[5]);
-            csa(ones, tB, ones, x[6], x[7]);
-            csa(twos, fB, twos, tA, tB);
-            csa(fours, eA, fours, fA, fB);
-            csa(ones, tA, ones, x[8], x[9]);
-            csa(ones, tB, ones, x[10], x[11]);
-            csa(twos, fA, twos, tA, tB);
-            csa(ones, tA, ones, x[12], x[13]);
-            csa(ones, tB, ones, x[14], x[15]);
-            csa(twos, fB, twos, tA, tB);
-            csa(fours, eB, fours, fA, fB);
-            csa(eights, s16, eights, eA, eB);
-            sixteens += __popc(s16);
+            const uint32_t fw = __ballot_sync(FULL, fl), uw = __ballot_sync(FULL, fl && up_new);
+            const uint32_t nlw = __ballot_sync(FULL, ln);
+            if (lane < CR) {
+                const uint32_t bar = dst_mb + 8u * uint32_t(par);
+                st_async2(dst_fu + 8u * 64u * uint32_t(par), fw, uw, bar);
+                st_async1(dst_nl + 4u * 64u * uint32_t(par), uint32_t(__popc(nlw)) | (uint32_t(__popc(fw)) << 16), bar);
+            }
+            const uint32_t my_bar = sm_addr(mbar + par);
+            if (tid == 0)
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(my_bar), "r"(kClusterTx)
+                             : "memory");
+            if (t >= 0) {
+                if (fl) s_up = up_new;
+                df = fl;
+                if (t + 1 < S) u = lane_draw(rng, k);            // next step's draw, while the words travel
+            }
+            if (ok && !cl_wait_for(my_bar, uint32_t((m >> 1) & 1), job.wait_ns)) {
+                ok = false;
+                if (job.err) atomicCAS(job.err, 0, kClusterErrRecv);
+            }
+            // n_lin and |F| of step t: each warp sums the 64 packed counts (low half: band, high half: flips)
+            uint32_t pc = NLc[par * 64 + 2 * lane] + NLc[par * 64 + 2 * lane + 1];
+    #pragma unroll
+            for (int o = 16; o >= 1; o >>= 1) pc += __shfl_xor_sync(FULL, pc, o);
+            int32_t nf = int32_t(pc >> 16);
+            if (t >= 0) {
+                nlin_prev = int32_t(pc & 0xffffu);
+                if (rank == 0 && tid == 0 && job.trace && job.out_trace) job.out_trace[size_t(c) * S + t] = nlin_prev;
+                if (tid == 0) flips += nf;
+            }
+            // D: the 64 words at once, or words 0 .. 31 here and 32 .. 63 by the helper (handed over at named barrier 1)
+            const uint4* FUv = reinterpret_cast<const uint4*>(FU + par * 64);   // {F_2q, U_2q, F_2q+1, U_2q+1}
+            const uint4* Jv = Jr + st * 16;
+            int32_t D;
+            if (HELP) {
+                D = cluster_words_d<2, 0>(Jv, FUv, st & 7);
+                asm volatile("bar.sync 1, %0;" ::"r"(2 * CT) : "memory");
+                D += Dh[par * CT + st];
+            } else {
+                D = cluster_words_d<4, 0>(Jv, FUv, st & 7);
+            }
+            // the diagonal: if y itself is in F, its term (J_yy = 0, stored as a 0 bit) was counted as -s'_y
+            if (fl) {
+                nf -= 1;
+                D -= up_new ? 1 : 0;
+            }
+            h += (t >= 0 ? 2 : 1) * (nf - 2 * D);
         }
-        int32_t D = 16 * sixteens + 8 * __popc(eights) + 4 * __popc(fours) + 2 * __popc(twos) + __popc(ones);
-        // the diagonal: if y itself is in F, its term (J_yy = 0, stored as a 0 bit) was counted as -s'_y
-        if (fl) {
-            nf -= 1;
-            D -= up_new ? 1 : 0;
+        // outputs: spins, sum s*h, sum b*s (active slots), flips
+        long long sh = 0, bs = 0;
+        if (valid) {
+            sh = s_up ? h : -h;
+            if (bias) bs = s_up ? bias[slot] : -bias[slot];
+            if (job.out_h) job.out_h[size_t(c) * n + slot] = h;
         }
-        h += (t >= 0 ? 2 : 1) * (nf - 2 * D);
+        const uint32_t sword = __ballot_sync(FULL, s_up);
+        if (lane == 0) {
+            if (LPC == 32) {
+                if (wi_own < nw) job.out_spins[size_t(c) * nw + wi_own] = sword & valid_mask(wi_own, n);
+            } else {
+                // the two 16-bit halves of the exchange word are half words of spin words 2w * 8 + r / 2 and
+                // (2w + 1) * 8 + r / 2; every half of every spin word is written by exactly one CTA
+                uint16_t* out16 = reinterpret_cast<uint16_t*>(job.out_spins + size_t(c) * nw);
+                for (int hh = 0; hh < 2; ++hh) {
+                    const int sw_i = (2 * w + hh) * 8 + int(rank) / 2, half = int(rank) & 1;
+                    if (sw_i < nw)
+                        out16[2 * sw_i + half] = uint16_t(((sword >> (16 * hh)) & 0xffffu) &
+                                                          (valid_mask(sw_i, n) >> (16 * half)));
+                }
+            }
+        }
+        sh = warp_sum64(sh);
+        bs = warp_sum64(bs);
+        if (lane == 0) {
+            s_red[0][w] = sh;
+            s_red[1][w] = bs;
+        }
     }
     if (!ok) {
         // a wait gave up: let pushes still in flight toward this CTA land before the cluster may exit
         const uint64_t t0 = cl_globaltimer();
         while (cl_globaltimer() - t0 < 200000ull) {
         }
-    }
-    // outputs: spins, sum s*h, sum b*s (active slots), flips
-    long long sh = 0, bs = 0;
-    if (valid) {
-        sh = s_up ? h : -h;
-        if (bias) bs = s_up ? bias[slot] : -bias[slot];
-        if (job.out_h) job.out_h[size_t(c) * n + slot] = h;
-    }
-    const uint32_t sword = __ballot_sync(FULL, s_up);
-    if (lane == 0) {
-        if (LPC == 32) {
-            if (wi_own < nw) job.out_spins[size_t(c) * nw + wi_own] = sword & valid_mask(wi_own, n);
-        } else {
-            // the two 16-bit halves of the exchange word are half words of spin words 2w * 8 + r / 2 and
-            // (2w + 1) * 8 + r / 2; every half of every spin word is written by exactly one CTA
-            uint16_t* out16 = reinterpret_cast<uint16_t*>(job.out_spins + size_t(c) * nw);
-            for (int hh = 0; hh < 2; ++hh) {
-                const int sw_i = (2 * w + hh) * 8 + int(rank) / 2, half = int(rank) & 1;
-                if (sw_i < nw)
-                    out16[2 * sw_i + half] = uint16_t(((sword >> (16 * hh)) & 0xffffu) &
-                                                      (valid_mask(sw_i, n) >> (16 * half)));
-            }
-        }
-    }
-    sh = warp_sum64(sh);
-    bs = warp_sum64(bs);
-    if (lane == 0) {
-        s_red[0][w] = sh;
-        s_red[1][w] = bs;
     }
     __syncthreads();
     if (tid == 0) {
@@ -940,7 +977,7 @@ template <int CR>
 int cluster_launch_t(const PlainJob& job, cudaStream_t st) {
     cudaError_t e = cluster_prepare<CR>();
     if (e != cudaSuccess) return int(e);
-    plain_cluster_kernel<CR><<<job.ntrials * CR, 2048 / CR, kClusterSmem, st>>>(job);
+    plain_cluster_kernel<CR><<<job.ntrials * CR, cluster_threads(CR), kClusterSmem, st>>>(job);
     return int(cudaGetLastError());
 }
 template <int CR>
@@ -956,7 +993,7 @@ int cluster_max_active_t(int* out) {
     cfg.attrs = at;
     cfg.numAttrs = 1;
     cfg.gridDim = dim3(CR);
-    cfg.blockDim = dim3(2048 / CR);
+    cfg.blockDim = dim3(cluster_threads(CR));
     cfg.dynamicSmemBytes = kClusterSmem;
     return int(cudaOccupancyMaxActiveClusters(out, plain_cluster_kernel<CR>, &cfg));
 }
