@@ -646,12 +646,13 @@ __device__ __forceinline__ uint32_t lane_draw(Xoshiro& rng, int k) {
 // D of one slot over the 16 NB words of blocks B0 .. B0 + NB - 1 (block b: words 16b .. 16b + 15): the sum of
 // popc(x_w), x_w = F_w & (U_w ^ J_yw), through a carry-save (Harley-Seal) tree -- 15 three-input adders and one
 // popcount per block of 16 words, 4 more popcounts at the end, where a popcount per word took 16 per block.
-template <int NB, int B0>
-__device__ __forceinline__ int32_t cluster_words_d(const uint4* Jv, const uint4* FUv, int swz) {
+template <int NB>
+__device__ __forceinline__ int32_t cluster_words_d(const uint4* Jv, const uint4* FUv, int swz, int B0) {
     uint32_t ones = 0u, twos = 0u, fours = 0u, eights = 0u;
     int32_t sixteens = 0;
 #pragma unroll
-    for (int b = B0; b < B0 + NB; ++b) {
+    for (int bb = 0; bb < NB; ++bb) {
+        const int b = B0 + bb;
         uint32_t x[16];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
@@ -683,8 +684,11 @@ __device__ __forceinline__ int32_t cluster_words_d(const uint4* Jv, const uint4*
     return 16 * sixteens + 8 * __popc(eights) + 4 * __popc(fours) + 2 * __popc(twos) + __popc(ones);
 }
 
-// Threads per CTA of the cluster kernel: one deciding thread per owned slot, and with 16 CTAs an update helper too.
-__host__ __device__ constexpr int cluster_threads(int cr) { return (2048 / cr) * (cr == 16 ? 2 : 1); }
+// Update helpers per owned slot and threads per CTA of the cluster kernel. With 16 CTAs one helper sums words
+// 32 .. 63 of each slot's update (1.062 ms per 1000 steps for one anneal; three helpers of 16 words each: 1.092; none:
+// 1.13); with 8 CTAs the SM's ALU is already the bound and a helper gained nothing.
+__host__ __device__ constexpr int cluster_helpers(int cr) { return cr == 16 ? 1 : 0; }
+__host__ __device__ constexpr int cluster_threads(int cr) { return (2048 / cr) * (1 + cluster_helpers(cr)); }
 
 template <int CR>
 __global__ void __cluster_dims__(CR, 1, 1) __launch_bounds__(cluster_threads(CR), 1)
@@ -692,7 +696,9 @@ __global__ void __cluster_dims__(CR, 1, 1) __launch_bounds__(cluster_threads(CR)
     constexpr int NWJ = 64;
     constexpr int CT = 2048 / CR;                 // owned slots (deciding threads) per CTA
     constexpr int LPC = 256 / CR;                 // RNG lanes per CTA
-    constexpr bool HELP = CR == 16;               // a helper thread per slot sums half of its update's words
+    constexpr int NH = cluster_helpers(CR);       // helper threads per slot, each summing part of its update
+    constexpr bool HELP = NH > 0;
+    constexpr int BPT = 4 / (NH + 1);             // 16-word blocks of the update per thread
     static_assert((CR == 8 || CR == 16) && (CT / 32) * CR == 64, "64 exchange words per step");
     extern __shared__ __align__(16) uint8_t smem_raw[];
     // J row of owned slot t in exchange-word order: 16 chunks of 16 bytes, chunk c at position c ^ (t & 7)
@@ -700,15 +706,15 @@ __global__ void __cluster_dims__(CR, 1, 1) __launch_bounds__(cluster_threads(CR)
     uint4* Jr = reinterpret_cast<uint4*>(smem_raw);                     // [CT][16]
     uint2* FU = reinterpret_cast<uint2*>(Jr + CT * 16);                 // [2 parities][64 words]: flip, new spin +1
     uint32_t* NLc = reinterpret_cast<uint32_t*>(FU + 2 * 64);            // [2][64]: band count | flip count << 16
-    int32_t* Dh = reinterpret_cast<int32_t*>(NLc + 2 * 64);              // [2][CT]: helpers' partial D (HELP)
-    uint64_t* mbar = reinterpret_cast<uint64_t*>(Dh + 2 * CT);           // [2]: exchange of each parity
+    int32_t* Dh = reinterpret_cast<int32_t*>(NLc + 2 * 64);              // [2][NH][CT]: helpers' partial D
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(Dh + 2 * NH * CT);      // [2]: exchange of each parity
     __shared__ long long s_red[2][CT / 32];
     __shared__ long long s_part[CR][3];                     // rank 0: every rank's sum of s*h, of b*s and flips
 
     // warp w covers rounds w * 32 / LPC ..; its lane holds round k of RNG lane l of this CTA's LPC lanes. Thread
-    // st + CT (HELP) is the update helper of slot st.
-    const int tid = threadIdx.x, st = tid % CT, lane = st & 31, w = st >> 5;
-    const bool decider = tid < CT;
+    // st + j CT (j = 1 .. NH) is update helper j of slot st.
+    const int tid = threadIdx.x, st = tid % CT, lane = st & 31, w = st >> 5, role = tid / CT;
+    const bool decider = role == 0;
     const int k = w * (32 / LPC) + lane / LPC;
     const uint32_t rank = cl_rank();
     const int c = int(cl_id());                             // anneal index within the launch
@@ -725,8 +731,8 @@ __global__ void __cluster_dims__(CR, 1, 1) __launch_bounds__(cluster_threads(CR)
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(sm_addr(mbar + q)) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    // with a helper, the deciding thread loads words 0 .. 31 of its slot's row and the helper words 32 .. 63
-    const int wlo = HELP ? 32 * (tid / CT) : 0, whi = HELP ? wlo + 32 : 64;
+    // each thread of a slot loads the words of the row it sums: words 16 BPT role .. 16 BPT (role + 1) - 1
+    const int wlo = 16 * BPT * role, whi = wlo + 16 * BPT;        // (role is 0 or 1 with one helper)
     if (LPC == 32) {
         // exchange word w * 8 + r is spin word w * 8 + r: the row as stored
         const uint4* row = reinterpret_cast<const uint4*>(job.planes + size_t(slot) * NWJ);
@@ -766,16 +772,16 @@ __global__ void __cluster_dims__(CR, 1, 1) __launch_bounds__(cluster_threads(CR)
     cl_sync();                                              // barriers initialised and J loaded in every CTA
 
     if (HELP && !decider) {
-        // helper: the partial D of slot st over words 32 .. 63 of every step, handed over through Dh
+        // helper `role`: the partial D of slot st over its blocks of every step, handed over through Dh
         for (int m = 0; m <= S; ++m) {
             const int par = m & 1;
             if (ok && !cl_wait_for(sm_addr(mbar + par), uint32_t((m >> 1) & 1), job.wait_ns)) {
                 ok = false;
                 if (job.err) atomicCAS(job.err, 0, kClusterErrRecv);
             }
-            Dh[par * CT + st] = cluster_words_d<2, 2>(Jr + st * 16, reinterpret_cast<const uint4*>(FU + par * 64),
-                                                      st & 7);
-            asm volatile("bar.arrive 1, %0;" ::"r"(2 * CT) : "memory");
+            Dh[(par * NH + role - 1) * CT + st] = cluster_words_d<BPT>(
+                Jr + st * 16, reinterpret_cast<const uint4*>(FU + par * 64), st & 7, NH == 1 ? BPT : BPT * role);
+            asm volatile("bar.arrive 1, %0;" ::"r"(cluster_threads(CR)) : "memory");
         }
     } else {
         for (int t = -1; t < S; ++t) {
@@ -827,16 +833,17 @@ __global__ void __cluster_dims__(CR, 1, 1) __launch_bounds__(cluster_threads(CR)
                 if (rank == 0 && tid == 0 && job.trace && job.out_trace) job.out_trace[size_t(c) * S + t] = nlin_prev;
                 if (tid == 0) flips += nf;
             }
-            // D: the 64 words at once, or words 0 .. 31 here and 32 .. 63 by the helper (handed over at named barrier 1)
+            // D: the 64 words at once, or the first blocks here and the rest by the helpers (handed over at barrier 1)
             const uint4* FUv = reinterpret_cast<const uint4*>(FU + par * 64);   // {F_2q, U_2q, F_2q+1, U_2q+1}
             const uint4* Jv = Jr + st * 16;
             int32_t D;
             if (HELP) {
-                D = cluster_words_d<2, 0>(Jv, FUv, st & 7);
-                asm volatile("bar.sync 1, %0;" ::"r"(2 * CT) : "memory");
-                D += Dh[par * CT + st];
+                D = cluster_words_d<BPT>(Jv, FUv, st & 7, 0);
+                asm volatile("bar.sync 1, %0;" ::"r"(cluster_threads(CR)) : "memory");
+#pragma unroll
+                for (int j = 0; j < NH; ++j) D += Dh[(par * NH + j) * CT + st];
             } else {
-                D = cluster_words_d<4, 0>(Jv, FUv, st & 7);
+                D = cluster_words_d<4>(Jv, FUv, st & 7, 0);
             }
             // the diagonal: if y itself is in F, its term (J_yy = 0, stored as a 0 bit) was counted as -s'_y
             if (fl) {
