@@ -61,6 +61,9 @@ def test_waves_and_availability():
     one = A.auto_estimate(2000, 1, 15, 1000, 0.3, w, fp4=True)
     two = A.auto_estimate(2000, 1, 16, 1000, 0.3, w, fp4=True)
     assert two["cluster"] == pytest.approx(2 * one["cluster"]) and two["plain"] == one["plain"]
+    # up to half an 8-CTA wave (7 anneals here) runs as one wave of 16-CTA clusters, at its own per-step cost
+    small = [A.auto_estimate(2000, 1, c, 1000, 0.3, w, fp4=True)["cluster"] for c in (1, 7, 8)]
+    assert small[0] == small[1] < small[2] == pytest.approx(one["cluster"])
     assert A.auto_estimate(2000, 1, 149, 1000, 0.3, w, fp4=True)["plain"] == pytest.approx(2 * one["plain"])
     sparse = A.auto_estimate(5000, 0, 64, 100, 0.1, {"plain": 148})
     assert sparse["pick"] == "plain" and set(sparse) == {"plain", "pick"}
