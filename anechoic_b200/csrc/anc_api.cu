@@ -137,6 +137,10 @@ struct anc_instance {
     DevBuf<uint32_t> planes;
     DevBuf<int32_t> row_ptr;
     DevBuf<uint32_t> adj;
+    // the CSR rows with 16-bit edges, two per word (every J_xy = +-1 and n < 32767; else empty): half the fetches
+    DevBuf<int32_t> row_ptr16;
+    DevBuf<uint32_t> adj16;
+    bool csr16 = false;
     DevBuf<int32_t> d_bias;
     std::vector<int8_t> dense;                    // host copy of dense couplings (tensor engine packs lazily)
     anc::TensorInstance tensor;                   // tensor-engine operands (built on first use)
@@ -305,8 +309,9 @@ anc::PlainJob make_job(anc_instance* I, anc_tables* tb, uint64_t seed, uint32_t 
     j.nwj = I->nwj;
     j.K = I->K;
     j.planes = I->planes.p;
-    j.row_ptr = I->row_ptr.p;
-    j.adj = I->adj.p;
+    j.row_ptr = I->csr16 ? I->row_ptr16.p : I->row_ptr.p;
+    j.adj = I->csr16 ? I->adj16.p : I->adj.p;
+    j.csr16 = I->csr16 ? 1 : 0;
     j.bias = I->bias.empty() ? nullptr : I->d_bias.p;
     j.tab = dev_tables(tb);
     j.seed = seed;
@@ -561,6 +566,17 @@ int run_device_impl(anc_instance* I, anc_tables* tb, uint64_t seed, uint32_t off
         if (rc) return cuda_fail(cudaError_t(rc), "cluster engine launch");
         g_last_kernel = ANC_KERNEL_PLAIN_CLUSTER;
         return ANC_OK;
+    }
+    if (I->K == 0 && o && o->kernel_variant > 0) {
+        // CSR edge format: 1 = 32-bit edges, 2 = 16-bit edges (unit weights and n < 32767 only)
+        if (o->kernel_variant > 2 || (o->kernel_variant == 2 && !I->csr16))
+            return fail(ANC_EINVAL, "kernel_variant %d: CSR instances take 1 (32-bit edges) or, with unit weights "
+                                    "and n < 32767, 2 (16-bit edges)", o->kernel_variant);
+        if (o->kernel_variant == 1) {
+            job.row_ptr = I->row_ptr.p;
+            job.adj = I->adj.p;
+            job.csr16 = 0;
+        }
     }
     const int forced = o ? (I->K == 0 ? o->sparse_variant : o->kernel_variant) : 0;
     rc = launch_plain_single(I, job, st, forced > 0 ? forced - 1 : -1);
@@ -1000,6 +1016,28 @@ int anc_instance_create_csr(int n, const int32_t* row_ptr, const int32_t* col, c
     if (e == cudaSuccess) e = I->adj.ensure(std::max<int64_t>(nnz, 1));
     if (e == cudaSuccess && nnz) e = cudaMemcpy(I->adj.p, adj.data(), size_t(nnz) * 4, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return cuda_fail(e, "upload CSR");
+    // unit weights and n < 32767: the same rows with 16-bit edges y | [J = -1] << 15, two per word, each row padded
+    // to a whole word with the skip edge 0x7fff; the CSR pass then fetches half the words
+    bool unit = n < 0x7fff;
+    for (int64_t k = 0; unit && k < nnz; ++k) unit = val[k] == 1 || val[k] == -1;
+    if (unit) {
+        std::vector<int32_t> rp16(size_t(n) + 1, 0);
+        for (int x = 0; x < n; ++x) rp16[x + 1] = rp16[x] + (row_ptr[x + 1] - row_ptr[x] + 1) / 2;
+        std::vector<uint32_t> a16(std::max<int32_t>(rp16[n], 1), 0x7fff7fffu);
+        for (int x = 0; x < n; ++x)
+            for (int k = row_ptr[x]; k < row_ptr[x + 1]; ++k) {
+                const int i = k - row_ptr[x];
+                const uint32_t ed = uint32_t(col[k]) | (val[k] < 0 ? 0x8000u : 0u);
+                uint32_t& wd = a16[size_t(rp16[x]) + i / 2];
+                wd = (i & 1) ? ((wd & 0xffffu) | (ed << 16)) : ((wd & 0xffff0000u) | ed);
+            }
+        e = I->row_ptr16.ensure(size_t(n) + 1);
+        if (e == cudaSuccess) e = cudaMemcpy(I->row_ptr16.p, rp16.data(), (size_t(n) + 1) * 4, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = I->adj16.ensure(a16.size());
+        if (e == cudaSuccess) e = cudaMemcpy(I->adj16.p, a16.data(), a16.size() * 4, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return cuda_fail(e, "upload 16-bit CSR");
+        I->csr16 = true;
+    }
     *out = I.release();
     return ANC_OK;
 }

@@ -32,8 +32,10 @@ struct PlainJob {
     // instance
     int n, np, nw, nwj, K;             // K = 0: sparse CSR
     const uint32_t* planes;            // dense: [max(K,1)][np][nwj]
-    const int32_t* row_ptr;            // sparse: [n + 1]
-    const uint32_t* adj;               // sparse: (y << 8) | uint8(J_xy)
+    const int32_t* row_ptr;            // sparse: [n + 1] (csr16: in words of two edges)
+    const uint32_t* adj;               // sparse: (y << 8) | uint8(J_xy); csr16: two 16-bit edges per word
+    int csr16;                         // sparse, every J_xy = +-1 and n < 32767: edge = y | [J_xy = -1] << 15, rows
+                                       // padded to whole words with the skip edge 0x7fff
     const int32_t* bias;               // [n] or null
     DevTables tab;
     uint64_t seed;

@@ -332,7 +332,19 @@ __device__ __forceinline__ int sparse_lanes_log2(int nnz, int n) {
     return lg;
 }
 
-template <int kSparseBatch, int kSparseEdges>
+// One word of edges: (y << 8) | uint8(J), or with E16 two edges y | [J = -1] << 15 (0x7fff: no edge).
+template <bool E16>
+__device__ __forceinline__ void sparse_apply(uint32_t v, int32_t m, int32_t* h) {
+    if (E16) {
+        const uint32_t lo = v & 0xffffu, hi = v >> 16;
+        if ((lo & 0x7fffu) != 0x7fffu) atomicAdd(&h[lo & 0x7fffu], (lo >> 15) ? -m : m);
+        if ((hi & 0x7fffu) != 0x7fffu) atomicAdd(&h[hi & 0x7fffu], (hi >> 15) ? -m : m);
+    } else {
+        atomicAdd(&h[v >> 8], m * int32_t(int8_t(v & 0xffu)));
+    }
+}
+
+template <int kSparseBatch, int kSparseEdges, bool E16 = false>
 __device__ __forceinline__ void sparse_pass(const int32_t* __restrict__ row_ptr, const uint32_t* __restrict__ adj,
                                             const uint32_t* flist, int nf, int lg, int32_t* h, int mult) {
     const int G = 1 << lg, sub = threadIdx.x & (G - 1), NG = T >> lg;
@@ -362,11 +374,8 @@ __device__ __forceinline__ void sparse_pass(const int32_t* __restrict__ row_ptr,
         for (int b = 0; b < kSparseBatch; ++b) {
 #pragma unroll
             for (int e = 0; e < kSparseEdges; ++e)
-                if (k0[b] + e * G < k1[b]) atomicAdd(&h[a[b][e] >> 8], m[b] * int32_t(int8_t(a[b][e] & 0xffu)));
-            for (int k = k0[b] + kSparseEdges * G; k < k1[b]; k += G) {
-                const uint32_t v = __ldg(adj + k);
-                atomicAdd(&h[v >> 8], m[b] * int32_t(int8_t(v & 0xffu)));
-            }
+                if (k0[b] + e * G < k1[b]) sparse_apply<E16>(a[b][e], m[b], h);
+            for (int k = k0[b] + kSparseEdges * G; k < k1[b]; k += G) sparse_apply<E16>(__ldg(adj + k), m[b], h);
         }
     }
 }
@@ -462,7 +471,8 @@ __global__ void __launch_bounds__(T, 1) plain_kernel(const __grid_constant__ Pla
         const int nf0 = s_nf;
         const int sparse_lg = SPARSE ? sparse_lanes_log2<SE>(__ldg(job.row_ptr + n), n) : 0;
         if (SPARSE) {
-            sparse_pass<SB, SE>(job.row_ptr, job.adj, flist, nf0, sparse_lg, h, 1);
+            if (job.csr16) sparse_pass<SB, SE, true>(job.row_ptr, job.adj, flist, nf0, sparse_lg, h, 1);
+            else sparse_pass<SB, SE>(job.row_ptr, job.adj, flist, nf0, sparse_lg, h, 1);
         } else {
             dense_pass<K, P, STREAM, DV>(planes, plane_stride, nwj, nf0, flist, comb, res, h, n, 1);
             if (!STREAM) {
@@ -512,7 +522,8 @@ __global__ void __launch_bounds__(T, 1) plain_kernel(const __grid_constant__ Pla
             nlin_prev = nlin;
             if (nf > 0) {
                 if (SPARSE) {
-                    sparse_pass<SB, SE>(job.row_ptr, job.adj, flist, nf, sparse_lg, h, 2);
+                    if (job.csr16) sparse_pass<SB, SE, true>(job.row_ptr, job.adj, flist, nf, sparse_lg, h, 2);
+                    else sparse_pass<SB, SE>(job.row_ptr, job.adj, flist, nf, sparse_lg, h, 2);
                 } else {
                     dense_pass<K, P, STREAM, DV>(planes, plane_stride, nwj, nf, flist, comb, res, h, n, 2);
                     if (!STREAM) {

@@ -120,7 +120,9 @@ typedef struct {
     int kernel_variant; /* dense instances on the plain engine and the tensor engine's fp4 kernel: 0 = the variant the
                            run-time tuner chose (anc_kernel_tuning; the default variant before any tuning), v + 1 =
                            force variant v. Cluster engine: 0 = 16 CTAs per anneal when the anneals fit one wave of
-                           16-CTA clusters, else 8; 1 = 8 CTAs; 2 = 16 CTAs */
+                           16-CTA clusters, else 8; 1 = 8 CTAs; 2 = 16 CTAs. CSR instances on the plain engine: the
+                           edge format -- 0 = 16-bit edges (two per fetched word) when every weight is +-1 and
+                           n < 32767, else 32-bit; 1 = 32-bit; 2 = 16-bit (EINVAL when not eligible) */
 } anc_run_opts;
 
 /* No counterpart in the reference (its kernel geometry is fixed per build by flags, sca_gpu_bias.cu:637-644). The

@@ -109,3 +109,57 @@ def test_sparse_tuner_variants_agree_and_pick_is_recorded(cuda, oracle):
     L.anc_sparse_tuning(dev._h, C.byref(v), us)
     assert 0 <= v.value < 4 and all(us[k] > 0 for k in range(4))
     assert us[v.value] == min(us[k] for k in range(4))
+
+
+def test_csr_edge_formats_agree(cuda, oracle):
+    """CSR instances with unit weights and n < 32767 keep their rows also as 16-bit edges, two per fetched word (the
+    default); anc_run_opts.kernel_variant forces 32-bit (1) or 16-bit (2) edges. Both give the golden model's bits, on
+    rows of odd and even length; an instance with a weight of magnitude above 1 refuses the 16-bit form."""
+    import ctypes as C
+    import numpy as np
+    from anechoic_b200 import _lib
+    L = _lib.load()
+    sc = dict(S=80, t0=6.0, t1=0.5, q=1.5, kappa=2.0, ramp=True)
+    tb = A.Tables.from_schedule(A.Schedule(**sc))
+    inst = I.random_graph(3001, 9000, True, 4242, bmax=2)
+    assert inst.stats()["maxabs"] == 1
+    dev = A.DeviceInstance(inst)
+    ref = oracle.run_batch(inst.n, oracle.tables(**sc), 5, 70, 6, csr=inst.to_csr(), bias=inst.bias)
+
+    def run(variant):
+        o = _lib.opts("plain")
+        o.kernel_variant = variant
+        r = A.RunResult(n=inst.n, trial_offset=70, spins=np.zeros((6, A.spin_words(inst.n)), np.uint64),
+                        sum_sh=np.zeros(6, np.int64), sum_bs=np.zeros(6, np.int64), flips=np.zeros(6, np.int64),
+                        trace=np.zeros((6, sc["S"]), np.int32))
+        rc = L.anc_run(dev._h, tb._h, 5, 70, 6, C.byref(o), r.spins.ctypes.data, r.sum_sh.ctypes.data,
+                       r.sum_bs.ctypes.data, r.flips.ctypes.data, r.trace.ctypes.data)
+        return rc, r
+
+    for variant in (0, 1, 2):
+        rc, r = run(variant)
+        assert rc == 0, L.anc_last_error().decode()
+        for c in range(6):
+            assert_same(r, {k: v[c] for k, v in ref.items()}, c, f"edge format {variant} chain {c}")
+    assert run(3)[0] == -1
+    # a weight of 2: only the 32-bit form
+    rp, col, val0 = (np.ascontiguousarray(a, t) for a, t in zip(inst.to_csr(), (np.int32, np.int32, np.int8)))
+    # keep J symmetric: double both directions of every edge whose (min, max) pair hashes to 0 mod 7
+    rows = np.repeat(np.arange(inst.n), np.diff(rp))
+    lo, hi = np.minimum(rows, col), np.maximum(rows, col)
+    val = np.ascontiguousarray(np.where((lo * 31 + hi) % 7 == 0, 2 * val0, val0), np.int8)
+    h = C.c_void_p()
+    _lib.check(L.anc_instance_create_csr(inst.n, rp.ctypes.data, col.ctypes.data, val.ctypes.data, None, C.byref(h)))
+    try:
+        o = _lib.opts("plain")
+        o.kernel_variant = 2
+        sp = np.zeros((1, A.spin_words(inst.n)), np.uint64)
+        sh = np.zeros(1, np.int64)
+        assert L.anc_run(h, tb._h, 5, 0, 1, C.byref(o), sp.ctypes.data, sh.ctypes.data, None, None, None) == -1
+        assert "16-bit edges" in L.anc_last_error().decode()
+        o.kernel_variant = 0
+        _lib.check(L.anc_run(h, tb._h, 5, 0, 1, C.byref(o), sp.ctypes.data, sh.ctypes.data, None, None, None))
+        ref2 = oracle.run_batch(inst.n, oracle.tables(**sc), 5, 0, 1, csr=(rp, col, val))
+        assert np.array_equal(sp[0], ref2["spins"][0]) and int(sh[0]) == int(ref2["sum_sh"][0])
+    finally:
+        L.anc_instance_destroy(h)
