@@ -541,7 +541,7 @@ EXTRA_DESC = {
 
 
 def run_extra(name: str, args, steps: int = 3, warmup: int = 1, target=None) -> dict:
-    """One of the other BASELINE workloads, timed on the device (the library's CUDA events around each launch, or
+    """One of the other benchmark workloads, timed on the device (the library's CUDA events around each launch, or
     events on the stream), outside the headline's timed region, with its own roofline. meanfield also tunes the
     schedule on the relaxation and judges the tuned and the default schedule on the exact engine (1024 anneals each,
     same trial ids): p at the default schedule's median cut and, when given, at the headline's target cut."""
