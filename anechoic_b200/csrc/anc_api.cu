@@ -81,10 +81,10 @@ int pad_np(int n) { return std::max(2048, ((n + 255) / 256) * 256); }
 //                                               flip rewrites n fields from one row of bit planes (K planes);
 //                                               a_1 = 3.4, a_2 = 5.1, a_4 = 10.2, c_1 = 5.4e-6, c_2 = 1.6e-5,
 //                                               c_4 = 3.3e-5 (least squares in log time over the one-wave launches)
-//   cluster  1.00 when the anneals fit one wave of 16-CTA clusters (taken as half the 8-CTA wave: 7 here), else
-//            1.30 per wave of 8-CTA clusters (1-bit couplings, NP = 2048: every thread sums popcounts over all 64
-//            flip words whatever flipped, so the step costs the same at any phi; measured 0.994 - 0.998 for 1 - 7
-//            anneals on 16 CTAs, 1.25 - 1.35 per wave of up to 15 on 8)
+//   cluster  0.86 when the anneals fit one wave of 16-CTA clusters (taken as half the 8-CTA wave: 7 here), else
+//            1.18 per wave of 8-CTA clusters (1-bit couplings, NP = 2048: every thread sums popcounts over all 64
+//            flip words whatever flipped, so the step costs the same at any phi; measured 0.852 - 0.859 for 1 - 7
+//            anneals on 16 CTAs, 1.18 - 1.19 per wave of up to 15 on 8)
 //   tensor   a constant per kernel: the MMA chain and the decisions cost the same whatever flips: fp4 8.1 (8.3 with
 //            more than one replica group per wave), int8 23.3 at NP = 2048, 21.7 and 28.3 at NP = 3072 and 4096,
 //            streaming 99.5 (measured 99.5 at NP = 10240 and 98 at NP = 16384: bound by its step latency, not by
@@ -118,8 +118,8 @@ int estimate_engines(int n, int K, int nchains, int S, double phi, bool fp4, con
         us[ANC_ENGINE_TENSOR] = waves(ANC_ENGINE_TENSOR) * S * tensor_step_us(n, fp4, (groups + 127) / 128);
     }
     if (per_wave[ANC_ENGINE_CLUSTER] > 0)
-        us[ANC_ENGINE_CLUSTER] = nchains <= per_wave[ANC_ENGINE_CLUSTER] / 2 ? S * 1.00
-                                                                             : waves(ANC_ENGINE_CLUSTER) * S * 1.30;
+        us[ANC_ENGINE_CLUSTER] = nchains <= per_wave[ANC_ENGINE_CLUSTER] / 2 ? S * 0.86
+                                                                             : waves(ANC_ENGINE_CLUSTER) * S * 1.18;
     int best = ANC_ENGINE_PLAIN;
     for (int e : {ANC_ENGINE_PLAIN, ANC_ENGINE_TENSOR, ANC_ENGINE_CLUSTER})
         if (us[e] >= 0 && (us[best] < 0 || us[e] < us[best])) best = e;

@@ -569,9 +569,9 @@ __global__ void __launch_bounds__(T, 1) plain_kernel(const __grid_constant__ Pla
 // Per step m (m = 0: the initial pass; m = t + 1 for step t), with p = m & 1:
 //   1. every thread decides its slot; warp k's ballots give flip word wi = k*8 + r (bit l = slot k*256 + 32r + l),
 //      the matching word of new spins +1 among the flipped, and the warp's counts of band slots and flips;
-//   2. lanes 0 .. 7 of warp k push the warp's word pair and its packed counts to CTA `lane` with st.async (12 bytes
-//      into that CTA's exchange buffer p, completing on its mbarrier p): every CTA receives 64 x 12 = 768 bytes per
-//      step, and its thread 0 arrives on its own mbarrier p expecting them;
+//   2. lanes 0 .. 7 of warp k push the warp's word pair and its packed counts to CTA `lane` with one 16-byte
+//      st.async (record wi of that CTA's exchange buffer p, completing on its mbarrier p): every CTA receives
+//      64 x 16 = 1024 bytes per step, and its thread 0 arrives on its own mbarrier p expecting them;
 //   3. every thread makes its next draws, then waits (bounded) for mbarrier p's phase (cluster-scope acquire: the
 //      remote stores are visible after it); each warp sums the 64 packed counts itself (n_lin for the next
 //      correction, |F|), so no CTA barrier is needed;
@@ -584,7 +584,7 @@ __global__ void __launch_bounds__(T, 1) plain_kernel(const __grid_constant__ Pla
 // CTA's words of step m + 1, and a CTA sends those only after each of its warps has finished reading buffer p of step
 // m (the words sent depend on the fields those reads updated); so the pushes of step m + 2 cannot overtake the reads
 // of step m, nor count toward mbarrier p's phase of step m.
-constexpr uint32_t kClusterTx = 64 * 12;  // exchange bytes a CTA receives per step
+constexpr uint32_t kClusterTx = 64 * 16;  // exchange bytes a CTA receives per step
 constexpr size_t kClusterSmem = 116 * 1024;   // above half an SM's shared memory: one CTA per SM
 
 __device__ __forceinline__ uint32_t sm_addr(const void* p) { return uint32_t(__cvta_generic_to_shared(p)); }
@@ -612,14 +612,10 @@ __device__ __forceinline__ uint64_t cl_globaltimer() {
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
 }
-// remote store of two words / one word into another CTA's shared memory, completing on its mbarrier
-__device__ __forceinline__ void st_async2(uint32_t addr, uint32_t a, uint32_t b, uint32_t bar) {
-    asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v2.b32 [%0], {%1, %2}, [%3];"
-                 ::"r"(addr), "r"(a), "r"(b), "r"(bar) : "memory");
-}
-__device__ __forceinline__ void st_async1(uint32_t addr, uint32_t a, uint32_t bar) {
-    asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.b32 [%0], %1, [%2];"
-                 ::"r"(addr), "r"(a), "r"(bar) : "memory");
+// remote store of one 16-byte record into another CTA's shared memory, completing on its mbarrier
+__device__ __forceinline__ void st_async4(uint32_t addr, uint32_t a, uint32_t b, uint32_t c, uint32_t d, uint32_t bar) {
+    asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v4.b32 [%0], {%1, %2, %3, %4}, [%5];"
+                 ::"r"(addr), "r"(a), "r"(b), "r"(c), "r"(d), "r"(bar) : "memory");
 }
 __device__ __forceinline__ bool cl_try_wait(uint32_t bar, uint32_t parity) {
     uint32_t ok;
@@ -658,7 +654,7 @@ __device__ __forceinline__ uint32_t lane_draw(Xoshiro& rng, int k) {
 // popc(x_w), x_w = F_w & (U_w ^ J_yw), through a carry-save (Harley-Seal) tree -- 15 three-input adders and one
 // popcount per block of 16 words, 4 more popcounts at the end, where a popcount per word took 16 per block.
 template <int NB>
-__device__ __forceinline__ int32_t cluster_words_d(const uint4* Jv, const uint4* FUv, int swz, int B0) {
+__device__ __forceinline__ int32_t cluster_words_d(const uint4* Jv, const uint4* FXv, int swz, int B0) {
     uint32_t ones = 0u, twos = 0u, fours = 0u, eights = 0u;
     int32_t sixteens = 0;
 #pragma unroll
@@ -668,11 +664,12 @@ __device__ __forceinline__ int32_t cluster_words_d(const uint4* Jv, const uint4*
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const int ch = 4 * b + q;               // 16-byte chunk of the J row: words 4ch .. 4ch+3
-            const uint4 J4 = Jv[ch ^ swz], A = FUv[2 * ch], B = FUv[2 * ch + 1];
+            const uint4 J4 = Jv[ch ^ swz], A = FXv[4 * ch], B = FXv[4 * ch + 1], C = FXv[4 * ch + 2],
+                        E = FXv[4 * ch + 3];
             x[4 * q + 0] = A.x & (A.y ^ J4.x);
-            x[4 * q + 1] = A.z & (A.w ^ J4.y);
-            x[4 * q + 2] = B.x & (B.y ^ J4.z);
-            x[4 * q + 3] = B.z & (B.w ^ J4.w);
+            x[4 * q + 1] = B.x & (B.y ^ J4.y);
+            x[4 * q + 2] = C.x & (C.y ^ J4.z);
+            x[4 * q + 3] = E.x & (E.y ^ J4.w);
         }
         uint32_t tA, tB, fA, fB, eA, eB, s16;
         csa(ones, tA, ones, x[0], x[1]);
@@ -696,8 +693,9 @@ __device__ __forceinline__ int32_t cluster_words_d(const uint4* Jv, const uint4*
 }
 
 // Update helpers per owned slot and threads per CTA of the cluster kernel. With 16 CTAs one helper sums words
-// 32 .. 63 of each slot's update (1.062 ms per 1000 steps for one anneal, 0.994 with the packed counts summed by one
-// warp reduction; three helpers of 16 words each: 1.092; none: 1.13); with 8 CTAs the SM's ALU is already the bound and a helper gained nothing.
+// 32 .. 63 of each slot's update (1.062 ms per 1000 steps for one anneal with two pushes per word, where three helpers
+// of 16 words each took 1.092 and none 1.13; 0.994 with the packed counts summed by one warp reduction; 0.870 with one
+// 16-byte push per word, 0.855 with the counts read at a 16-byte stride); with 8 CTAs the SM's ALU is already the bound and a helper gained nothing.
 __host__ __device__ constexpr int cluster_helpers(int cr) { return cr == 16 ? 1 : 0; }
 __host__ __device__ constexpr int cluster_threads(int cr) { return (2048 / cr) * (1 + cluster_helpers(cr)); }
 
@@ -715,9 +713,9 @@ __global__ void __cluster_dims__(CR, 1, 1) __launch_bounds__(cluster_threads(CR)
     // J row of owned slot t in exchange-word order: 16 chunks of 16 bytes, chunk c at position c ^ (t & 7)
     // (conflict-free 16-byte loads)
     uint4* Jr = reinterpret_cast<uint4*>(smem_raw);                     // [CT][16]
-    uint2* FU = reinterpret_cast<uint2*>(Jr + CT * 16);                 // [2 parities][64 words]: flip, new spin +1
-    uint32_t* NLc = reinterpret_cast<uint32_t*>(FU + 2 * 64);            // [2][64]: band count | flip count << 16
-    int32_t* Dh = reinterpret_cast<int32_t*>(NLc + 2 * 64);              // [2][NH][CT]: helpers' partial D
+    // [2 parities][64 words] of {flip, new spin +1, band count | flip count << 16, 0}: one 16-byte push per word
+    uint4* FX = Jr + CT * 16;
+    int32_t* Dh = reinterpret_cast<int32_t*>(FX + 2 * 64);               // [2][NH][CT]: helpers' partial D
     uint64_t* mbar = reinterpret_cast<uint64_t*>(Dh + 2 * NH * CT);      // [2]: exchange of each parity
     __shared__ long long s_red[2][CT / 32];
     __shared__ long long s_part[CR][3];                     // rank 0: every rank's sum of s*h, of b*s and flips
@@ -761,8 +759,7 @@ __global__ void __cluster_dims__(CR, 1, 1) __launch_bounds__(cluster_threads(CR)
     }
     // remote addresses this thread pushes to (lanes 0 .. CR - 1: CTA `lane`), word wi_own of each buffer
     const uint32_t dst_rank = uint32_t(lane % CR);
-    const uint32_t dst_fu = cl_map(sm_addr(FU + wi_own), dst_rank);
-    const uint32_t dst_nl = cl_map(sm_addr(NLc + wi_own), dst_rank);
+    const uint32_t dst_fx = cl_map(sm_addr(FX + wi_own), dst_rank);
     const uint32_t dst_mb = cl_map(sm_addr(mbar), dst_rank);
 
     Xoshiro rng;
@@ -791,7 +788,7 @@ __global__ void __cluster_dims__(CR, 1, 1) __launch_bounds__(cluster_threads(CR)
                 if (job.err) atomicCAS(job.err, 0, kClusterErrRecv);
             }
             Dh[(par * NH + role - 1) * CT + st] = cluster_words_d<BPT>(
-                Jr + st * 16, reinterpret_cast<const uint4*>(FU + par * 64), st & 7, NH == 1 ? BPT : BPT * role);
+                Jr + st * 16, FX + par * 64, st & 7, NH == 1 ? BPT : BPT * role);
             asm volatile("bar.arrive 1, %0;" ::"r"(cluster_threads(CR)) : "memory");
         }
     } else {
@@ -818,8 +815,8 @@ __global__ void __cluster_dims__(CR, 1, 1) __launch_bounds__(cluster_threads(CR)
             const uint32_t nlw = __ballot_sync(FULL, ln);
             if (lane < CR) {
                 const uint32_t bar = dst_mb + 8u * uint32_t(par);
-                st_async2(dst_fu + 8u * 64u * uint32_t(par), fw, uw, bar);
-                st_async1(dst_nl + 4u * 64u * uint32_t(par), uint32_t(__popc(nlw)) | (uint32_t(__popc(fw)) << 16), bar);
+                st_async4(dst_fx + 16u * 64u * uint32_t(par), fw, uw,
+                          uint32_t(__popc(nlw)) | (uint32_t(__popc(fw)) << 16), 0u, bar);
             }
             const uint32_t my_bar = sm_addr(mbar + par);
             if (tid == 0)
@@ -835,8 +832,9 @@ __global__ void __cluster_dims__(CR, 1, 1) __launch_bounds__(cluster_threads(CR)
                 if (job.err) atomicCAS(job.err, 0, kClusterErrRecv);
             }
             // n_lin and |F| of step t: each warp sums the 64 packed counts (low half: band, high half: flips)
-            // (one warp reduction instruction instead of a chain of five shuffles)
-            const uint32_t pc = __reduce_add_sync(FULL, NLc[par * 64 + 2 * lane] + NLc[par * 64 + 2 * lane + 1]);
+            // (one warp reduction instruction instead of a chain of five shuffles; records lane and lane + 32, so a
+            // load's 32 fields fall on 8 banks, where records 2 lane and 2 lane + 1 fell on 4)
+            const uint32_t pc = __reduce_add_sync(FULL, FX[par * 64 + lane].z + FX[par * 64 + 32 + lane].z);
             int32_t nf = int32_t(pc >> 16);
             if (t >= 0) {
                 nlin_prev = int32_t(pc & 0xffffu);
@@ -844,16 +842,16 @@ __global__ void __cluster_dims__(CR, 1, 1) __launch_bounds__(cluster_threads(CR)
                 if (tid == 0) flips += nf;
             }
             // D: the 64 words at once, or the first blocks here and the rest by the helpers (handed over at barrier 1)
-            const uint4* FUv = reinterpret_cast<const uint4*>(FU + par * 64);   // {F_2q, U_2q, F_2q+1, U_2q+1}
+            const uint4* FXv = FX + par * 64;
             const uint4* Jv = Jr + st * 16;
             int32_t D;
             if (HELP) {
-                D = cluster_words_d<BPT>(Jv, FUv, st & 7, 0);
+                D = cluster_words_d<BPT>(Jv, FXv, st & 7, 0);
                 asm volatile("bar.sync 1, %0;" ::"r"(cluster_threads(CR)) : "memory");
 #pragma unroll
                 for (int j = 0; j < NH; ++j) D += Dh[(par * NH + j) * CT + st];
             } else {
-                D = cluster_words_d<4>(Jv, FUv, st & 7, 0);
+                D = cluster_words_d<4>(Jv, FXv, st & 7, 0);
             }
             // the diagonal: if y itself is in F, its term (J_yy = 0, stored as a 0 bit) was counted as -s'_y
             if (fl) {
