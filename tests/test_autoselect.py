@@ -24,7 +24,7 @@ def _estimate(c):
 
 def test_picks_near_the_fastest_engine():
     """With the flip fraction a run saw, the model's pick is within 20% of the fastest measured engine in every
-    case (11% measured), and within 3% over the geometric mean of all cases (0.3% measured)."""
+    case (6% measured), and within 3% over the geometric mean of all cases (0.2% measured)."""
     logs = []
     for c in _cases():
         est = _estimate(c)
