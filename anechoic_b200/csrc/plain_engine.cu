@@ -695,7 +695,8 @@ __device__ __forceinline__ int32_t cluster_words_d(const uint4* Jv, const uint4*
 // Update helpers per owned slot and threads per CTA of the cluster kernel. With 16 CTAs one helper sums words
 // 32 .. 63 of each slot's update (1.062 ms per 1000 steps for one anneal with two pushes per word, where three helpers
 // of 16 words each took 1.092 and none 1.13; 0.994 with the packed counts summed by one warp reduction; 0.870 with one
-// 16-byte push per word, 0.855 with the counts read at a 16-byte stride); with 8 CTAs the SM's ALU is already the bound and a helper gained nothing.
+// 16-byte push per word, 0.855 with the counts read at a 16-byte stride); with 8 CTAs the SM's ALU is already the
+// bound and a helper gained nothing.
 __host__ __device__ constexpr int cluster_helpers(int cr) { return cr == 16 ? 1 : 0; }
 __host__ __device__ constexpr int cluster_threads(int cr) { return (2048 / cr) * (1 + cluster_helpers(cr)); }
 
